@@ -1,0 +1,350 @@
+"""Test helpers: fixtures, the compiled-model arrays, and ctypes wrappers over the checkers in oracle/_ref.
+
+Only tests, __graft_entry__.smoke() and bench.py's CPU baseline use this module; the oracle is the checker of the
+CUDA path, never part of it.
+"""
+import ctypes as C
+import gzip
+import json
+import os
+import shutil
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+_CACHE = os.path.join(tempfile.gettempdir(), "sinksim_b200_fixtures")
+
+
+def fixture(name):
+    """Path of a fixture in tests/golden, decompressed into a temporary cache when it is stored gzip-compressed."""
+    src = os.path.join(GOLDEN, name)
+    if os.path.exists(src):
+        return src
+    gz = src + ".gz"
+    if not os.path.exists(gz):
+        raise FileNotFoundError(src)
+    os.makedirs(_CACHE, exist_ok=True)
+    dst = os.path.join(_CACHE, name)
+    if not os.path.exists(dst) or os.path.getmtime(dst) < os.path.getmtime(gz):
+        with gzip.open(gz, "rb") as f, open(dst + ".tmp", "wb") as g:
+            shutil.copyfileobj(f, g)
+        os.replace(dst + ".tmp", dst)
+    return dst
+
+
+def read_json(path):
+    if path.endswith(".gz"):
+        with gzip.open(path, "rt") as f:
+            return json.load(f)
+    with open(path) as f:
+        return json.load(f)
+
+
+def titanic():
+    return fixture("titanic64.ship.json"), fixture("titanic.sim.json")
+
+
+# ----------------------------------------------------------------------------------------------- model arrays
+
+def f64(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.float64))
+
+
+def i32(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.int32))
+
+
+def u8(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.uint8))
+
+
+def load_model(ship_path, sim_path):
+    """The arrays of a compiled ship and sim as numpy arrays (the members the kernel reads)."""
+    s = read_json(ship_path)
+    m = read_json(sim_path)
+    c, n, g = s["columns"], s["nodes"], s["segments"]
+    ship = dict(x=f64(c["x"]), y=f64(c["y"]), dxdy=f64(c["dxdy"]), zlo=f64(c["zlo"]), zhi=f64(c["zhi"]),
+                segCol=i32(g["col"]), segA=f64(g["a"]), segE=f64(g["e"]), mu=f64(n["mu"]), vmax=f64(n["vmax"]),
+                amin=f64(n["amin"]), aov=f64(n["aov"]), segStart=i32(n["segStart"]), segCount=i32(n["segCount"]))
+    G, K, Mo, Mk, Fo, B, R, S0 = (m[k] for k in ("groups", "connections", "monitors", "marks", "founder", "body", "readout", "state0"))
+    sim = dict(rho=float(m["constants"]["rho"]), g=float(m["constants"]["g"]), dt=float(m["scheme"]["dt"]),
+               gStart=i32(G["nodeStart"]), gCount=i32(G["nodeCount"]), gNodes=i32(G["nodes"]), gMode=u8(G["mode"]),
+               gpx=f64(G["px"]), gpy=f64(G["py"]), gpz=f64(G["pz"]), gMargin=float(G["margin"]),
+               ca=i32(K["a"]), cb=i32(K["b"]), law=u8(K["type"]), cx=f64(K["x"]), cy=f64(K["y"]), cz=f64(K["z"]),
+               area=f64(K["area"]), coef=f64(K["coef"]), kind=u8(K["kind"]), idx=i32(K["idx"]), en=u8(K["en"]),
+               tOn=f64(K["tOn"]), skipGroup=i32(K["skipGroup"]), monitor=i32(K["monitor"]),
+               kindNames=list(K.get("kindNames", [])),
+               nmon=len(Mo["id"]), monThreshold=float(Mo["threshold"]), monitorId=list(Mo["id"]), markId=list(Mk["id"]),
+               mkx=f64(Mk["x"]), mky=f64(Mk["y"]), mkz=f64(Mk["z"]), mkWhen=u8(Mk["when"]),
+               founder=[float(Fo[k]) for k in ("hullTopBelow", "pitchAbsAbove", "buoyancyBelow", "minT")],
+               body=[float(B["ms"]), float(B["KG"]), *map(float, B["g0"]), float(B["XO"]), float(B["YO"]),
+                     *(float(B[k]) for k in ("mh0", "Ith0", "Iph0", "cDz", "cDth", "cDph", "qz", "qth", "qph"))],
+               xFP=float(R["xFP"]), xAP=float(R["xAP"]),
+               state0=[float(S0[k]) for k in ("t", "zO", "pitch", "roll", "vz", "wth", "wph")],
+               vol0=f64(S0["vol"]), level0=f64(S0["level"]), cx0=f64(S0["cx"]), cy0=f64(S0["cy"]), cz0=f64(S0["cz"]))
+    return ship, sim
+
+
+def trace_records(tr, which):
+    """Records of a trace's dense or samples block as an (n, 10 + 5 N) array in the record layout."""
+    d = tr[which]
+    N = tr["nodes"]
+    n = d["n"]
+    out = np.empty((n, 10 + 5 * N))
+    for j, k in enumerate(("t", "zO", "pitch", "roll", "vz", "wth", "wph", "inflow", "Vb", "hullTop")):
+        out[:, j] = d[k]
+    for j, k in enumerate(("vol", "level", "cx", "cy", "cz")):
+        out[:, 10 + j * N:10 + (j + 1) * N] = np.asarray(d[k], dtype=np.float64).reshape(n, N)
+    return out
+
+
+# ----------------------------------------------------------------------------------------------- the C restatement
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class _Ship(C.Structure):
+    _fields_ = [("ncol", C.c_int32), ("nseg", C.c_int32), ("nnode", C.c_int32)] + \
+               [(k, C.POINTER(C.c_double)) for k in ("x", "y", "dxdy", "zlo", "zhi")] + \
+               [("segCol", C.POINTER(C.c_int32))] + [(k, C.POINTER(C.c_double)) for k in ("segA", "segE", "mu", "vmax", "amin", "aov")] + \
+               [(k, C.POINTER(C.c_int32)) for k in ("segStart", "segCount")]
+
+
+class _Sim(C.Structure):
+    _fields_ = [("rho", C.c_double), ("g", C.c_double), ("dt", C.c_double), ("ngroup", C.c_int32)] + \
+               [(k, C.POINTER(C.c_int32)) for k in ("gStart", "gCount", "gNodes")] + [("gMode", C.POINTER(C.c_uint8))] + \
+               [(k, C.POINTER(C.c_double)) for k in ("gpx", "gpy", "gpz")] + [("gMargin", C.c_double), ("nconn", C.c_int32)] + \
+               [(k, C.POINTER(C.c_int32)) for k in ("ca", "cb")] + [("law", C.POINTER(C.c_uint8))] + \
+               [(k, C.POINTER(C.c_double)) for k in ("cx", "cy", "cz", "area", "coef")] + [("en", C.POINTER(C.c_uint8)), ("tOn", C.POINTER(C.c_double))] + \
+               [(k, C.POINTER(C.c_int32)) for k in ("skipGroup", "monitor")] + [("nmon", C.c_int32), ("monThreshold", C.c_double), ("nmark", C.c_int32)] + \
+               [(k, C.POINTER(C.c_double)) for k in ("mkx", "mky", "mkz")] + [("mkWhen", C.POINTER(C.c_uint8))] + \
+               [(k, C.c_double) for k in ("hullTopBelow", "pitchAbsAbove", "buoyancyBelow", "minT")] + \
+               [("body", C.c_double * 16), ("xFP", C.c_double), ("xAP", C.c_double), ("state0", C.c_double * 7)] + \
+               [(k, C.POINTER(C.c_double)) for k in ("vol0", "level0", "cx0", "cy0", "cz0")]
+
+
+class _Counters(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("steps", "columns", "passes", "segVisits", "segWet", "colWet", "weirPow", "orifice", "weir", "newton")]
+
+
+_oracle_lib = None
+
+
+def oracle_lib():
+    global _oracle_lib
+    if _oracle_lib is None:
+        lib = C.CDLL(os.path.join(REF_DIR, "libsinksim_oracle.so"))
+        lib.sso_create.restype = C.c_void_p
+        lib.sso_create.argtypes = [C.POINTER(_Ship), C.POINTER(_Sim), C.c_int]
+        for name in ("sso_destroy", "sso_reset"):
+            getattr(lib, name).argtypes = [C.c_void_p]
+        lib.sso_set_connection.argtypes = [C.c_void_p, C.c_int32, C.c_int, C.c_double, C.c_double]
+        lib.sso_step.argtypes = [C.c_void_p, C.c_int64]
+        lib.sso_get_record.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.sso_restore.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.sso_readouts.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.sso_events.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
+        lib.sso_foundered.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.sso_counters_get.argtypes = [C.c_void_p, C.POINTER(_Counters)]
+        lib.sso_flows.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        _oracle_lib = lib
+    return _oracle_lib
+
+
+class Oracle:
+    """The C restatement of the reference step (oracle/sinksim_oracle.c) on one compiled model."""
+
+    def __init__(self, ship, sim, mixed=False):
+        self.lib = oracle_lib()
+        self.ship, self.sim = ship, sim
+        self.nodes = len(ship["mu"])
+        self.nconn = len(sim["ca"])
+        S = _Ship(len(ship["x"]), len(ship["segCol"]), self.nodes,
+                  *(_p(ship[k], C.c_double) for k in ("x", "y", "dxdy", "zlo", "zhi")), _p(ship["segCol"], C.c_int32),
+                  *(_p(ship[k], C.c_double) for k in ("segA", "segE", "mu", "vmax", "amin", "aov")),
+                  _p(ship["segStart"], C.c_int32), _p(ship["segCount"], C.c_int32))
+        m = sim
+        M = _Sim(m["rho"], m["g"], m["dt"], len(m["gCount"]), _p(m["gStart"], C.c_int32), _p(m["gCount"], C.c_int32),
+                 _p(m["gNodes"], C.c_int32), _p(m["gMode"], C.c_uint8), _p(m["gpx"], C.c_double), _p(m["gpy"], C.c_double),
+                 _p(m["gpz"], C.c_double), m["gMargin"], len(m["ca"]), _p(m["ca"], C.c_int32), _p(m["cb"], C.c_int32),
+                 _p(m["law"], C.c_uint8), *(_p(m[k], C.c_double) for k in ("cx", "cy", "cz", "area", "coef")),
+                 _p(m["en"], C.c_uint8), _p(m["tOn"], C.c_double), _p(m["skipGroup"], C.c_int32), _p(m["monitor"], C.c_int32),
+                 m["nmon"], m["monThreshold"], len(m["mkx"]), *(_p(m[k], C.c_double) for k in ("mkx", "mky", "mkz")),
+                 _p(m["mkWhen"], C.c_uint8), *m["founder"], (C.c_double * 16)(*m["body"]), m["xFP"], m["xAP"],
+                 (C.c_double * 7)(*m["state0"]), *(_p(m[k], C.c_double) for k in ("vol0", "level0", "cx0", "cy0", "cz0")))
+        self.h = self.lib.sso_create(C.byref(S), C.byref(M), 1 if mixed else 0)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.sso_destroy(self.h)
+            self.h = None
+
+    def reset(self):
+        self.lib.sso_reset(self.h)
+
+    def set_connection(self, c, enabled=-1, area=float("nan"), tOn=float("nan")):
+        self.lib.sso_set_connection(self.h, c, enabled, area, tOn)
+
+    def step(self, n=1):
+        self.lib.sso_step(self.h, n)
+
+    def record(self):
+        r = np.empty(10 + 5 * self.nodes)
+        self.lib.sso_get_record(self.h, _p(r, C.c_double))
+        return r
+
+    def restore(self, rec):
+        rec = f64(rec)
+        self.lib.sso_restore(self.h, _p(rec, C.c_double))
+
+    def readouts(self):
+        r = np.empty(7)
+        self.lib.sso_readouts(self.h, _p(r, C.c_double))
+        return r
+
+    def events(self):
+        buf = np.empty(3 * 1024)
+        n = self.lib.sso_events(self.h, _p(buf, C.c_double), 1024)
+        return [(buf[3 * i], int(buf[3 * i + 1]), int(buf[3 * i + 2])) for i in range(n)]
+
+    def foundered(self):
+        t = C.c_double()
+        f = self.lib.sso_foundered(self.h, C.byref(t))
+        return bool(f), t.value
+
+    def counters(self):
+        c = _Counters()
+        self.lib.sso_counters_get(self.h, C.byref(c))
+        return {k: getattr(c, k) for k, _ in _Counters._fields_}
+
+    def flows(self):
+        q = np.empty(self.nconn)
+        self.lib.sso_flows(self.h, _p(q, C.c_double))
+        return q
+
+
+# ----------------------------------------------------------------------------------------------- the reference engine
+
+_ref_lib = None
+
+
+def ref_lib():
+    global _ref_lib
+    if _ref_lib is None:
+        lib = C.CDLL(os.path.join(REF_DIR, "libsinksim_ref.so"))
+        lib.ssref_last_error.restype = C.c_char_p
+        lib.ssref_open.restype = C.c_void_p
+        lib.ssref_open.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p]
+        lib.ssref_close.argtypes = [C.c_void_p]
+        lib.ssref_nodes.argtypes = [C.c_void_p]
+        lib.ssref_connections.argtypes = [C.c_void_p]
+        lib.ssref_set_connection.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double]
+        lib.ssref_apply_sweep_instance.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
+        lib.ssref_step.argtypes = [C.c_void_p, C.c_longlong]
+        lib.ssref_state.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.ssref_restore.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.ssref_evaluate_hydro.argtypes = [C.c_void_p]
+        lib.ssref_events.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
+        lib.ssref_foundered.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.ssref_readouts.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.ssref_run.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double), C.c_int]
+        lib.ssref_time_steps.restype = C.c_longlong
+        lib.ssref_time_steps.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_longlong, C.c_int, C.POINTER(C.c_double)]
+        _ref_lib = lib
+    return _ref_lib
+
+
+class RefSim:
+    """The reference CPU engine (sinksim::Simulation) on one compiled ship and sim."""
+
+    def __init__(self, ship_path, sim_path, numerics="portable"):
+        self.lib = ref_lib()
+        self.h = self.lib.ssref_open(ship_path.encode(), sim_path.encode(), numerics.encode())
+        if not self.h:
+            raise RuntimeError(self.lib.ssref_last_error().decode())
+        self.nodes = self.lib.ssref_nodes(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ssref_close(self.h)
+            self.h = None
+
+    def _ok(self, rc):
+        if rc < 0:
+            raise RuntimeError(self.lib.ssref_last_error().decode())
+        return rc
+
+    def set_connection(self, c, enabled=-1, area=float("nan"), tOn=float("nan")):
+        self._ok(self.lib.ssref_set_connection(self.h, c, enabled, area, tOn))
+
+    def apply_sweep_instance(self, sweep_path, i):
+        self._ok(self.lib.ssref_apply_sweep_instance(self.h, sweep_path.encode(), i))
+
+    def step(self, n=1):
+        self._ok(self.lib.ssref_step(self.h, n))
+
+    def record(self):
+        r = np.empty(10 + 5 * self.nodes)
+        self.lib.ssref_state(self.h, _p(r, C.c_double))
+        return r
+
+    def restore(self, rec):
+        rec = f64(rec)
+        self._ok(self.lib.ssref_restore(self.h, _p(rec, C.c_double)))
+
+    def readouts(self):
+        r = np.empty(7)
+        self.lib.ssref_readouts(self.h, _p(r, C.c_double))
+        return r
+
+    def events(self):
+        buf = np.empty(3 * 1024)
+        n = self._ok(self.lib.ssref_events(self.h, _p(buf, C.c_double), 1024))
+        return [(buf[3 * i], int(buf[3 * i + 1]), int(buf[3 * i + 2])) for i in range(n)]
+
+    def foundered(self):
+        t = C.c_double()
+        f = self.lib.ssref_foundered(self.h, C.byref(t))
+        return bool(f), t.value
+
+    def run(self, tMax, every, stop_when_stable=False, rule=None, cap=4096):
+        """Simulation::run; returns (summary dict, curve array (records, 7))."""
+        summary = np.zeros(5)
+        curve = np.empty((cap, 7))
+        rule_arr = f64(rule) if rule is not None else None
+        rp = _p(rule_arr, C.c_double) if rule_arr is not None else None
+        n = self._ok(self.lib.ssref_run(self.h, tMax, every, 1 if stop_when_stable else 0, rp, _p(summary, C.c_double),
+                                        _p(curve, C.c_double), cap))
+        return dict(steps=int(summary[0]), foundered=bool(summary[1]), founderT=summary[2], tEnd=summary[3],
+                    retired=int(summary[4])), curve[:min(n, cap)].copy()
+
+
+def ref_time_steps(ship_path, sim_path, numerics, count, max_steps, threads):
+    """Times the reference CPU engine over a bounded sample; returns (steps, seconds)."""
+    lib = ref_lib()
+    sec = C.c_double()
+    steps = lib.ssref_time_steps(ship_path.encode(), sim_path.encode(), numerics.encode(), count, max_steps, threads, C.byref(sec))
+    if steps < 0:
+        raise RuntimeError(lib.ssref_last_error().decode())
+    return steps, sec.value
+
+
+def ref_tool(name):
+    return os.path.join(REF_DIR, name)
+
+
+def fdlibm_ref():
+    lib = C.CDLL(os.path.join(REF_DIR, "libfdlibm_ref.so"))
+    for fn in ("fdlibm_sin", "fdlibm_cos"):
+        getattr(lib, fn).restype = C.c_double
+        getattr(lib, fn).argtypes = [C.c_double]
+    lib.fdlibm_pow.restype = C.c_double
+    lib.fdlibm_pow.argtypes = [C.c_double, C.c_double]
+    lib.fdlibm_scalbn.restype = C.c_double
+    lib.fdlibm_scalbn.argtypes = [C.c_double, C.c_int]
+    return lib
