@@ -1,0 +1,163 @@
+/* sinksim-b200: the C ABI of the B200 batch flooding engine (libsinksim_b200.so).
+ *
+ * A drop-in for the batch path of the reference sinksim engine: the same compiled ship / sim / sweep files, the
+ * same per-instance connection setters and the same batch-results, curves, events and traces. Each entry point
+ * names the reference interface it replaces (paths are files of the reference repository).
+ *
+ * Conventions: plain pointers and sizes only. Every function returns SSB_OK (0) on success or a negative SSB_E*
+ * code; ssb_last_error() then describes the failure (thread-local, valid until the next call on that thread).
+ * Handles are not thread-safe; use one per thread. Numerics: 0 = "portable" (double precision), 1 = "portable32"
+ * (single-precision column partials); the reference's "oracle" and "std" numerics exist on its CPU only and are
+ * rejected here (SSB_EUNSUPPORTED), as the reference's GPU runner rejects them (apps/sinksim_cuda_run.cpp:171-175).
+ *
+ * State records use the reference trace record layout (engine/src/trace.cpp:140-150): t, zO, pitch, roll, vz,
+ * wth, wph, inflow, Vb, hullTop, then vol, level, cx, cy, cz for each of the N nodes: 10 + 5 N doubles.
+ * Readout records are 7 doubles: t, trim (deg), list (deg), water (t), inflow (t/min), draftF, draftA
+ * (engine/include/sinksim/cuda/batch.hpp:39-43).
+ */
+#ifndef SINKSIM_B200_H
+#define SINKSIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SSB_OK 0
+#define SSB_EINVAL (-1)       /* bad argument: the reference throws std::invalid_argument / std::out_of_range */
+#define SSB_ERUNTIME (-2)     /* I/O, format, hash or CUDA failure: the reference throws std::runtime_error */
+#define SSB_ESTATE (-3)       /* call out of order (set after run, result before run): std::logic_error */
+#define SSB_EUNSUPPORTED (-4) /* a numerics or option the GPU engine does not provide */
+#define SSB_ENODEVICE (-5)    /* no usable CUDA device */
+
+typedef struct ssb_batch ssb_batch;
+
+/* Options of a batch: engine/include/sinksim/cuda/batch.hpp:27-37 (BatchOptions), plus the launch shape and the
+ * batching workloads' extra retire rule. Initialise with ssb_batch_options_init. */
+typedef struct ssb_batch_options {
+  int32_t count;             /* instances (>= 1) */
+  int32_t numerics;          /* 0 portable, 1 portable32 (the reference's mixedPrecision) */
+  int32_t traced_instances;  /* leading instances that record traces */
+  int32_t dense_steps;       /* dense records at the start of each trace */
+  double sample_every;       /* s between sampled trace records */
+  double curve_every;        /* s between readout-curve records of every instance; 0: none */
+  double t_max;              /* s: every instance stops here if it has not foundered */
+  int64_t steps_per_launch;  /* 0: one persistent launch; > 0: bounded launches (the reference's stepsPerLaunch) */
+  int32_t warps_per_block;   /* simulations per block; 0: chosen by the engine */
+  int32_t blocks;            /* grid size; 0: persistent grid sized to the device */
+  int32_t device;            /* CUDA device ordinal */
+  /* extra retire rule (disabled when rule_enabled == 0): an instance stops once |pitch| > rule_pitch and the deck
+   * edge point (rule_x, +-rule_y, rule_z) is below the sea ("sink"), or once |pitch rate| < rule_wth has held for
+   * rule_settle seconds ("settle"). It never changes the physics. */
+  int32_t rule_enabled;
+  double rule_pitch, rule_x, rule_y, rule_z, rule_wth, rule_settle;
+} ssb_batch_options;
+
+typedef struct ssb_device_info {
+  char name[256];
+  int32_t major, minor, multiprocessors;
+  uint64_t global_memory, shared_per_block_optin;
+  int32_t runtime_version, driver_version;
+} ssb_device_info;
+
+/* Summary of one instance after a run: engine/include/sinksim/cuda/batch.hpp:45-54 (InstanceResult). */
+typedef struct ssb_instance_summary {
+  int32_t foundered;
+  int32_t stop_reason; /* 1 foundered, 2 tMax, 3 sink rule, 4 settle rule, 0 still running */
+  double founder_t, t_end;
+  int64_t steps;
+  int32_t event_count;
+  int32_t curve_count;  /* records of ssb_batch_curve, the final record included */
+  double outputs[7];    /* inflow, Vb, hullTop, mw, bx, by, bz of the last step */
+} ssb_instance_summary;
+
+typedef struct ssb_launch_info {
+  int32_t warps_per_block, blocks, blocks_per_sm;
+  uint64_t slot_bytes;  /* shared memory of one simulation */
+} ssb_launch_info;
+
+/* The message of the last failure on this thread. */
+const char* ssb_last_error(void);
+/* Library version string. */
+const char* ssb_version(void);
+
+/* Is a CUDA device present? Returns 1 or 0; `why` (may be NULL) receives the reason. cuda::available,
+ * engine/include/sinksim/cuda/batch.hpp:17. */
+int ssb_available(char* why, size_t why_cap);
+/* cuda::device_info, engine/include/sinksim/cuda/batch.hpp:19-25. */
+int ssb_get_device_info(int32_t device, ssb_device_info* out);
+
+void ssb_batch_options_init(ssb_batch_options* opt);
+
+/* Loads and verifies a compiled ship and sim (io::load_ship / io::load_sim / io::check_pairing,
+ * engine/src/compiled.cpp:108-279) and creates a batch of opt->count instances of it
+ * (cuda::Batch::Batch, engine/cuda/batch.cu:170-209). */
+int ssb_batch_create(const char* ship_path, const char* sim_path, const ssb_batch_options* opt, ssb_batch** out);
+void ssb_batch_destroy(ssb_batch* b);
+int ssb_batch_nodes(const ssb_batch* b, int32_t* nodes, int32_t* connections);
+int ssb_batch_launch_info(const ssb_batch* b, ssb_launch_info* out);
+
+/* Per-instance setup before the run: cuda::Batch::restore / set_connection_enabled / set_connection_area /
+ * set_connection_activation (engine/cuda/batch.cu:217-243). */
+int ssb_batch_restore(ssb_batch* b, int32_t instance, const double* record);
+int ssb_batch_set_connection_enabled(ssb_batch* b, int32_t instance, int32_t connection, int32_t enabled);
+int ssb_batch_set_connection_area(ssb_batch* b, int32_t instance, int32_t connection, double area);
+int ssb_batch_set_connection_activation(ssb_batch* b, int32_t instance, int32_t connection, double t_on);
+/* Instance i takes instance i of a sweep file: sweep::apply (engine/include/sinksim/sweep.hpp:49-65) through the
+ * setters above, as sinksim_cuda_run --sweep does (apps/sinksim_cuda_run.cpp:37-41). The sweep must have exactly
+ * opt->count instances. */
+int ssb_batch_apply_sweep(ssb_batch* b, const char* sweep_path);
+
+/* cuda::Batch::run (engine/cuda/batch.cu:245-308): uploads the instances, runs every one to its end, downloads the
+ * results. *seconds (may be NULL) receives the wall time. */
+int ssb_batch_run(ssb_batch* b, double* seconds);
+/* The same in three parts, for callers that time the device alone: ssb_batch_launch's *device_ms is measured with
+ * CUDA events on the engine's stream around the kernel launches. */
+int ssb_batch_upload(ssb_batch* b);
+/* Makes a finished batch runnable again from its staged inputs (initial states and connection fields as set):
+ * repeated runs of one batch, for calibration loops and benchmarks. No counterpart in the reference, whose
+ * cuda::Batch::run throws when called twice (engine/cuda/batch.cu:246). */
+int ssb_batch_reset(ssb_batch* b);
+int ssb_batch_launch(ssb_batch* b, float* device_ms);
+int ssb_batch_download(ssb_batch* b);
+/* Bytes one run copies host to device and device to host (inputs and results). */
+int ssb_batch_transfer_bytes(const ssb_batch* b, uint64_t* h2d, uint64_t* d2h);
+
+/* Results after the run: cuda::Batch::total_steps / result / curve / final_readouts / trace
+ * (engine/cuda/batch.cu:302-400). */
+int ssb_batch_total_steps(const ssb_batch* b, int64_t* steps);
+int ssb_batch_summary(const ssb_batch* b, int32_t instance, ssb_instance_summary* out);
+int ssb_batch_state(const ssb_batch* b, int32_t instance, double* record);
+/* Events in firing order: time, index (monitor or mark; -1 for the founder) and kind (0 overflow, 1 mark,
+ * 2 founder). Writes at most cap; returns the count through *count. */
+int ssb_batch_events(const ssb_batch* b, int32_t instance, double* t, int32_t* id, int32_t* kind, int32_t cap, int32_t* count);
+/* The readout curve (7 values per record), closed by the final readouts; at most cap records. */
+int ssb_batch_curve(const ssb_batch* b, int32_t instance, double* records, int32_t cap, int32_t* count);
+int ssb_batch_final_readouts(const ssb_batch* b, int32_t instance, double* record7);
+/* io::save_trace of cuda::Batch::trace(instance) (engine/src/trace.cpp:272-308). */
+int ssb_batch_save_trace(const ssb_batch* b, int32_t instance, const char* path);
+/* sweep::save_results of the batch (engine/src/sweep.cpp:163-201); instance ids come from the sweep file when
+ * sweep_path is not NULL. */
+int ssb_batch_save_results(const ssb_batch* b, const char* sweep_path, const char* results_path);
+
+/* sinksim_cuda_run --sweep (apps/sinksim_cuda_run.cpp:26-83) in one call: numerics "portable" or "portable32".
+ * *steps and *seconds (may be NULL) receive the aggregate steps and the wall time. */
+int ssb_run_sweep(const char* ship_path, const char* sim_path, const char* sweep_path, const char* numerics, const char* results_path,
+                  int64_t* steps, double* seconds);
+/* sinksim_sweep --compare (apps/sinksim_sweep.cpp:19-31, engine/src/sweep.cpp:234-281): exact comparison.
+ * *differing receives the count of differing values; first (may be NULL) the first difference. */
+int ssb_compare_results(const char* a_path, const char* b_path, uint64_t* compared, uint64_t* differing, char* first, size_t first_cap);
+
+/* The portable math of the engine, evaluated on the host and on the device (for parity checks of the device
+ * code): op 0 sin(x), 1 cos(x), 2 pow(x, y), 3 scalbn(x, (int)y). The reference's fdlibm port,
+ * engine/include/sinksim/kernel/fdlibm_portable.hpp:71-435. */
+int ssb_portable_math_host(int32_t op, const double* x, const double* y, double* out, int64_t n);
+int ssb_portable_math_device(int32_t op, const double* x, const double* y, double* out, int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,306 @@
+"""sinksim_b200: a B200-native batch engine for ship flooding simulation.
+
+A drop-in for the batch path of the reference sinksim engine: it reads the same compiled ship, sim and sweep files,
+computes the same "portable" / "portable32" numerics bit for bit, and writes the same batch-results and traces.
+This module is the Python face of the C ABI in include/sinksim_b200.h (libsinksim_b200.so, built in the source tree
+by ``python -m sinksim_b200.build``). It mirrors the reference's ``cuda::Batch`` (engine/include/sinksim/cuda/batch.hpp)
+and the two batch tools (apps/sinksim_cuda_run.cpp, apps/sinksim_sweep.cpp).
+
+There is no CPU fallback: without the built library or a CUDA device every entry point raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = ["Batch", "SinksimError", "available", "device_info", "run_sweep", "compare_results", "portable_math", "library_path",
+           "STOP_REASONS", "NUMERICS"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsinksim_b200.so")
+NUMERICS = {"portable": 0, "portable32": 1}
+STOP_REASONS = {0: "running", 1: "foundered", 2: "tmax", 3: "sink-rule", 4: "settle-rule"}
+_ERRORS = {-1: "invalid argument", -2: "runtime error", -3: "call out of order", -4: "unsupported", -5: "no CUDA device"}
+
+
+class SinksimError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"{_ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+class _Options(C.Structure):
+    _fields_ = [("count", C.c_int32), ("numerics", C.c_int32), ("traced_instances", C.c_int32), ("dense_steps", C.c_int32),
+                ("sample_every", C.c_double), ("curve_every", C.c_double), ("t_max", C.c_double), ("steps_per_launch", C.c_int64),
+                ("warps_per_block", C.c_int32), ("blocks", C.c_int32), ("device", C.c_int32), ("rule_enabled", C.c_int32),
+                ("rule_pitch", C.c_double), ("rule_x", C.c_double), ("rule_y", C.c_double), ("rule_z", C.c_double),
+                ("rule_wth", C.c_double), ("rule_settle", C.c_double)]
+
+
+class _DeviceInfo(C.Structure):
+    _fields_ = [("name", C.c_char * 256), ("major", C.c_int32), ("minor", C.c_int32), ("multiprocessors", C.c_int32),
+                ("global_memory", C.c_uint64), ("shared_per_block_optin", C.c_uint64), ("runtime_version", C.c_int32),
+                ("driver_version", C.c_int32)]
+
+
+class _Summary(C.Structure):
+    _fields_ = [("foundered", C.c_int32), ("stop_reason", C.c_int32), ("founder_t", C.c_double), ("t_end", C.c_double),
+                ("steps", C.c_int64), ("event_count", C.c_int32), ("curve_count", C.c_int32), ("outputs", C.c_double * 7)]
+
+
+class _LaunchInfo(C.Structure):
+    _fields_ = [("warps_per_block", C.c_int32), ("blocks", C.c_int32), ("blocks_per_sm", C.c_int32), ("slot_bytes", C.c_uint64)]
+
+
+_lib = None
+
+_SIGNATURES = {
+    "ssb_last_error": (C.c_char_p, []),
+    "ssb_version": (C.c_char_p, []),
+    "ssb_available": (C.c_int, [C.c_char_p, C.c_size_t]),
+    "ssb_get_device_info": (C.c_int, [C.c_int32, C.POINTER(_DeviceInfo)]),
+    "ssb_batch_options_init": (None, [C.POINTER(_Options)]),
+    "ssb_batch_create": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_Options), C.POINTER(C.c_void_p)]),
+    "ssb_batch_destroy": (None, [C.c_void_p]),
+    "ssb_batch_nodes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "ssb_batch_launch_info": (C.c_int, [C.c_void_p, C.POINTER(_LaunchInfo)]),
+    "ssb_batch_restore": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
+    "ssb_batch_set_connection_enabled": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
+    "ssb_batch_set_connection_area": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double]),
+    "ssb_batch_set_connection_activation": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double]),
+    "ssb_batch_apply_sweep": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "ssb_batch_run": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "ssb_batch_upload": (C.c_int, [C.c_void_p]),
+    "ssb_batch_reset": (C.c_int, [C.c_void_p]),
+    "ssb_batch_launch": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "ssb_batch_download": (C.c_int, [C.c_void_p]),
+    "ssb_batch_transfer_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "ssb_batch_total_steps": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "ssb_batch_summary": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_Summary)]),
+    "ssb_batch_state": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
+    "ssb_batch_events": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32,
+                                   C.POINTER(C.c_int32)]),
+    "ssb_batch_curve": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_int32)]),
+    "ssb_batch_final_readouts": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
+    "ssb_batch_save_trace": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p]),
+    "ssb_batch_save_results": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p]),
+    "ssb_run_sweep": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
+    "ssb_compare_results": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]),
+    "ssb_portable_math_host": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64]),
+    "ssb_portable_math_device": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64]),
+}
+
+
+def library_path():
+    return LIB_PATH
+
+
+def lib():
+    """The loaded libsinksim_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m sinksim_b200.build` (there is no CPU fallback)")
+        h = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            f = getattr(h, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = h
+    return _lib
+
+
+def _check(rc):
+    if rc < 0:
+        raise SinksimError(rc, lib().ssb_last_error().decode())
+    return rc
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _b(s):
+    return None if s is None else os.fsencode(s)
+
+
+def available():
+    """(ok, reason): is a CUDA device usable?"""
+    why = C.create_string_buffer(512)
+    ok = lib().ssb_available(why, 512)
+    return bool(ok), why.value.decode()
+
+
+def device_info(device=0):
+    d = _DeviceInfo()
+    _check(lib().ssb_get_device_info(device, C.byref(d)))
+    return dict(name=d.name.decode(), major=d.major, minor=d.minor, multiprocessors=d.multiprocessors,
+                global_memory=d.global_memory, shared_per_block_optin=d.shared_per_block_optin,
+                runtime_version=d.runtime_version, driver_version=d.driver_version)
+
+
+class Batch:
+    """Many instances of one compiled ship and sim on one GPU (the reference's cuda::Batch).
+
+    numerics: "portable" (double precision) or "portable32" (single-precision column partials).
+    rule: optional dict(pitch=, x=, y=, z=, wth=, settle=) for the extra sink/settle retire rule.
+    """
+
+    def __init__(self, ship_path, sim_path, count=1, numerics="portable32", traced_instances=0, dense_steps=400, sample_every=60.0,
+                 curve_every=0.0, t_max=5 * 3600.0, steps_per_launch=0, warps_per_block=0, blocks=0, device=0, rule=None):
+        if numerics not in NUMERICS:
+            raise SinksimError(-4, f"numerics {numerics!r} is not available on the GPU (portable or portable32)")
+        o = _Options()
+        lib().ssb_batch_options_init(C.byref(o))
+        o.count, o.numerics, o.traced_instances, o.dense_steps = count, NUMERICS[numerics], traced_instances, dense_steps
+        o.sample_every, o.curve_every, o.t_max, o.steps_per_launch = sample_every, curve_every, t_max, steps_per_launch
+        o.warps_per_block, o.blocks, o.device = warps_per_block, blocks, device
+        if rule:
+            o.rule_enabled = 1
+            o.rule_pitch, o.rule_x, o.rule_y, o.rule_z = rule["pitch"], rule["x"], rule["y"], rule["z"]
+            o.rule_wth, o.rule_settle = rule["wth"], rule["settle"]
+        h = C.c_void_p()
+        _check(lib().ssb_batch_create(_b(ship_path), _b(sim_path), C.byref(o), C.byref(h)))
+        self._h = h
+        self.count = count
+        self.numerics = numerics
+        n, c = C.c_int32(), C.c_int32()
+        _check(lib().ssb_batch_nodes(self._h, C.byref(n), C.byref(c)))
+        self.nodes, self.connections = n.value, c.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ssb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def launch_info(self):
+        li = _LaunchInfo()
+        _check(lib().ssb_batch_launch_info(self._h, C.byref(li)))
+        return dict(warps_per_block=li.warps_per_block, blocks=li.blocks, blocks_per_sm=li.blocks_per_sm, slot_bytes=li.slot_bytes)
+
+    # per-instance setup
+    def restore(self, instance, record):
+        rec = np.ascontiguousarray(record, dtype=np.float64)
+        if rec.size != 10 + 5 * self.nodes:
+            raise SinksimError(-1, f"a state record has {10 + 5 * self.nodes} values, got {rec.size}")
+        _check(lib().ssb_batch_restore(self._h, instance, _dptr(rec)))
+
+    def set_connection_enabled(self, instance, connection, enabled):
+        _check(lib().ssb_batch_set_connection_enabled(self._h, instance, connection, 1 if enabled else 0))
+
+    def set_connection_area(self, instance, connection, area):
+        _check(lib().ssb_batch_set_connection_area(self._h, instance, connection, float(area)))
+
+    def set_connection_activation(self, instance, connection, t_on):
+        _check(lib().ssb_batch_set_connection_activation(self._h, instance, connection, float(t_on)))
+
+    def apply_sweep(self, sweep_path):
+        _check(lib().ssb_batch_apply_sweep(self._h, _b(sweep_path)))
+
+    # running
+    def run(self):
+        s = C.c_double()
+        _check(lib().ssb_batch_run(self._h, C.byref(s)))
+        return s.value
+
+    def reset(self):
+        """Make the batch runnable again from its staged inputs."""
+        _check(lib().ssb_batch_reset(self._h))
+
+    def upload(self):
+        _check(lib().ssb_batch_upload(self._h))
+
+    def launch(self):
+        ms = C.c_float()
+        _check(lib().ssb_batch_launch(self._h, C.byref(ms)))
+        return ms.value
+
+    def download(self):
+        _check(lib().ssb_batch_download(self._h))
+
+    def transfer_bytes(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(lib().ssb_batch_transfer_bytes(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    # results
+    def total_steps(self):
+        s = C.c_int64()
+        _check(lib().ssb_batch_total_steps(self._h, C.byref(s)))
+        return s.value
+
+    def summary(self, instance):
+        s = _Summary()
+        _check(lib().ssb_batch_summary(self._h, instance, C.byref(s)))
+        return dict(foundered=bool(s.foundered), stop=STOP_REASONS.get(s.stop_reason, s.stop_reason), founder_t=s.founder_t,
+                    t_end=s.t_end, steps=s.steps, event_count=s.event_count, curve_count=s.curve_count, outputs=list(s.outputs))
+
+    def state(self, instance):
+        r = np.empty(10 + 5 * self.nodes)
+        _check(lib().ssb_batch_state(self._h, instance, _dptr(r)))
+        return r
+
+    def events(self, instance, cap=4096):
+        t = np.empty(cap)
+        ids = np.empty(cap, dtype=np.int32)
+        kinds = np.empty(cap, dtype=np.int32)
+        n = C.c_int32()
+        _check(lib().ssb_batch_events(self._h, instance, _dptr(t), ids.ctypes.data_as(C.POINTER(C.c_int32)),
+                                      kinds.ctypes.data_as(C.POINTER(C.c_int32)), cap, C.byref(n)))
+        k = min(n.value, cap)
+        return [(float(t[i]), int(ids[i]), int(kinds[i])) for i in range(k)]
+
+    def curve(self, instance, cap=None):
+        cap = cap or self.summary(instance)["curve_count"]
+        out = np.empty((max(cap, 1), 7))
+        n = C.c_int32()
+        _check(lib().ssb_batch_curve(self._h, instance, _dptr(out), cap, C.byref(n)))
+        return out[:min(n.value, cap)].copy()
+
+    def final_readouts(self, instance):
+        r = np.empty(7)
+        _check(lib().ssb_batch_final_readouts(self._h, instance, _dptr(r)))
+        return r
+
+    def save_trace(self, instance, path):
+        _check(lib().ssb_batch_save_trace(self._h, instance, _b(path)))
+
+    def save_results(self, path, sweep_path=None):
+        _check(lib().ssb_batch_save_results(self._h, _b(sweep_path), _b(path)))
+
+
+def run_sweep(ship_path, sim_path, sweep_path, numerics="portable32", results_path=None):
+    """sinksim_cuda_run --sweep in one call; returns (aggregate steps, wall seconds)."""
+    steps, secs = C.c_int64(), C.c_double()
+    _check(lib().ssb_run_sweep(_b(ship_path), _b(sim_path), _b(sweep_path), numerics.encode(), _b(results_path), C.byref(steps), C.byref(secs)))
+    return steps.value, secs.value
+
+
+def compare_results(a_path, b_path):
+    """Exact value-for-value comparison of two batch-results files; returns (compared, differing, first difference)."""
+    comp, diff = C.c_uint64(), C.c_uint64()
+    first = C.create_string_buffer(1024)
+    _check(lib().ssb_compare_results(_b(a_path), _b(b_path), C.byref(comp), C.byref(diff), first, 1024))
+    return comp.value, diff.value, first.value.decode()
+
+
+_OPS = {"sin": 0, "cos": 1, "pow": 2, "scalbn": 3}
+
+
+def portable_math(op, x, y=None, device=True):
+    """The engine's portable sin/cos/pow/scalbn on arrays, evaluated on the GPU (device=True) or the host."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    yy = None if y is None else np.ascontiguousarray(np.broadcast_to(np.asarray(y, dtype=np.float64), x.shape))
+    out = np.empty_like(x)
+    f = lib().ssb_portable_math_device if device else lib().ssb_portable_math_host
+    _check(f(_OPS[op], _dptr(x), None if yy is None else _dptr(yy), _dptr(out), x.size))
+    return out

@@ -1,0 +1,621 @@
+#include "batch.h"
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <stdexcept>
+
+#include <cuda_runtime.h>
+
+#include "batch_kernel.h"
+
+namespace ssb {
+
+namespace {
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + what + ": " + cudaGetErrorString(e));
+}
+
+// A device array that owns its allocation.
+template <class T>
+class DevBuf {
+ public:
+  DevBuf() = default;
+  ~DevBuf() { release(); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  void alloc(std::size_t n) {
+    if (p_ && n == n_) return;  // same size: keep the allocation (a re-run reuses every buffer)
+    release();
+    n_ = n;
+    if (n) check(cudaMalloc(reinterpret_cast<void**>(&p_), n * sizeof(T)), "cudaMalloc");
+  }
+  void upload(const std::vector<T>& v, cudaStream_t s) {
+    if (v.size() != n_) alloc(v.size());
+    if (n_) check(cudaMemcpyAsync(p_, v.data(), n_ * sizeof(T), cudaMemcpyHostToDevice, s), "copy to device");
+  }
+  void download(std::vector<T>& v, cudaStream_t s) const {
+    v.resize(n_);
+    if (n_) check(cudaMemcpyAsync(v.data(), p_, n_ * sizeof(T), cudaMemcpyDeviceToHost, s), "copy to host");
+  }
+  T* get() const { return p_; }
+  std::size_t size() const { return n_; }
+  std::size_t bytes() const { return n_ * sizeof(T); }
+
+ private:
+  T* p_ = nullptr;
+  std::size_t n_ = 0;
+  void release() {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = 0;
+  }
+};
+
+template <class T>
+std::vector<T> repeat(const std::vector<T>& v, std::size_t times) {
+  std::vector<T> out;
+  out.reserve(v.size() * times);
+  for (std::size_t i = 0; i < times; ++i) out.insert(out.end(), v.begin(), v.end());
+  return out;
+}
+
+std::uint32_t take(std::uint32_t& off, std::size_t bytes) {
+  const std::uint32_t at = off;
+  off = static_cast<std::uint32_t>((off + bytes + 15) & ~static_cast<std::size_t>(15));
+  return at;
+}
+
+}  // namespace
+
+bool cuda_available(std::string* why) {
+  int n = 0;
+  const cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    if (why) *why = cudaGetErrorString(e);
+    return false;
+  }
+  if (n == 0) {
+    if (why) *why = "no CUDA device";
+    return false;
+  }
+  return true;
+}
+
+DeviceInfo device_info(int device) {
+  DeviceInfo d;
+  cudaDeviceProp p{};
+  check(cudaGetDeviceProperties(&p, device), "cudaGetDeviceProperties");
+  d.name = p.name;
+  d.major = p.major; d.minor = p.minor; d.multiprocessors = p.multiProcessorCount;
+  d.globalMemory = p.totalGlobalMem; d.sharedPerBlockOptIn = p.sharedMemPerBlockOptin; d.sharedPerSM = p.sharedMemPerMultiprocessor;
+  cudaRuntimeGetVersion(&d.runtimeVersion);
+  cudaDriverGetVersion(&d.driverVersion);
+  return d;
+}
+
+struct Batch::Impl {
+  std::shared_ptr<const CompiledShip> ship;
+  CompiledSim sim;
+  Incidence inc;
+  MonitorLists mons;
+  DeviceInfo info;
+  std::int32_t NN = 0, NC = 0, NG = 0, nmon = 0, nmark = 0, evCap = 0, maxGroup = 0, recSize = 0, maxSamples = 0, curveMax = 0;
+  SlotLayout layout{};
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  // model
+  DevBuf<double> colX, colY, colA, colLo, colHi, segX, segY, segAr, segLo, segHi, mu, vmax, amin, aov;
+  DevBuf<std::int32_t> segStart, segCount, gStart, gCount, gNodes, ca, cb, skip, incStart, incCount, incConn, sea, monStart, monCount, monConn;
+  DevBuf<std::uint8_t> gMode, law, incSide, mkWhen;
+  DevBuf<double> gpx, gpy, gpz, kx, ky, kz, coef, mkx, mky, mkz;
+  DevModel dm{};
+
+  // per instance (device)
+  DevBuf<std::uint8_t> en;
+  DevBuf<double> area, tOn, st, out, vol, level, cx, cy, cz, evT, overT, markT, founderT, curveRec, nextCurve, finalRec, denseRec,
+      sampleRec, nextSample;
+  DevBuf<std::int32_t> evId, evKind, evCount, foundered, stop, curveCount, denseCount, sampleCount, queue, error;
+  DevBuf<long long> steps;
+
+  // host staging
+  std::vector<std::uint8_t> hEn;
+  std::vector<double> hArea, hTOn, hSt, hVol, hLevel, hCx, hCy, hCz;
+  // host results
+  struct {
+    std::vector<double> st, out, vol, level, cx, cy, cz, evT, founderT, curveRec, finalRec, denseRec, sampleRec;
+    std::vector<std::int32_t> evId, evKind, evCount, foundered, stop, curveCount, denseCount, sampleCount;
+    std::vector<long long> steps;
+  } r;
+  bool uploaded = false, launched = false, downloaded = false;
+
+  DevBatch devBatch(const BatchOptions& opt, long long maxSteps, int firstLaunch) {
+    DevBatch b{};
+    b.count = opt.count;
+    b.en = en.get(); b.area = area.get(); b.tOn = tOn.get();
+    b.st = st.get(); b.out = out.get();
+    b.vol = vol.get(); b.level = level.get(); b.cx = cx.get(); b.cy = cy.get(); b.cz = cz.get();
+    b.evT = evT.get(); b.evId = evId.get(); b.evKind = evKind.get(); b.evCount = evCount.get();
+    b.overT = overT.get(); b.markT = markT.get(); b.foundered = foundered.get(); b.founderT = founderT.get();
+    b.steps = steps.get(); b.stop = stop.get();
+    b.curveEvery = opt.curveEvery; b.curveMax = curveMax;
+    b.curveRec = curveRec.get(); b.curveCount = curveCount.get(); b.nextCurve = nextCurve.get();
+    b.finalRec = finalRec.get();
+    b.traced = opt.tracedInstances; b.denseSteps = opt.denseSteps; b.maxSamples = maxSamples; b.recSize = recSize;
+    b.sampleEvery = opt.sampleEvery;
+    b.denseRec = denseRec.get(); b.sampleRec = sampleRec.get();
+    b.denseCount = denseCount.get(); b.sampleCount = sampleCount.get(); b.nextSample = nextSample.get();
+    b.tMax = opt.tMax;
+    b.maxSteps = maxSteps;
+    b.firstLaunch = firstLaunch;
+    b.rule = opt.rule;
+    b.queue = queue.get();
+    b.error = error.get();
+    return b;
+  }
+};
+
+Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, const BatchOptions& opt) : I_(new Impl), opt_(opt) {
+  Impl& I = *I_;
+  if (!ship) throw std::invalid_argument("Batch: null ship");
+  if (opt_.count < 1) throw std::invalid_argument("Batch: count must be at least 1");
+  if (!(opt_.tMax > 0)) throw std::invalid_argument("Batch: tMax must be positive");
+  if (opt_.tracedInstances > opt_.count) opt_.tracedInstances = opt_.count;
+  if (opt_.tracedInstances < 0) opt_.tracedInstances = 0;
+  if (opt_.tracedInstances > 0 && !(opt_.sampleEvery > 0)) throw std::invalid_argument("Batch: sampleEvery must be positive");
+  std::string why;
+  if (!cuda_available(&why)) throw std::runtime_error("Batch: " + why);
+  check(cudaSetDevice(opt_.device), "cudaSetDevice");
+  I.ship = std::move(ship);
+  I.sim = sim;
+  check_pairing(*I.ship, I.sim);
+  I.inc = build_incidence(I.sim);
+  I.mons = build_monitor_lists(I.sim);
+  I.info = device_info(opt_.device);
+  I.NN = I.ship->nodes(); I.NC = I.sim.connections(); I.NG = I.sim.groups();
+  I.nmon = I.sim.monitors(); I.nmark = I.sim.marks(); I.evCap = I.nmon + I.nmark + 1; I.maxGroup = I.sim.maxGroupSize();
+  I.recSize = 10 + 5 * I.NN;
+  I.maxSamples = opt_.tracedInstances > 0 ? static_cast<std::int32_t>(std::floor(opt_.tMax / opt_.sampleEvery)) + 2 : 0;
+  I.curveMax = opt_.curveEvery > 0 ? static_cast<std::int32_t>(std::floor(opt_.tMax / opt_.curveEvery)) + 2 : 0;
+
+  // shared-memory slot of one simulation
+  SlotLayout& L = I.layout;
+  std::uint32_t off = 0;
+  const std::size_t nb = sizeof(double) * static_cast<std::size_t>(I.NN);
+  L.vol = take(off, nb); L.level = take(off, nb); L.cx = take(off, nb); L.cy = take(off, nb); L.cz = take(off, nb);
+  L.area = take(off, nb); L.zmax = take(off, nb); L.hEff = take(off, nb); L.aEff = take(off, nb); L.acc = take(off, nb);
+  L.deg = take(off, sizeof(std::int32_t) * static_cast<std::size_t>(I.NN));
+  L.dV = take(off, sizeof(double) * static_cast<std::size_t>(std::max(I.NC, 1)));
+  L.q = take(off, sizeof(double) * static_cast<std::size_t>(std::max(I.NC, 1)));
+  L.tmp = take(off, 6 * nb);
+  L.passes = take(off, 7 * sizeof(double) * static_cast<std::size_t>(I.maxGroup));
+  L.merged = take(off, static_cast<std::size_t>(std::max(I.NG, 1)));
+  L.bytes = off;
+
+  // launch shape: warps (simulations) per block from the slot size and the batch size; a persistent grid
+  const std::size_t optin = I.info.sharedPerBlockOptIn;
+  const int maxBySmem = static_cast<int>(optin / L.bytes);
+  if (maxBySmem < 1)
+    throw std::runtime_error("Batch: one simulation needs " + std::to_string(L.bytes) + " bytes of shared memory, the device allows " + std::to_string(optin) + " per block");
+  int W = opt_.warpsPerBlock;
+  if (W <= 0) {
+    const int sms = I.info.multiprocessors;
+    W = static_cast<int>((opt_.count + sms - 1) / sms);
+    W = std::max(1, std::min(W, kMaxWarpsPerBlock));
+  }
+  W = std::min({W, maxBySmem, kMaxWarpsPerBlock});
+  cfg_.warpsPerBlock = W;
+  cfg_.slotBytes = L.bytes;
+  const std::size_t smem = static_cast<std::size_t>(W) * L.bytes;
+  check(configure_batch_kernel(opt_.mixedPrecision, smem), "cudaFuncSetAttribute");
+  int perSM = 0;
+  check(batch_kernel_occupancy(opt_.mixedPrecision, W, smem, &perSM), "occupancy");
+  if (perSM < 1) throw std::runtime_error("Batch: the kernel cannot be resident with " + std::to_string(W) + " simulations per block");
+  cfg_.blocksPerSM = perSM;
+  const int needed = static_cast<int>((opt_.count + W - 1) / W);
+  cfg_.blocks = opt_.blocks > 0 ? opt_.blocks : std::min(needed, perSM * I.info.multiprocessors);
+
+  // model upload
+  check(cudaStreamCreateWithFlags(&I.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaEventCreate(&I.ev0), "cudaEventCreate");
+  check(cudaEventCreate(&I.ev1), "cudaEventCreate");
+  const CompiledShip& S = *I.ship;
+  const CompiledSim& M = I.sim;
+  cudaStream_t s = I.stream;
+  I.colX.upload(S.x, s); I.colY.upload(S.y, s); I.colA.upload(S.dxdy, s); I.colLo.upload(S.zlo, s); I.colHi.upload(S.zhi, s);
+  {
+    const std::size_t ns = S.segCol.size();
+    std::vector<double> sx(ns), sy(ns), sa(ns);
+    for (std::size_t j = 0; j < ns; ++j) {
+      const auto c = static_cast<std::size_t>(S.segCol[j]);
+      sx[j] = S.x[c]; sy[j] = S.y[c]; sa[j] = S.dxdy[c];
+    }
+    I.segX.upload(sx, s); I.segY.upload(sy, s); I.segAr.upload(sa, s);
+    check(cudaStreamSynchronize(s), "stream sync");
+  }
+  I.segLo.upload(S.segA, s); I.segHi.upload(S.segE, s);
+  I.mu.upload(S.mu, s); I.vmax.upload(S.vmax, s); I.amin.upload(S.amin, s); I.aov.upload(S.aov, s);
+  I.segStart.upload(S.segStart, s); I.segCount.upload(S.segCount, s);
+  I.gStart.upload(M.gNodeStart, s); I.gCount.upload(M.gNodeCount, s); I.gNodes.upload(M.gNodes, s); I.gMode.upload(M.gMode, s);
+  I.gpx.upload(M.gpx, s); I.gpy.upload(M.gpy, s); I.gpz.upload(M.gpz, s);
+  I.ca.upload(M.ca, s); I.cb.upload(M.cb, s); I.skip.upload(M.cSkipGroup, s); I.law.upload(M.cLaw, s);
+  I.kx.upload(M.cx, s); I.ky.upload(M.cy, s); I.kz.upload(M.cz, s); I.coef.upload(M.cCoef, s);
+  I.incStart.upload(I.inc.start, s); I.incCount.upload(I.inc.count, s); I.incConn.upload(I.inc.conn, s); I.incSide.upload(I.inc.side, s);
+  I.sea.upload(I.inc.sea.empty() ? std::vector<std::int32_t>{0} : I.inc.sea, s);
+  I.monStart.upload(I.mons.start.empty() ? std::vector<std::int32_t>{0} : I.mons.start, s);
+  I.monCount.upload(I.mons.count.empty() ? std::vector<std::int32_t>{0} : I.mons.count, s);
+  I.monConn.upload(I.mons.conn.empty() ? std::vector<std::int32_t>{0} : I.mons.conn, s);
+  I.mkx.upload(M.mkx.empty() ? std::vector<double>{0} : M.mkx, s);
+  I.mky.upload(M.mky.empty() ? std::vector<double>{0} : M.mky, s);
+  I.mkz.upload(M.mkz.empty() ? std::vector<double>{0} : M.mkz, s);
+  I.mkWhen.upload(M.mkWhen.empty() ? std::vector<std::uint8_t>{0} : M.mkWhen, s);
+  check(cudaStreamSynchronize(s), "model upload");
+
+  DevModel& d = I.dm;
+  d.ncol = S.columns();
+  d.colX = I.colX.get(); d.colY = I.colY.get(); d.colA = I.colA.get(); d.colLo = I.colLo.get(); d.colHi = I.colHi.get();
+  d.nseg = S.segments();
+  d.segX = I.segX.get(); d.segY = I.segY.get(); d.segAr = I.segAr.get(); d.segLo = I.segLo.get(); d.segHi = I.segHi.get();
+  d.nn = I.NN;
+  d.mu = I.mu.get(); d.vmax = I.vmax.get(); d.amin = I.amin.get(); d.aov = I.aov.get();
+  d.segStart = I.segStart.get(); d.segCount = I.segCount.get();
+  d.ng = I.NG;
+  d.gStart = I.gStart.get(); d.gCount = I.gCount.get(); d.gNodes = I.gNodes.get(); d.gMode = I.gMode.get();
+  d.gpx = I.gpx.get(); d.gpy = I.gpy.get(); d.gpz = I.gpz.get(); d.gMargin = M.gMargin; d.maxGroup = I.maxGroup;
+  d.nc = I.NC;
+  d.ca = I.ca.get(); d.cb = I.cb.get(); d.skip = I.skip.get(); d.law = I.law.get();
+  d.kx = I.kx.get(); d.ky = I.ky.get(); d.kz = I.kz.get(); d.coef = I.coef.get();
+  d.incStart = I.incStart.get(); d.incCount = I.incCount.get(); d.incConn = I.incConn.get(); d.incSide = I.incSide.get();
+  d.nsea = static_cast<std::int32_t>(I.inc.sea.size()); d.sea = I.sea.get();
+  d.nmon = I.nmon; d.monThreshold = M.monitorThreshold;
+  d.monStart = I.monStart.get(); d.monCount = I.monCount.get(); d.monConn = I.monConn.get();
+  d.nmark = I.nmark; d.mkx = I.mkx.get(); d.mky = I.mky.get(); d.mkz = I.mkz.get(); d.mkWhen = I.mkWhen.get();
+  d.hullTopBelow = M.hullTopBelow; d.pitchAbsAbove = M.pitchAbsAbove; d.buoyancyBelow = M.buoyancyBelow; d.minT = M.minT;
+  d.rho = M.rho; d.g = M.g; d.sq2g = std::sqrt(2 * M.g); d.dt = M.dt;
+  d.ms = M.body[0]; d.g0x = M.body[2]; d.g0y = M.body[3]; d.g0z = M.body[4]; d.XO = M.body[5]; d.YO = M.body[6];
+  d.mh0 = M.body[7]; d.Ith0 = M.body[8]; d.Iph0 = M.body[9]; d.cDz = M.body[10]; d.cDth = M.body[11]; d.cDph = M.body[12];
+  d.qz = M.body[13]; d.qth = M.body[14]; d.qph = M.body[15];
+  d.xFP = M.xFP; d.xAP = M.xAP;
+  d.evCap = I.evCap;
+
+  // per-instance staging: the compiled connection table and initial state in every instance
+  const auto count = static_cast<std::size_t>(opt_.count);
+  I.hEn = repeat(M.cEn, count); I.hArea = repeat(M.cArea, count); I.hTOn = repeat(M.cTOn, count);
+  I.hSt.resize(count * 8);
+  for (std::size_t i = 0; i < count; ++i) {
+    double* p = &I.hSt[i * 8];
+    p[0] = M.t0; p[1] = M.zO0; p[2] = M.pitch0; p[3] = M.roll0; p[4] = M.vz0; p[5] = M.wth0; p[6] = M.wph0; p[7] = 0;
+  }
+  I.hVol = repeat(M.vol0, count); I.hLevel = repeat(M.level0, count);
+  I.hCx = repeat(M.cx0, count); I.hCy = repeat(M.cy0, count); I.hCz = repeat(M.cz0, count);
+}
+
+Batch::~Batch() {
+  if (I_) {
+    if (I_->stream) cudaStreamSynchronize(I_->stream);
+    if (I_->ev0) cudaEventDestroy(I_->ev0);
+    if (I_->ev1) cudaEventDestroy(I_->ev1);
+    if (I_->stream) cudaStreamDestroy(I_->stream);
+  }
+}
+
+std::int32_t Batch::nodes() const { return I_->NN; }
+std::int32_t Batch::connections() const { return I_->NC; }
+std::size_t Batch::slot_bytes() const { return I_->layout.bytes; }
+
+static void check_inst(const BatchOptions& o, std::int32_t inst) {
+  if (inst < 0 || inst >= o.count) throw std::out_of_range("Batch: instance " + std::to_string(inst) + " out of range");
+}
+
+void Batch::restore(std::int32_t inst, const double* rec) {
+  Impl& I = *I_;
+  if (I.uploaded) throw std::logic_error("Batch: restore after run");
+  check_inst(opt_, inst);
+  const auto i = static_cast<std::size_t>(inst);
+  const auto N = static_cast<std::size_t>(I.NN);
+  for (int k = 0; k < 7; ++k) I.hSt[i * 8 + static_cast<std::size_t>(k)] = rec[k];
+  I.hSt[i * 8 + 7] = 0;
+  for (std::size_t n = 0; n < N; ++n) {
+    I.hVol[i * N + n] = rec[10 + n];
+    I.hLevel[i * N + n] = rec[10 + N + n];
+    I.hCx[i * N + n] = rec[10 + 2 * N + n];
+    I.hCy[i * N + n] = rec[10 + 3 * N + n];
+    I.hCz[i * N + n] = rec[10 + 4 * N + n];
+  }
+}
+
+void Batch::set_connection_enabled(std::int32_t inst, std::int32_t c, bool en) {
+  if (I_->uploaded) throw std::logic_error("Batch: set after run");
+  check_inst(opt_, inst);
+  if (c < 0 || c >= I_->NC) throw std::out_of_range("Batch: connection " + std::to_string(c));
+  I_->hEn[static_cast<std::size_t>(inst) * I_->NC + static_cast<std::size_t>(c)] = en ? 1 : 0;
+}
+
+void Batch::set_connection_area(std::int32_t inst, std::int32_t c, double area) {
+  if (I_->uploaded) throw std::logic_error("Batch: set after run");
+  check_inst(opt_, inst);
+  if (c < 0 || c >= I_->NC) throw std::out_of_range("Batch: connection " + std::to_string(c));
+  I_->hArea[static_cast<std::size_t>(inst) * I_->NC + static_cast<std::size_t>(c)] = area;
+}
+
+void Batch::set_connection_activation(std::int32_t inst, std::int32_t c, double tOn) {
+  if (I_->uploaded) throw std::logic_error("Batch: set after run");
+  check_inst(opt_, inst);
+  if (c < 0 || c >= I_->NC) throw std::out_of_range("Batch: connection " + std::to_string(c));
+  I_->hTOn[static_cast<std::size_t>(inst) * I_->NC + static_cast<std::size_t>(c)] = tOn;
+}
+
+void Batch::apply_sweep(const Sweep& sw) {
+  Impl& I = *I_;
+  if (I.uploaded) throw std::logic_error("Batch: set after run");
+  if (static_cast<std::int32_t>(sw.instances.size()) != opt_.count) throw std::invalid_argument("Batch: sweep instance count differs from the batch count");
+  for (std::int32_t i = 0; i < opt_.count; ++i) {
+    const std::size_t o = static_cast<std::size_t>(i) * I.NC;
+    apply_instance(sw.instances[static_cast<std::size_t>(i)], I.sim, I.hEn.data() + o, I.hArea.data() + o, I.hTOn.data() + o);
+  }
+}
+
+void Batch::upload() {
+  Impl& I = *I_;
+  if (I.uploaded) throw std::logic_error("Batch: run twice");
+  I.uploaded = true;
+  check(cudaSetDevice(opt_.device), "cudaSetDevice");
+  cudaStream_t s = I.stream;
+  const auto count = static_cast<std::size_t>(opt_.count);
+  I.en.upload(I.hEn, s); I.area.upload(I.hArea, s); I.tOn.upload(I.hTOn, s);
+  I.st.upload(I.hSt, s);
+  I.vol.upload(I.hVol, s); I.level.upload(I.hLevel, s); I.cx.upload(I.hCx, s); I.cy.upload(I.hCy, s); I.cz.upload(I.hCz, s);
+  // outputs and bookkeeping start at zero / -1 on the device
+  I.out.alloc(count * 7); check(cudaMemsetAsync(I.out.get(), 0, I.out.bytes(), s), "memset");
+  I.evT.alloc(count * static_cast<std::size_t>(I.evCap)); I.evId.alloc(count * static_cast<std::size_t>(I.evCap));
+  I.evKind.alloc(count * static_cast<std::size_t>(I.evCap));
+  I.evCount.alloc(count); check(cudaMemsetAsync(I.evCount.get(), 0, I.evCount.bytes(), s), "memset");
+  I.overT.upload(std::vector<double>(std::max<std::size_t>(count * static_cast<std::size_t>(I.nmon), 1), -1), s);
+  I.markT.upload(std::vector<double>(std::max<std::size_t>(count * static_cast<std::size_t>(I.nmark), 1), -1), s);
+  I.foundered.alloc(count); check(cudaMemsetAsync(I.foundered.get(), 0, I.foundered.bytes(), s), "memset");
+  I.founderT.upload(std::vector<double>(count, -1), s);
+  I.steps.alloc(count); check(cudaMemsetAsync(I.steps.get(), 0, I.steps.bytes(), s), "memset");
+  I.stop.alloc(count); check(cudaMemsetAsync(I.stop.get(), 0, I.stop.bytes(), s), "memset");
+  I.finalRec.alloc(count * 7);
+  const auto traced = static_cast<std::size_t>(opt_.tracedInstances);
+  const auto rec = static_cast<std::size_t>(I.recSize);
+  I.denseRec.alloc(std::max<std::size_t>(traced * static_cast<std::size_t>(opt_.denseSteps + 1) * rec, 1));
+  I.sampleRec.alloc(std::max<std::size_t>(traced * static_cast<std::size_t>(I.maxSamples) * rec, 1));
+  I.denseCount.alloc(std::max<std::size_t>(traced, 1)); check(cudaMemsetAsync(I.denseCount.get(), 0, I.denseCount.bytes(), s), "memset");
+  I.sampleCount.alloc(std::max<std::size_t>(traced, 1)); check(cudaMemsetAsync(I.sampleCount.get(), 0, I.sampleCount.bytes(), s), "memset");
+  I.nextSample.upload(std::vector<double>(std::max<std::size_t>(traced, 1), opt_.sampleEvery), s);
+  I.curveRec.alloc(std::max<std::size_t>(count * static_cast<std::size_t>(I.curveMax) * 7, 1));
+  I.curveCount.alloc(count); check(cudaMemsetAsync(I.curveCount.get(), 0, I.curveCount.bytes(), s), "memset");
+  I.nextCurve.alloc(count); check(cudaMemsetAsync(I.nextCurve.get(), 0, I.nextCurve.bytes(), s), "memset");
+  I.queue.alloc(1);
+  I.error.alloc(1); check(cudaMemsetAsync(I.error.get(), 0, I.error.bytes(), s), "memset");
+}
+
+float Batch::launch() {
+  Impl& I = *I_;
+  if (!I.uploaded) throw std::logic_error("Batch: launch before upload");
+  if (I.launched) throw std::logic_error("Batch: launch twice");
+  I.launched = true;
+  check(cudaSetDevice(opt_.device), "cudaSetDevice");
+  cudaStream_t s = I.stream;
+  const long long maxSteps = opt_.stepsPerLaunch > 0 ? opt_.stepsPerLaunch : LLONG_MAX;
+  check(cudaEventRecord(I.ev0, s), "cudaEventRecord");
+  int first = 1;
+  for (;;) {
+    check(cudaMemsetAsync(I.queue.get(), 0, sizeof(std::int32_t), s), "memset");
+    check(launch_batch_kernel(opt_.mixedPrecision, I.dm, I.devBatch(opt_, maxSteps, first), I.layout, cfg_.blocks, cfg_.warpsPerBlock, s),
+          "kernel launch");
+    first = 0;
+    if (opt_.stepsPerLaunch <= 0) break;
+    std::vector<std::int32_t> stops;
+    I.stop.download(stops, s);
+    check(cudaStreamSynchronize(s), "kernel execution");
+    bool active = false;
+    for (const std::int32_t v : stops) if (v == kRunning) { active = true; break; }
+    if (!active) break;
+  }
+  check(cudaEventRecord(I.ev1, s), "cudaEventRecord");
+  check(cudaEventSynchronize(I.ev1), "kernel execution");
+  float ms = 0;
+  check(cudaEventElapsedTime(&ms, I.ev0, I.ev1), "cudaEventElapsedTime");
+  return ms;
+}
+
+void Batch::download() {
+  Impl& I = *I_;
+  if (!I.launched) throw std::logic_error("Batch: download before launch");
+  cudaStream_t s = I.stream;
+  auto& r = I.r;
+  I.st.download(r.st, s); I.out.download(r.out, s);
+  I.vol.download(r.vol, s); I.level.download(r.level, s); I.cx.download(r.cx, s); I.cy.download(r.cy, s); I.cz.download(r.cz, s);
+  I.evT.download(r.evT, s); I.evId.download(r.evId, s); I.evKind.download(r.evKind, s); I.evCount.download(r.evCount, s);
+  I.foundered.download(r.foundered, s); I.founderT.download(r.founderT, s); I.steps.download(r.steps, s); I.stop.download(r.stop, s);
+  I.finalRec.download(r.finalRec, s);
+  if (opt_.curveEvery > 0) { I.curveRec.download(r.curveRec, s); I.curveCount.download(r.curveCount, s); }
+  if (opt_.tracedInstances > 0) {
+    I.denseRec.download(r.denseRec, s); I.sampleRec.download(r.sampleRec, s);
+    I.denseCount.download(r.denseCount, s); I.sampleCount.download(r.sampleCount, s);
+  }
+  check(cudaStreamSynchronize(s), "copy to host");
+  I.downloaded = true;
+}
+
+void Batch::reset() {
+  Impl& I = *I_;
+  if (I.uploaded && !I.launched) throw std::logic_error("Batch: reset between upload and launch");
+  check(cudaStreamSynchronize(I.stream), "stream sync");
+  I.uploaded = false;
+  I.launched = false;
+}
+
+double Batch::run() {
+  const auto t0 = std::chrono::steady_clock::now();
+  upload();
+  launch();
+  download();
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+std::size_t Batch::upload_bytes() const {
+  const Impl& I = *I_;
+  return I.hEn.size() + sizeof(double) * (I.hArea.size() + I.hTOn.size() + I.hSt.size() + I.hVol.size() + I.hLevel.size() + I.hCx.size() +
+                                          I.hCy.size() + I.hCz.size());
+}
+
+std::size_t Batch::download_bytes() const {
+  const Impl& I = *I_;
+  std::size_t b = I.st.bytes() + I.out.bytes() + I.vol.bytes() + I.level.bytes() + I.cx.bytes() + I.cy.bytes() + I.cz.bytes() + I.evT.bytes() +
+                  I.evId.bytes() + I.evKind.bytes() + I.evCount.bytes() + I.foundered.bytes() + I.founderT.bytes() + I.steps.bytes() +
+                  I.stop.bytes() + I.finalRec.bytes();
+  if (opt_.curveEvery > 0) b += I.curveRec.bytes() + I.curveCount.bytes();
+  if (opt_.tracedInstances > 0) b += I.denseRec.bytes() + I.sampleRec.bytes() + I.denseCount.bytes() + I.sampleCount.bytes();
+  return b;
+}
+
+std::int64_t Batch::total_steps() const {
+  if (!I_->downloaded) throw std::logic_error("Batch: results before run");
+  std::int64_t t = 0;
+  for (const long long s : I_->r.steps) t += s;
+  return t;
+}
+
+Batch::Summary Batch::summary(std::int32_t inst) const {
+  const Impl& I = *I_;
+  if (!I.downloaded) throw std::logic_error("Batch: result before run");
+  check_inst(opt_, inst);
+  const auto i = static_cast<std::size_t>(inst);
+  Summary s{};
+  s.foundered = I.r.foundered[i] != 0;
+  s.founderT = I.r.founderT[i];
+  s.tEnd = I.r.st[i * 8];
+  s.steps = I.r.steps[i];
+  s.stop = I.r.stop[i];
+  for (int k = 0; k < 7; ++k) s.outputs[k] = I.r.out[i * 7 + static_cast<std::size_t>(k)];
+  return s;
+}
+
+void Batch::state(std::int32_t inst, double* rec) const {
+  const Impl& I = *I_;
+  if (!I.downloaded) throw std::logic_error("Batch: result before run");
+  check_inst(opt_, inst);
+  const auto i = static_cast<std::size_t>(inst);
+  const auto N = static_cast<std::size_t>(I.NN);
+  for (int k = 0; k < 7; ++k) rec[k] = I.r.st[i * 8 + static_cast<std::size_t>(k)];
+  rec[7] = I.r.out[i * 7]; rec[8] = I.r.out[i * 7 + 1]; rec[9] = I.r.out[i * 7 + 2];
+  for (std::size_t n = 0; n < N; ++n) {
+    rec[10 + n] = I.r.vol[i * N + n];
+    rec[10 + N + n] = I.r.level[i * N + n];
+    rec[10 + 2 * N + n] = I.r.cx[i * N + n];
+    rec[10 + 3 * N + n] = I.r.cy[i * N + n];
+    rec[10 + 4 * N + n] = I.r.cz[i * N + n];
+  }
+}
+
+std::vector<int> Batch::event_kinds(std::int32_t inst) const {
+  const Impl& I = *I_;
+  const auto i = static_cast<std::size_t>(inst);
+  std::vector<int> out;
+  for (std::int32_t k = 0; k < I.r.evCount[i]; ++k) out.push_back(I.r.evKind[i * static_cast<std::size_t>(I.evCap) + static_cast<std::size_t>(k)]);
+  return out;
+}
+
+std::vector<int> Batch::event_ids(std::int32_t inst) const {
+  const Impl& I = *I_;
+  const auto i = static_cast<std::size_t>(inst);
+  std::vector<int> out;
+  for (std::int32_t k = 0; k < I.r.evCount[i]; ++k) out.push_back(I.r.evId[i * static_cast<std::size_t>(I.evCap) + static_cast<std::size_t>(k)]);
+  return out;
+}
+
+const CompiledSim& Batch::sim() const { return I_->sim; }
+
+std::vector<EventRecord> Batch::events(std::int32_t inst) const {
+  const Impl& I = *I_;
+  if (!I.downloaded) throw std::logic_error("Batch: result before run");
+  check_inst(opt_, inst);
+  const auto i = static_cast<std::size_t>(inst);
+  std::vector<EventRecord> out;
+  for (std::int32_t k = 0; k < I.r.evCount[i]; ++k) {
+    const std::size_t j = i * static_cast<std::size_t>(I.evCap) + static_cast<std::size_t>(k);
+    const std::int32_t id = I.r.evId[j];
+    switch (I.r.evKind[j]) {
+      case 0: out.push_back(EventRecord{I.r.evT[j], I.sim.monitorId[static_cast<std::size_t>(id)], I.sim.monitorLabel[static_cast<std::size_t>(id)]}); break;
+      case 1: out.push_back(EventRecord{I.r.evT[j], I.sim.markId[static_cast<std::size_t>(id)], I.sim.markLabel[static_cast<std::size_t>(id)]}); break;
+      default: out.push_back(EventRecord{I.r.evT[j], "founder", "Foundered"}); break;
+    }
+  }
+  return out;
+}
+
+CurveRecord Batch::final_readouts(std::int32_t inst) const {
+  const Impl& I = *I_;
+  if (!I.downloaded) throw std::logic_error("Batch: result before run");
+  check_inst(opt_, inst);
+  const double* p = &I.r.finalRec[static_cast<std::size_t>(inst) * 7];
+  return CurveRecord{p[0], p[1], p[2], p[3], p[4], p[5], p[6]};
+}
+
+std::vector<CurveRecord> Batch::curve(std::int32_t inst) const {
+  const Impl& I = *I_;
+  if (!I.downloaded) throw std::logic_error("Batch: curve before run");
+  if (opt_.curveEvery <= 0) throw std::logic_error("Batch: curves were not recorded (curveEvery is 0)");
+  check_inst(opt_, inst);
+  const auto i = static_cast<std::size_t>(inst);
+  std::vector<CurveRecord> out;
+  for (std::int32_t k = 0; k < I.r.curveCount[i]; ++k) {
+    const double* p = &I.r.curveRec[(i * static_cast<std::size_t>(I.curveMax) + static_cast<std::size_t>(k)) * 7];
+    out.push_back(CurveRecord{p[0], p[1], p[2], p[3], p[4], p[5], p[6]});
+  }
+  out.push_back(final_readouts(inst));
+  return out;
+}
+
+std::string Batch::engine_name() const { return "sinksim-b200 CUDA engine on " + I_->info.name; }
+
+Trace Batch::trace(std::int32_t inst) const {
+  const Impl& I = *I_;
+  if (!I.downloaded) throw std::logic_error("Batch: trace before run");
+  if (inst < 0 || inst >= opt_.tracedInstances) throw std::out_of_range("Batch: instance was not traced");
+  const auto i = static_cast<std::size_t>(inst);
+  Trace tr;
+  tr.ship = I.ship->id; tr.sim = I.sim.id; tr.title = I.sim.title;
+  tr.producer = opt_.mixedPrecision ? "sinksim-b200 CUDA engine, numerics portable32" : "sinksim-b200 CUDA engine, numerics portable";
+  tr.engine = "sinksim-b200 0.1.0 on " + I.info.name;
+  tr.dt = I.sim.dt; tr.nodes = I.NN; tr.denseSteps = opt_.denseSteps; tr.sampleEvery = opt_.sampleEvery;
+  const Summary s = summary(inst);
+  tr.steps = s.steps; tr.tEnd = s.tEnd; tr.foundered = s.foundered; tr.founderT = s.founderT;
+  for (const EventRecord& e : events(inst)) tr.events.push_back(TraceEvent{e.t, e.id, e.label});
+  const auto rec = static_cast<std::size_t>(I.recSize);
+  const std::size_t db = i * static_cast<std::size_t>(opt_.denseSteps + 1) * rec, sb = i * static_cast<std::size_t>(I.maxSamples) * rec;
+  for (std::int32_t k = 0; k < I.r.denseCount[i]; ++k) tr.dense.push_record(&I.r.denseRec[db + static_cast<std::size_t>(k) * rec], I.NN);
+  for (std::int32_t k = 0; k < I.r.sampleCount[i]; ++k) tr.samples.push_record(&I.r.sampleRec[sb + static_cast<std::size_t>(k) * rec], I.NN);
+  return tr;
+}
+
+Results Batch::results(const Sweep* sw) const {
+  const Impl& I = *I_;
+  Results r;
+  r.ship = I.ship->id;
+  r.sim = I.sim.id;
+  r.numerics = opt_.mixedPrecision ? "portable32" : "portable";
+  r.engine = engine_name();
+  r.tMax = opt_.tMax;
+  r.every = opt_.curveEvery;
+  for (std::int32_t i = 0; i < opt_.count; ++i) {
+    InstanceResult in;
+    in.id = sw ? sw->instances[static_cast<std::size_t>(i)].id : "instance" + std::to_string(i);
+    const Summary s = summary(i);
+    in.foundered = s.foundered; in.founderT = s.founderT; in.tEnd = s.tEnd; in.steps = s.steps;
+    const CurveRecord f = final_readouts(i);
+    in.fTrim = f.trim; in.fList = f.list; in.fWater = f.water; in.fInflow = f.inflow; in.fDraftF = f.dF; in.fDraftA = f.dA;
+    in.events = events(i);
+    if (opt_.curveEvery > 0) in.curve = curve(i);
+    r.instances.push_back(std::move(in));
+  }
+  return r;
+}
+
+}  // namespace ssb

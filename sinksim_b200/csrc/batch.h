@@ -1,0 +1,108 @@
+// The batch engine: many instances of one compiled ship and sim on one GPU. The host-side counterpart of the
+// reference's cuda::Batch (engine/include/sinksim/cuda/batch.hpp:27-87): per-instance setters staged on the host,
+// run() to completion, then results, curves, final readouts and traces.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "device_model.h"
+#include "model.h"
+#include "sweep.h"
+
+namespace ssb {
+
+struct BatchOptions {
+  std::int32_t count = 1;
+  bool mixedPrecision = true;      // portable32 numerics; false: portable (double precision)
+  std::int32_t tracedInstances = 1;
+  std::int32_t denseSteps = 400;
+  double sampleEvery = 60;
+  double curveEvery = 0;           // s between readout-curve records (0: none)
+  double tMax = 5 * 3600;
+  std::int64_t stepsPerLaunch = 0; // 0: one launch runs every instance to its end; > 0: bounded launches
+  std::int32_t warpsPerBlock = 0;  // 0: chosen from the slot size and the batch size
+  std::int32_t blocks = 0;         // 0: persistent grid sized to the device
+  RetireRule rule{};
+  int device = 0;
+};
+
+struct DeviceInfo {
+  std::string name;
+  int major = 0, minor = 0, multiprocessors = 0;
+  std::size_t globalMemory = 0, sharedPerBlockOptIn = 0, sharedPerSM = 0;
+  int runtimeVersion = 0, driverVersion = 0;
+};
+
+bool cuda_available(std::string* why);
+DeviceInfo device_info(int device);
+
+struct LaunchConfig {
+  int warpsPerBlock = 0, blocks = 0, blocksPerSM = 0;
+  std::size_t slotBytes = 0;
+};
+
+class Batch {
+ public:
+  Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, const BatchOptions& opt);
+  ~Batch();
+  Batch(const Batch&) = delete;
+  Batch& operator=(const Batch&) = delete;
+
+  // Per-instance setup before run(): a state record (10 + 5 N values, the trace record layout) and connection fields.
+  void restore(std::int32_t inst, const double* record);
+  void set_connection_enabled(std::int32_t inst, std::int32_t c, bool en);
+  void set_connection_area(std::int32_t inst, std::int32_t c, double area);
+  void set_connection_activation(std::int32_t inst, std::int32_t c, double tOn);
+  void apply_sweep(const Sweep& sw);  // instance i takes sweep instance i
+
+  // run() = upload() + launch() + download(); returns the wall seconds of all three.
+  double run();
+  // Makes the batch runnable again from its staged inputs (the setters' values persist); the last results stay
+  // readable until the next download().
+  void reset();
+  void upload();
+  // Runs every instance to its end on the device; returns the device time in milliseconds (CUDA events on the
+  // launching stream).
+  float launch();
+  void download();
+
+  const BatchOptions& options() const { return opt_; }
+  const LaunchConfig& launch_config() const { return cfg_; }
+  std::int64_t total_steps() const;
+  std::size_t slot_bytes() const;
+  std::int32_t nodes() const;
+  std::int32_t connections() const;
+  // h2d and d2h bytes of one run() (the per-instance inputs and the results that download() reads back)
+  std::size_t upload_bytes() const;
+  std::size_t download_bytes() const;
+
+  struct Summary {
+    bool foundered;
+    double founderT, tEnd;
+    std::int64_t steps;
+    std::int32_t stop;
+    double outputs[7];  // inflow, Vb, hullTop, mw, bx, by, bz
+  };
+  Summary summary(std::int32_t inst) const;
+  void state(std::int32_t inst, double* record) const;
+  std::vector<EventRecord> events(std::int32_t inst) const;
+  std::vector<int> event_kinds(std::int32_t inst) const;
+  std::vector<int> event_ids(std::int32_t inst) const;  // monitor or mark index, -1 for the founder
+  const CompiledSim& sim() const;
+  std::vector<CurveRecord> curve(std::int32_t inst) const;  // the device records closed by the final readouts
+  CurveRecord final_readouts(std::int32_t inst) const;
+  Trace trace(std::int32_t inst) const;
+  Results results(const Sweep* sw) const;
+  std::string engine_name() const;
+
+ private:
+  struct Impl;
+  std::unique_ptr<Impl> I_;
+  BatchOptions opt_;
+  LaunchConfig cfg_;
+};
+
+}  // namespace ssb

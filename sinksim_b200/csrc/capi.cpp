@@ -1,0 +1,378 @@
+// The extern "C" boundary (include/sinksim_b200.h): exceptions become status codes and a thread-local message.
+#include "sinksim_b200.h"
+
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "batch.h"
+#include "model.h"
+#include "sweep.h"
+
+namespace ssb {
+void portable_math_host(int op, const double* x, const double* y, double* out, std::int64_t n);
+cudaError_t portable_math_device(int op, const double* x, const double* y, double* out, std::int64_t n);
+}  // namespace ssb
+
+struct ssb_batch {
+  std::shared_ptr<ssb::Batch> batch;
+  std::unique_ptr<ssb::Sweep> sweep;  // the sweep applied by ssb_batch_apply_sweep, for instance ids
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+struct Unsupported : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct NoDevice : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return SSB_OK;
+  } catch (const Unsupported& e) {
+    g_error = e.what();
+    return SSB_EUNSUPPORTED;
+  } catch (const NoDevice& e) {
+    g_error = e.what();
+    return SSB_ENODEVICE;
+  } catch (const std::invalid_argument& e) {
+    g_error = e.what();
+    return SSB_EINVAL;
+  } catch (const std::out_of_range& e) {
+    g_error = e.what();
+    return SSB_EINVAL;
+  } catch (const std::logic_error& e) {
+    g_error = e.what();
+    return SSB_ESTATE;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return SSB_ERUNTIME;
+  } catch (...) {
+    g_error = "unknown error";
+    return SSB_ERUNTIME;
+  }
+}
+
+void need(const void* p, const char* what) {
+  if (!p) throw std::invalid_argument(std::string(what) + " is NULL");
+}
+
+ssb::BatchOptions to_options(const ssb_batch_options& o) {
+  if (o.numerics != 0 && o.numerics != 1) throw Unsupported("numerics " + std::to_string(o.numerics) + " is not available on the GPU (0 portable, 1 portable32)");
+  ssb::BatchOptions b;
+  b.count = o.count;
+  b.mixedPrecision = o.numerics == 1;
+  b.tracedInstances = o.traced_instances;
+  b.denseSteps = o.dense_steps;
+  b.sampleEvery = o.sample_every;
+  b.curveEvery = o.curve_every;
+  b.tMax = o.t_max;
+  b.stepsPerLaunch = o.steps_per_launch;
+  b.warpsPerBlock = o.warps_per_block;
+  b.blocks = o.blocks;
+  b.device = o.device;
+  b.rule.enabled = o.rule_enabled;
+  b.rule.pitchLimit = o.rule_pitch;
+  b.rule.xDeck = o.rule_x; b.rule.yDeck = o.rule_y; b.rule.zDeck = o.rule_z;
+  b.rule.wthLimit = o.rule_wth;
+  b.rule.settleTime = o.rule_settle;
+  return b;
+}
+
+void need_device() {
+  std::string why;
+  if (!ssb::cuda_available(&why)) throw NoDevice("no usable CUDA device (" + why + ")");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ssb_last_error(void) { return g_error.c_str(); }
+const char* ssb_version(void) { return "sinksim-b200 0.1.0"; }
+
+int ssb_available(char* why, size_t cap) {
+  std::string w;
+  const bool ok = ssb::cuda_available(&w);
+  if (why && cap) {
+    std::strncpy(why, w.c_str(), cap - 1);
+    why[cap - 1] = 0;
+  }
+  return ok ? 1 : 0;
+}
+
+int ssb_get_device_info(int32_t device, ssb_device_info* out) {
+  return guard([&] {
+    need(out, "out");
+    need_device();
+    const ssb::DeviceInfo d = ssb::device_info(device);
+    std::memset(out, 0, sizeof *out);
+    std::strncpy(out->name, d.name.c_str(), sizeof out->name - 1);
+    out->major = d.major; out->minor = d.minor; out->multiprocessors = d.multiprocessors;
+    out->global_memory = d.globalMemory; out->shared_per_block_optin = d.sharedPerBlockOptIn;
+    out->runtime_version = d.runtimeVersion; out->driver_version = d.driverVersion;
+  });
+}
+
+void ssb_batch_options_init(ssb_batch_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->count = 1;
+  o->numerics = 1;
+  o->traced_instances = 1;
+  o->dense_steps = 400;
+  o->sample_every = 60;
+  o->curve_every = 0;
+  o->t_max = 5 * 3600;
+}
+
+int ssb_batch_create(const char* ship_path, const char* sim_path, const ssb_batch_options* opt, ssb_batch** out) {
+  return guard([&] {
+    need(ship_path, "ship_path"); need(sim_path, "sim_path"); need(opt, "opt"); need(out, "out");
+    *out = nullptr;
+    const ssb::BatchOptions bo = to_options(*opt);
+    need_device();
+    auto ship = ssb::load_ship(ship_path);
+    const ssb::CompiledSim sim = ssb::load_sim(sim_path);
+    ssb::check_pairing(*ship, sim);
+    auto h = std::make_unique<ssb_batch>();
+    h->batch = std::make_shared<ssb::Batch>(ship, sim, bo);
+    *out = h.release();
+  });
+}
+
+void ssb_batch_destroy(ssb_batch* b) { delete b; }
+
+int ssb_batch_nodes(const ssb_batch* b, int32_t* nodes, int32_t* connections) {
+  return guard([&] {
+    need(b, "batch");
+    if (nodes) *nodes = b->batch->nodes();
+    if (connections) *connections = b->batch->connections();
+  });
+}
+
+int ssb_batch_launch_info(const ssb_batch* b, ssb_launch_info* out) {
+  return guard([&] {
+    need(b, "batch"); need(out, "out");
+    const ssb::LaunchConfig& c = b->batch->launch_config();
+    out->warps_per_block = c.warpsPerBlock; out->blocks = c.blocks; out->blocks_per_sm = c.blocksPerSM; out->slot_bytes = c.slotBytes;
+  });
+}
+
+int ssb_batch_restore(ssb_batch* b, int32_t instance, const double* record) {
+  return guard([&] { need(b, "batch"); need(record, "record"); b->batch->restore(instance, record); });
+}
+
+int ssb_batch_set_connection_enabled(ssb_batch* b, int32_t instance, int32_t c, int32_t enabled) {
+  return guard([&] { need(b, "batch"); b->batch->set_connection_enabled(instance, c, enabled != 0); });
+}
+
+int ssb_batch_set_connection_area(ssb_batch* b, int32_t instance, int32_t c, double area) {
+  return guard([&] { need(b, "batch"); b->batch->set_connection_area(instance, c, area); });
+}
+
+int ssb_batch_set_connection_activation(ssb_batch* b, int32_t instance, int32_t c, double t_on) {
+  return guard([&] { need(b, "batch"); b->batch->set_connection_activation(instance, c, t_on); });
+}
+
+int ssb_batch_apply_sweep(ssb_batch* b, const char* sweep_path) {
+  return guard([&] {
+    need(b, "batch"); need(sweep_path, "sweep_path");
+    auto sw = std::make_unique<ssb::Sweep>(ssb::load_sweep(sweep_path, b->batch->sim()));
+    b->batch->apply_sweep(*sw);
+    b->sweep = std::move(sw);
+  });
+}
+
+int ssb_batch_run(ssb_batch* b, double* seconds) {
+  return guard([&] {
+    need(b, "batch");
+    const double s = b->batch->run();
+    if (seconds) *seconds = s;
+  });
+}
+
+int ssb_batch_reset(ssb_batch* b) {
+  return guard([&] { need(b, "batch"); b->batch->reset(); });
+}
+
+int ssb_batch_upload(ssb_batch* b) {
+  return guard([&] { need(b, "batch"); b->batch->upload(); });
+}
+
+int ssb_batch_launch(ssb_batch* b, float* device_ms) {
+  return guard([&] {
+    need(b, "batch");
+    const float ms = b->batch->launch();
+    if (device_ms) *device_ms = ms;
+  });
+}
+
+int ssb_batch_download(ssb_batch* b) {
+  return guard([&] { need(b, "batch"); b->batch->download(); });
+}
+
+int ssb_batch_transfer_bytes(const ssb_batch* b, uint64_t* h2d, uint64_t* d2h) {
+  return guard([&] {
+    need(b, "batch");
+    if (h2d) *h2d = b->batch->upload_bytes();
+    if (d2h) *d2h = b->batch->download_bytes();
+  });
+}
+
+int ssb_batch_total_steps(const ssb_batch* b, int64_t* steps) {
+  return guard([&] { need(b, "batch"); need(steps, "steps"); *steps = b->batch->total_steps(); });
+}
+
+int ssb_batch_summary(const ssb_batch* b, int32_t instance, ssb_instance_summary* out) {
+  return guard([&] {
+    need(b, "batch"); need(out, "out");
+    const ssb::Batch::Summary s = b->batch->summary(instance);
+    out->foundered = s.foundered ? 1 : 0;
+    out->stop_reason = s.stop;
+    out->founder_t = s.founderT;
+    out->t_end = s.tEnd;
+    out->steps = s.steps;
+    out->event_count = static_cast<int32_t>(b->batch->events(instance).size());
+    out->curve_count = b->batch->options().curveEvery > 0 ? static_cast<int32_t>(b->batch->curve(instance).size()) : 0;
+    for (int k = 0; k < 7; ++k) out->outputs[k] = s.outputs[k];
+  });
+}
+
+int ssb_batch_state(const ssb_batch* b, int32_t instance, double* record) {
+  return guard([&] { need(b, "batch"); need(record, "record"); b->batch->state(instance, record); });
+}
+
+int ssb_batch_events(const ssb_batch* b, int32_t instance, double* t, int32_t* id, int32_t* kind, int32_t cap, int32_t* count) {
+  return guard([&] {
+    need(b, "batch");
+    const auto ev = b->batch->events(instance);
+    const auto kinds = b->batch->event_kinds(instance);
+    const auto ids = b->batch->event_ids(instance);
+    for (int32_t k = 0; k < static_cast<int32_t>(ev.size()) && k < cap; ++k) {
+      const auto i = static_cast<std::size_t>(k);
+      if (t) t[k] = ev[i].t;
+      if (kind) kind[k] = kinds[i];
+      if (id) id[k] = kinds[i] == 2 ? -1 : ids[i];
+    }
+    if (count) *count = static_cast<int32_t>(ev.size());
+  });
+}
+
+int ssb_batch_curve(const ssb_batch* b, int32_t instance, double* records, int32_t cap, int32_t* count) {
+  return guard([&] {
+    need(b, "batch");
+    const auto c = b->batch->curve(instance);
+    for (int32_t k = 0; k < static_cast<int32_t>(c.size()) && k < cap; ++k) {
+      const ssb::CurveRecord& r = c[static_cast<std::size_t>(k)];
+      double* p = records + 7 * k;
+      p[0] = r.t; p[1] = r.trim; p[2] = r.list; p[3] = r.water; p[4] = r.inflow; p[5] = r.dF; p[6] = r.dA;
+    }
+    if (count) *count = static_cast<int32_t>(c.size());
+  });
+}
+
+int ssb_batch_final_readouts(const ssb_batch* b, int32_t instance, double* r7) {
+  return guard([&] {
+    need(b, "batch"); need(r7, "record7");
+    const ssb::CurveRecord r = b->batch->final_readouts(instance);
+    r7[0] = r.t; r7[1] = r.trim; r7[2] = r.list; r7[3] = r.water; r7[4] = r.inflow; r7[5] = r.dF; r7[6] = r.dA;
+  });
+}
+
+int ssb_batch_save_trace(const ssb_batch* b, int32_t instance, const char* path) {
+  return guard([&] { need(b, "batch"); need(path, "path"); ssb::save_trace(b->batch->trace(instance), path); });
+}
+
+int ssb_batch_save_results(const ssb_batch* b, const char* sweep_path, const char* results_path) {
+  return guard([&] {
+    need(b, "batch"); need(results_path, "results_path");
+    std::unique_ptr<ssb::Sweep> own;
+    const ssb::Sweep* sw = b->sweep.get();
+    if (sweep_path) {
+      own = std::make_unique<ssb::Sweep>(ssb::load_sweep(sweep_path, b->batch->sim()));
+      sw = own.get();
+    }
+    if (sw && static_cast<std::int32_t>(sw->instances.size()) != b->batch->options().count)
+      throw std::invalid_argument("the sweep's instance count differs from the batch's");
+    ssb::Results r = b->batch->results(sw);
+    if (sw) { r.tMax = sw->tMax; r.every = sw->every; }
+    ssb::save_results(r, results_path);
+  });
+}
+
+int ssb_run_sweep(const char* ship_path, const char* sim_path, const char* sweep_path, const char* numerics, const char* results_path,
+                  int64_t* steps, double* seconds) {
+  return guard([&] {
+    need(ship_path, "ship_path"); need(sim_path, "sim_path"); need(sweep_path, "sweep_path"); need(numerics, "numerics");
+    const std::string nm = numerics;
+    if (nm != "portable" && nm != "portable32")
+      throw Unsupported("numerics " + nm + " is not available on the GPU engine (use portable or portable32)");
+    need_device();
+    auto ship = ssb::load_ship(ship_path);
+    const ssb::CompiledSim sim = ssb::load_sim(sim_path);
+    ssb::check_pairing(*ship, sim);
+    const ssb::Sweep sw = ssb::load_sweep(sweep_path, sim);
+    if (sw.stopWhenStable) throw Unsupported("stopWhenStable is not supported on the GPU; run the sweep with sinksim_sweep");
+    if (sw.instances.empty()) throw std::invalid_argument("the sweep has no instances");
+    ssb::BatchOptions opt;
+    opt.count = static_cast<std::int32_t>(sw.instances.size());
+    opt.mixedPrecision = nm == "portable32";
+    opt.tracedInstances = 0;
+    opt.tMax = sw.tMax;
+    opt.curveEvery = sw.every;
+    ssb::Batch batch(ship, sim, opt);
+    batch.apply_sweep(sw);
+    const double s = batch.run();
+    if (steps) *steps = batch.total_steps();
+    if (seconds) *seconds = s;
+    if (results_path) {
+      ssb::Results r = batch.results(&sw);
+      r.tMax = sw.tMax;
+      r.every = sw.every;
+      ssb::save_results(r, results_path);
+    }
+  });
+}
+
+int ssb_compare_results(const char* a_path, const char* b_path, uint64_t* compared, uint64_t* differing, char* first, size_t first_cap) {
+  return guard([&] {
+    need(a_path, "a_path"); need(b_path, "b_path");
+    const ssb::Diff d = ssb::compare_results(ssb::load_results(a_path), ssb::load_results(b_path));
+    if (compared) *compared = d.compared;
+    if (differing) *differing = d.differing;
+    if (first && first_cap) {
+      std::strncpy(first, d.first.c_str(), first_cap - 1);
+      first[first_cap - 1] = 0;
+    }
+  });
+}
+
+int ssb_portable_math_host(int32_t op, const double* x, const double* y, double* out, int64_t n) {
+  return guard([&] {
+    need(x, "x"); need(out, "out");
+    if (op < 0 || op > 3) throw std::invalid_argument("op must be 0..3");
+    ssb::portable_math_host(op, x, y, out, n);
+  });
+}
+
+int ssb_portable_math_device(int32_t op, const double* x, const double* y, double* out, int64_t n) {
+  return guard([&] {
+    need(x, "x"); need(out, "out");
+    if (op < 0 || op > 3) throw std::invalid_argument("op must be 0..3");
+    need_device();
+    const cudaError_t e = ssb::portable_math_device(op, x, y, out, n);
+    if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e));
+  });
+}
+
+}  // extern "C"

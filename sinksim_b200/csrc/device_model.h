@@ -1,0 +1,129 @@
+// Device-side layout of one compiled model (ship + sim) and of a batch of its instances.
+//
+// Layout in HBM. Everything a step reads from the model is structure-of-arrays so that a warp reading entries
+// j..j+31 moves whole 128-byte lines:
+//   columns   x, y, dxdy, zlo, zhi                     [ncol] f64       the buoyancy clip (hydro pass)
+//   segments  x, y, A (= dxdy of the column), a, e     [nseg] f64       the node pass, with the column gather of the
+//                                                                       reference (segCol -> x, y, dxdy) resolved once
+//                                                                       on the host, so a segment visit has no
+//                                                                       dependent load
+//   nodes, groups, connections, incidence (CSR), monitor lists (CSR), marks: small tables read through L1.
+// Per instance (count instances): the connection fields a sweep may change (en, area, tOn), the state (t, pose,
+// rates, per-node volume, level and centroid), the outputs, the event log, the readout curve and, for the first
+// `traced` instances, the trace records. The state of an instance being stepped lives in shared memory and
+// registers of its warp; global memory holds it between launches and after the run.
+#pragma once
+
+#include <cstdint>
+
+namespace ssb {
+
+struct DevModel {
+  // columns
+  std::int32_t ncol;
+  const double *colX, *colY, *colA, *colLo, *colHi;
+  // segments (column gather resolved)
+  std::int32_t nseg;
+  const double *segX, *segY, *segAr, *segLo, *segHi;
+  // nodes
+  std::int32_t nn;
+  const double *mu, *vmax, *amin, *aov;
+  const std::int32_t *segStart, *segCount;
+  // groups
+  std::int32_t ng;
+  const std::int32_t *gStart, *gCount, *gNodes;
+  const std::uint8_t* gMode;
+  const double *gpx, *gpy, *gpz;
+  double gMargin;
+  std::int32_t maxGroup;
+  // connections (the immutable fields)
+  std::int32_t nc;
+  const std::int32_t *ca, *cb, *skip;
+  const std::uint8_t* law;
+  const double *kx, *ky, *kz, *coef;
+  // incidence: per node its connections in increasing order (side 1 at the b end), and the sea connections
+  const std::int32_t *incStart, *incCount, *incConn;
+  const std::uint8_t* incSide;
+  std::int32_t nsea;
+  const std::int32_t* sea;
+  // monitors: per monitor its connections in increasing order
+  std::int32_t nmon;
+  double monThreshold;
+  const std::int32_t *monStart, *monCount, *monConn;
+  // marks
+  std::int32_t nmark;
+  const double *mkx, *mky, *mkz;
+  const std::uint8_t* mkWhen;
+  // founder rule
+  double hullTopBelow, pitchAbsAbove, buoyancyBelow, minT;
+  // physics and body
+  double rho, g, sq2g, dt;
+  double ms, g0x, g0y, g0z, XO, YO, mh0, Ith0, Iph0, cDz, cDth, cDph, qz, qth, qph;
+  // readout geometry
+  double xFP, xAP;
+  std::int32_t evCap;
+};
+
+// An extra retire predicate evaluated after every step (the batching workloads' "sink" and "settle" rules); it
+// never changes the physics. Disabled when enabled == 0.
+struct RetireRule {
+  std::int32_t enabled;
+  double pitchLimit;           // rad: sink when |pitch| exceeds this ...
+  double xDeck, yDeck, zDeck;  // ... and the deck edge at (xDeck, +-yDeck, zDeck) is below the sea
+  double wthLimit;             // rad/s: settle when |pitch rate| stays below this ...
+  double settleTime;           // s: ... for this long
+};
+
+// Why an instance stopped.
+enum StopReason : std::int32_t { kRunning = 0, kFoundered = 1, kTimeLimit = 2, kSinkRule = 3, kSettleRule = 4 };
+
+struct DevBatch {
+  std::int32_t count;
+  // connection fields per instance [count * nc]
+  const std::uint8_t* en;
+  const double* area;
+  const double* tOn;
+  // state per instance
+  double* st;       // [count * 8]: t, zO, pitch, roll, vz, wth, wph, calm (seconds the settle rule has held)
+  double* out;      // [count * 7]: inflow, Vb, hullTop, mw, bx, by, bz
+  double *vol, *level, *cx, *cy, *cz;   // [count * nn]
+  // events
+  double* evT;             // [count * evCap]
+  std::int32_t* evId;      // [count * evCap]
+  std::int32_t* evKind;    // [count * evCap]
+  std::int32_t* evCount;   // [count]
+  double* overT;           // [count * nmon]
+  double* markT;           // [count * nmark]
+  std::int32_t* foundered; // [count]
+  double* founderT;        // [count]
+  long long* steps;        // [count]
+  std::int32_t* stop;      // [count] StopReason
+  // readout curve of every instance: 7 values per record when t >= nextCurve
+  double curveEvery;       // <= 0 disables
+  std::int32_t curveMax;
+  double* curveRec;        // [count * curveMax * 7]
+  std::int32_t* curveCount;
+  double* nextCurve;
+  // final readouts of every instance, computed on the device when the instance stops: 7 values
+  double* finalRec;        // [count * 7]
+  // traces of the first `traced` instances
+  std::int32_t traced, denseSteps, maxSamples, recSize;
+  double sampleEvery;
+  double *denseRec, *sampleRec;
+  std::int32_t *denseCount, *sampleCount;
+  double* nextSample;
+  // run control
+  double tMax;
+  long long maxSteps;          // steps per instance per launch
+  std::int32_t firstLaunch;
+  RetireRule rule;
+  std::int32_t* queue;         // work-queue head (atomic), reset to 0 before each launch
+  std::int32_t* error;         // first error code seen by any warp (0 = none)
+};
+
+// Byte offsets of one simulation slot (one warp) in dynamic shared memory; `bytes` is the slot stride.
+struct SlotLayout {
+  std::uint32_t vol, level, cx, cy, cz, area, zmax, hEff, aEff, acc, deg, dV, q, tmp, passes, merged, bytes;
+};
+
+}  // namespace ssb

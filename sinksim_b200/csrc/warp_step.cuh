@@ -1,0 +1,697 @@
+// One time step of one simulation, computed by one warp. The physics is the reference's kernel::step in the
+// "portable" (double precision) and "portable32" (single-precision column partials) numerics
+// (engine/include/sinksim/kernel/step.hpp:41-54), reproduced bit for bit:
+//
+//   * the buoyancy integral keeps the reference's 256 partial sums (partial p sums columns p, p+256, ... in
+//     order), reduces each group of 32 partials with the halving tree (offsets 16..1) and adds the eight group
+//     results in order (kernel/reduce.hpp:12-79, hydro.hpp:241-258). One warp computes all of them: lane l holds
+//     partial w*32+l of group w, and a shuffle butterfly performs the tree, each pair combined as (lower, upper);
+//   * a node pass keeps the reference's 32 lane partials over strided segments and the same tree
+//     (hydro.hpp:305-316, reduce.hpp:52-71);
+//   * every other reduction (group sums, incidence gathers, sea inflow, excess, loads, monitors, water) runs in
+//     the reference's serial order, and every expression keeps its operation order (no contraction: -fmad=false).
+//
+// All 32 lanes hold identical copies of every scalar, so control flow stays uniform and no lane waits on another
+// except at __syncwarp points between phases that exchange per-node or per-connection arrays through shared memory.
+#pragma once
+
+#include <cstdint>
+
+#include "device_model.h"
+#include "portable_math.cuh"
+
+namespace ssb {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kLanes = 32;
+
+// Scheme v1 constants (engine/include/sinksim/kernel/scheme.hpp:11-28).
+constexpr double kEmptyVolume = 1e-6;
+constexpr double kFullFraction = 1.0 - 1e-7;
+constexpr double kLimiterShare = 0.5;
+constexpr double kOrificeHeadFloor = 0.01;
+constexpr double kWeirCoefficient = 2.0 / 3.0;
+constexpr double kWeirExponent = 1.5;
+constexpr double kVillemonteExponent = 0.385;
+constexpr int kNewtonFast = 6;
+constexpr double kSlopeMin = 1e-9;
+constexpr double kCentroidMinVolume = 1e-9;
+constexpr double kNoHead = -1e9;
+constexpr double kNoHeadTest = -1e8;
+constexpr double kPitchClamp = 1.35;
+constexpr double kRollClamp = 1.4;
+constexpr double kPi = 3.141592653589793;
+
+// JavaScript Math.max / Math.min: the first argument wins ties (kernel/math.hpp:29-30).
+__device__ __forceinline__ double jmax(double a, double b) { return (b > a) ? b : a; }
+__device__ __forceinline__ double jmin(double a, double b) { return (b < a) ? b : a; }
+
+// Pose R = Ry(pitch) Rx(roll) and translation (kernel/frame.hpp:9-21), with the single-precision copies the
+// portable32 column arithmetic uses (kernel/reduce.hpp:86-98).
+struct Pose {
+  double R00, R01, R02, R10, R11, R12, R20, R21, R22, tx, ty, tz, cth, iR;
+  float fR20, fR21, fR22, ftz, fiR;
+};
+
+__device__ __forceinline__ Pose make_pose(const DevModel& M, double zO, double th, double ph) {
+  const double cth = pm::cos(th), sth = pm::sin(th), cph = pm::cos(ph), sph = pm::sin(ph);
+  Pose F;
+  F.R00 = cth; F.R01 = sth * sph; F.R02 = sth * cph;
+  F.R10 = 0;   F.R11 = cph;       F.R12 = -sph;
+  F.R20 = -sth; F.R21 = cth * sph; F.R22 = cth * cph;
+  F.tx = M.XO - (F.R00 * M.g0x + F.R01 * M.g0y + F.R02 * M.g0z);
+  F.ty = M.YO - (F.R10 * M.g0x + F.R11 * M.g0y + F.R12 * M.g0z);
+  F.tz = zO - (F.R20 * M.g0x + F.R21 * M.g0y + F.R22 * M.g0z);
+  F.cth = cth;
+  F.iR = 1 / F.R22;
+  F.fR20 = static_cast<float>(F.R20);
+  F.fR21 = static_cast<float>(F.R21);
+  F.fR22 = static_cast<float>(F.R22);
+  F.ftz = static_cast<float>(F.tz);
+  F.fiR = 1.0f / F.fR22;
+  return F;
+}
+
+__device__ __forceinline__ double world_z(const Pose& F, double x, double y, double z) {
+  return F.R20 * x + F.R21 * y + F.R22 * z + F.tz;
+}
+
+// ----------------------------------------------------------------------------- butterfly steps of the canonical tree
+// At offset `off` the tree combines partial l (l < off) with partial l + off. With xor shuffles every lane pairs
+// with lane ^ off; sums are exact to swap (IEEE addition is commutative) and the min / max keep the reference's
+// operand order (lower partner first), so every lane ends with the bits of the tree's lane 0.
+
+template <class T>
+__device__ __forceinline__ T bsum(T v, int off) { return v + __shfl_xor_sync(kFull, v, off); }
+
+template <class T>
+__device__ __forceinline__ T bmin(T v, int off, int lane) {
+  const T o = __shfl_xor_sync(kFull, v, off);
+  const bool lower = (lane & off) == 0;
+  const T a = lower ? v : o, b = lower ? o : v;
+  return (b < a) ? b : a;
+}
+
+template <class T>
+__device__ __forceinline__ T bmax(T v, int off, int lane) {
+  const T o = __shfl_xor_sync(kFull, v, off);
+  const bool lower = (lane & off) == 0;
+  const T a = lower ? v : o, b = lower ? o : v;
+  return (b > a) ? b : a;
+}
+
+// ----------------------------------------------------------------------------- buoyancy (hydro pass, tree order)
+
+struct Buoy {
+  double V, x, y, z, top;
+};
+
+template <bool MIXED>
+__device__ __forceinline__ Buoy buoyancy(const DevModel& M, const Pose& F, int lane) {
+  double V = 0, Mx = 0, My = 0, Mz = 0, top = -1e9;
+  for (int w = 0; w < 8; ++w) {
+    double gV, gMx, gMy, gMz, gTop;
+    if constexpr (!MIXED) {
+      double pV = 0, pMx = 0, pMy = 0, pMz = 0, pTop = -1e9;
+      for (int i = w * kLanes + lane; i < M.ncol; i += 256) {
+        const double x = __ldg(M.colX + i), y = __ldg(M.colY + i), lo = __ldg(M.colLo + i), hi = __ldg(M.colHi + i);
+        const double base = F.R20 * x + F.R21 * y + F.tz;
+        const double wt = base + F.R22 * hi;
+        if (wt > pTop) pTop = wt;
+        const double zp = -base * F.iR;
+        if (zp <= lo) continue;
+        const double s = zp >= hi ? hi - lo : zp - lo;
+        const double v = __ldg(M.colA + i) * s;
+        pV += v; pMx += v * x; pMy += v * y; pMz += v * (lo + 0.5 * s);
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        pV = bsum(pV, off); pMx = bsum(pMx, off); pMy = bsum(pMy, off); pMz = bsum(pMz, off);
+        pTop = bmax(pTop, off, lane);
+      }
+      gV = pV; gMx = pMx; gMy = pMy; gMz = pMz; gTop = pTop;
+    } else {
+      float pV = 0.0f, pMx = 0.0f, pMy = 0.0f, pMz = 0.0f, pTop = -1e9f;
+      for (int i = w * kLanes + lane; i < M.ncol; i += 256) {
+        const float x = static_cast<float>(__ldg(M.colX + i)), y = static_cast<float>(__ldg(M.colY + i));
+        const float lo = static_cast<float>(__ldg(M.colLo + i)), hi = static_cast<float>(__ldg(M.colHi + i));
+        const float base = F.fR20 * x + F.fR21 * y + F.ftz;
+        const float wt = base + F.fR22 * hi;
+        if (wt > pTop) pTop = wt;
+        const float zp = -base * F.fiR;
+        if (zp <= lo) continue;
+        const float s = zp >= hi ? hi - lo : zp - lo;
+        const float v = static_cast<float>(__ldg(M.colA + i)) * s;
+        pV += v; pMx += v * x; pMy += v * y; pMz += v * (lo + 0.5f * s);
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        pV = bsum(pV, off); pMx = bsum(pMx, off); pMy = bsum(pMy, off); pMz = bsum(pMz, off);
+        pTop = bmax(pTop, off, lane);
+      }
+      gV = static_cast<double>(pV); gMx = static_cast<double>(pMx); gMy = static_cast<double>(pMy);
+      gMz = static_cast<double>(pMz); gTop = static_cast<double>(pTop);
+    }
+    if (w == 0) {
+      V = gV; Mx = gMx; My = gMy; Mz = gMz; top = gTop;
+    } else {
+      V += gV; Mx += gMx; My += gMy; Mz += gMz;
+      if (gTop > top) top = gTop;
+    }
+  }
+  Buoy b;
+  b.V = V;
+  b.x = V > 0 ? Mx / V : 0;
+  b.y = V > 0 ? My / V : 0;
+  b.z = V > 0 ? Mz / V : 0;
+  b.top = top;
+  return b;
+}
+
+// ----------------------------------------------------------------------------- node pass (tree order)
+
+struct PassR {
+  double vol, dv, mx, my, mz, zmin, zmax;
+};
+
+template <bool MIXED>
+__device__ __forceinline__ PassR node_pass(const DevModel& M, const Pose& F, int n, double h, int lane) {
+  const int s0 = __ldg(M.segStart + n), s1 = s0 + __ldg(M.segCount + n);
+  double vol, dv, mx, my, mz, zmin, zmax;
+  if constexpr (!MIXED) {
+    vol = 0; dv = 0; mx = 0; my = 0; mz = 0; zmin = 1e9; zmax = -1e9;
+    for (int j = s0 + lane; j < s1; j += kLanes) {
+      const double x = __ldg(M.segX + j), y = __ldg(M.segY + j), a = __ldg(M.segLo + j), b = __ldg(M.segHi + j);
+      const double base = F.R20 * x + F.R21 * y + F.tz;
+      const double wa = base + F.R22 * a, wb = base + F.R22 * b;
+      if (wa < zmin) zmin = wa;
+      if (wb > zmax) zmax = wb;
+      const double zp = (h - base) * F.iR;
+      if (zp <= a) continue;
+      const double A = __ldg(M.segAr + j);
+      double L;
+      if (zp >= b) {
+        L = b - a;
+      } else {
+        L = zp - a;
+        dv += A;
+      }
+      const double v = A * L;
+      vol += v; mx += v * x; my += v * y; mz += v * (a + 0.5 * L);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      vol = bsum(vol, off); dv = bsum(dv, off); mx = bsum(mx, off); my = bsum(my, off); mz = bsum(mz, off);
+      zmin = bmin(zmin, off, lane); zmax = bmax(zmax, off, lane);
+    }
+  } else {
+    const float hf = static_cast<float>(h);
+    float fvol = 0.0f, fdv = 0.0f, fmx = 0.0f, fmy = 0.0f, fmz = 0.0f, fzmin = 1e9f, fzmax = -1e9f;
+    for (int j = s0 + lane; j < s1; j += kLanes) {
+      const float x = static_cast<float>(__ldg(M.segX + j)), y = static_cast<float>(__ldg(M.segY + j));
+      const float a = static_cast<float>(__ldg(M.segLo + j)), b = static_cast<float>(__ldg(M.segHi + j));
+      const float base = F.fR20 * x + F.fR21 * y + F.ftz;
+      const float wa = base + F.fR22 * a, wb = base + F.fR22 * b;
+      if (wa < fzmin) fzmin = wa;
+      if (wb > fzmax) fzmax = wb;
+      const float zp = (hf - base) * F.fiR;
+      if (zp <= a) continue;
+      const float A = static_cast<float>(__ldg(M.segAr + j));
+      float L;
+      if (zp >= b) {
+        L = b - a;
+      } else {
+        L = zp - a;
+        fdv += A;
+      }
+      const float v = A * L;
+      fvol += v; fmx += v * x; fmy += v * y; fmz += v * (a + 0.5f * L);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      fvol = bsum(fvol, off); fdv = bsum(fdv, off); fmx = bsum(fmx, off); fmy = bsum(fmy, off); fmz = bsum(fmz, off);
+      fzmin = bmin(fzmin, off, lane); fzmax = bmax(fzmax, off, lane);
+    }
+    vol = fvol; dv = fdv; mx = fmx; my = fmy; mz = fmz; zmin = fzmin; zmax = fzmax;
+  }
+  const double mu = __ldg(M.mu + n);
+  PassR r;
+  r.vol = vol * mu;
+  r.dv = dv * mu * F.iR;
+  r.mx = mx * mu; r.my = my * mu; r.mz = mz * mu;
+  r.zmin = zmin; r.zmax = zmax;
+  return r;
+}
+
+// ----------------------------------------------------------------------------- per-warp view of the slot in shared memory
+
+struct Slot {
+  double *vol, *level, *cx, *cy, *cz, *area, *zmax, *hEff, *aEff, *acc, *dV, *q, *tmp;
+  int* deg;
+  PassR* passes;
+  std::uint8_t* merged;
+};
+
+__device__ __forceinline__ Slot carve_slot(unsigned char* base, const SlotLayout& L) {
+  Slot s;
+  s.vol = reinterpret_cast<double*>(base + L.vol);
+  s.level = reinterpret_cast<double*>(base + L.level);
+  s.cx = reinterpret_cast<double*>(base + L.cx);
+  s.cy = reinterpret_cast<double*>(base + L.cy);
+  s.cz = reinterpret_cast<double*>(base + L.cz);
+  s.area = reinterpret_cast<double*>(base + L.area);
+  s.zmax = reinterpret_cast<double*>(base + L.zmax);
+  s.hEff = reinterpret_cast<double*>(base + L.hEff);
+  s.aEff = reinterpret_cast<double*>(base + L.aEff);
+  s.acc = reinterpret_cast<double*>(base + L.acc);
+  s.dV = reinterpret_cast<double*>(base + L.dV);
+  s.q = reinterpret_cast<double*>(base + L.q);
+  s.tmp = reinterpret_cast<double*>(base + L.tmp);
+  s.deg = reinterpret_cast<int*>(base + L.deg);
+  s.passes = reinterpret_cast<PassR*>(base + L.passes);
+  s.merged = base + L.merged;
+  return s;
+}
+
+// ----------------------------------------------------------------------------- free-surface levels (kernel/levels.hpp)
+// Warp-uniform: every lane runs the solver on identical pass results and stores identical values.
+
+__device__ __forceinline__ void set_centroid(Slot& S, int n, const PassR& p) {
+  if (p.vol > kCentroidMinVolume) { S.cx[n] = p.mx / p.vol; S.cy[n] = p.my / p.vol; S.cz[n] = p.mz / p.vol; }
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void solve_single(const DevModel& M, const Pose& F, Slot& S, int n, int lane) {
+  const double V = S.vol[n], Vmax = __ldg(M.vmax + n);
+  double h = S.level[n];
+  PassR p = node_pass<MIXED>(M, F, n, h, lane);
+  const double lo = p.zmin, hi = p.zmax;
+  S.zmax[n] = hi;
+  if (V <= kEmptyVolume) { S.level[n] = lo; S.area[n] = 0; return; }
+  if (V >= Vmax * kFullFraction) {
+    p = node_pass<MIXED>(M, F, n, hi, lane);
+    const double aov = __ldg(M.aov + n);
+    S.level[n] = hi + jmax(0.0, V - Vmax) / aov;
+    S.area[n] = aov;
+    set_centroid(S, n, p);
+    return;
+  }
+  if (h < lo || h > hi) {
+    h = jmin(hi, jmax(lo, h));
+    p = node_pass<MIXED>(M, F, n, h, lane);
+  }
+  const double tol = jmax(1e-3 * Vmax, 0.5);
+  double a = lo, b = hi;
+  for (int it = 0; it < kNewtonFast; ++it) {
+    const double err = p.vol - V;
+    if (fabs(err) < tol) break;
+    if (err > 0) b = h; else a = h;
+    double hn = p.dv > kSlopeMin ? h - err / p.dv : 0.5 * (a + b);
+    if (!(hn > a && hn < b)) hn = 0.5 * (a + b);
+    h = hn;
+    p = node_pass<MIXED>(M, F, n, h, lane);
+  }
+  S.level[n] = h; S.area[n] = p.dv;
+  set_centroid(S, n, p);
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Slot& S, const int* m, int N, int lane) {
+  PassR* P = S.passes;
+  double V = 0, Vmax = 0;
+  for (int k = 0; k < N; ++k) { V += S.vol[__ldg(m + k)]; Vmax += __ldg(M.vmax + __ldg(m + k)); }
+  bool allWet = true;
+  int firstWet = -1;
+  for (int k = 0; k < N; ++k) {
+    if (S.vol[__ldg(m + k)] > 0) { if (firstWet < 0) firstWet = k; }
+    else allWet = false;
+  }
+  double h;
+  if (allWet) {
+    double s = 0;
+    for (int k = 0; k < N; ++k) s += S.level[__ldg(m + k)];
+    h = s / static_cast<double>(N);
+  } else {
+    h = S.level[__ldg(m + (firstWet >= 0 ? firstWet : N - 1))];
+  }
+  for (int k = 0; k < N; ++k) P[k] = node_pass<MIXED>(M, F, __ldg(m + k), h, lane);
+  for (int k = 0; k < N; ++k) S.zmax[__ldg(m + k)] = P[k].zmax;
+  double lo = P[0].zmin, hi = P[0].zmax;
+  for (int k = 1; k < N; ++k) { if (P[k].zmin < lo) lo = P[k].zmin; if (P[k].zmax > hi) hi = P[k].zmax; }
+
+  if (V <= kEmptyVolume) {
+    for (int k = 0; k < N; ++k) { const int n = __ldg(m + k); S.vol[n] = 0; S.level[n] = P[k].zmin; S.area[n] = 0; }
+    return;
+  }
+  if (V >= Vmax * kFullFraction) {
+    const double over = jmax(0.0, V - Vmax);
+    double aSum = 0;
+    for (int k = 0; k < N; ++k) aSum += __ldg(M.aov + __ldg(m + k));
+    const double dh = over / aSum;
+    double assigned = 0;
+    for (int k = 0; k < N - 1; ++k) {
+      const int n = __ldg(m + k);
+      const double v = __ldg(M.vmax + n) + dh * __ldg(M.aov + n);
+      S.vol[n] = v;
+      assigned += v;
+    }
+    S.vol[__ldg(m + N - 1)] = V - assigned;
+    for (int k = 0; k < N; ++k) {
+      const int n = __ldg(m + k);
+      P[k] = node_pass<MIXED>(M, F, n, hi, lane);
+      S.level[n] = hi + dh; S.area[n] = __ldg(M.aov + n);
+      set_centroid(S, n, P[k]);
+    }
+    return;
+  }
+  if (!(h >= lo && h <= hi)) {
+    h = jmin(hi, jmax(lo, h));
+    for (int k = 0; k < N; ++k) P[k] = node_pass<MIXED>(M, F, __ldg(m + k), h, lane);
+  }
+  const double tol = jmax(1e-3 * Vmax, 0.5);
+  double a = lo, b = hi;
+  for (int it = 0; it < kNewtonFast; ++it) {
+    double sum = 0;
+    for (int k = 0; k < N; ++k) sum += P[k].vol;
+    const double err = sum - V;
+    if (fabs(err) < tol) break;
+    if (err > 0) b = h; else a = h;
+    double dvs = 0;
+    for (int k = 0; k < N; ++k) dvs += P[k].dv;
+    double hn = dvs > kSlopeMin ? h - err / dvs : 0.5 * (a + b);
+    if (!(hn > a && hn < b)) hn = 0.5 * (a + b);
+    h = hn;
+    for (int k = 0; k < N; ++k) P[k] = node_pass<MIXED>(M, F, __ldg(m + k), h, lane);
+  }
+  double tot = 0;
+  for (int k = 0; k < N; ++k) tot += P[k].vol;
+  double assigned = 0;
+  for (int k = 0; k < N - 1; ++k) {
+    const int n = __ldg(m + k);
+    double v = tot > 0 ? V * P[k].vol / tot : V / static_cast<double>(N);
+    const double vm = __ldg(M.vmax + n);
+    if (v > vm) v = vm;
+    S.vol[n] = v;
+    assigned += v;
+  }
+  const double vmaxLast = __ldg(M.vmax + __ldg(m + N - 1));
+  if (V - assigned > vmaxLast) {
+    // the last member would overflow: the ones before it hold V - vmaxLast, filled from the end (levels.hpp:136-155)
+    const double need = V - vmaxLast;
+    double capped = 0;
+    for (int k = N - 2; k >= 0; --k) {
+      double prior = 0;
+      for (int j = 0; j < k; ++j) prior += S.vol[__ldg(m + j)];
+      const int n = __ldg(m + k);
+      const double v = (need - capped) - prior;
+      const double vm = __ldg(M.vmax + n);
+      if (v > vm && k > 0) {
+        S.vol[n] = vm;
+        capped += vm;
+        continue;
+      }
+      S.vol[n] = v;
+      break;
+    }
+    assigned = 0;
+    for (int k = 0; k < N - 1; ++k) assigned += S.vol[__ldg(m + k)];
+  }
+  S.vol[__ldg(m + N - 1)] = V - assigned;
+  for (int k = 0; k < N; ++k) {
+    const int n = __ldg(m + k);
+    S.level[n] = h; S.area[n] = P[k].dv;
+    set_centroid(S, n, P[k]);
+  }
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, Slot& S, int lane) {
+  for (int g = 0; g < M.ng; ++g) {
+    const int N = __ldg(M.gCount + g);
+    const int* m = M.gNodes + __ldg(M.gStart + g);
+    const int mode = __ldg(M.gMode + g);
+    bool merged = false;
+    if (N >= 2) {
+      if (mode == 1) {
+        merged = true;
+      } else if (mode == 2) {
+        const double zMw = world_z(F, __ldg(M.gpx + g), __ldg(M.gpy + g), __ldg(M.gpz + g));
+        merged = true;
+        for (int k = 0; k < N; ++k) {
+          const int n = __ldg(m + k);
+          if (!(S.vol[n] > kEmptyVolume && S.level[n] > zMw + M.gMargin)) { merged = false; break; }
+        }
+      }
+    }
+    S.merged[g] = merged ? 1 : 0;
+    if (merged) solve_group<MIXED>(M, F, S, m, N, lane);
+    else for (int k = 0; k < N; ++k) solve_single<MIXED>(M, F, S, __ldg(m + k), lane);
+  }
+}
+
+// ----------------------------------------------------------------------------- flows (kernel/flows.hpp:38-78)
+
+__device__ __forceinline__ double connection_flow(const DevModel& M, const Pose& F, double t, const Slot& S, const std::uint8_t* en,
+                                                  const double* area, const double* tOn, int c, double& qOut) {
+  if (!__ldg(en + c) || __ldg(tOn + c) > t) { qOut = 0; return 0; }
+  const int sk = __ldg(M.skip + c);
+  if (sk >= 0 && S.merged[sk]) { qOut = 0; return 0; }
+  const int a = __ldg(M.ca + c), b = __ldg(M.cb + c);
+  const double zo = F.R20 * __ldg(M.kx + c) + F.R21 * __ldg(M.ky + c) + F.R22 * __ldg(M.kz + c) + F.tz;
+  const double ha = a < 0 ? 0.0 : S.hEff[a], hbv = S.hEff[b];
+  const double Ha = ha > zo ? ha - zo : 0.0, Hb = hbv > zo ? hbv - zo : 0.0;
+  double q = 0;
+  if (__ldg(M.law + c) == 0) {
+    const double d = Ha - Hb;
+    if (d != 0) q = __ldg(M.coef + c) * __ldg(area + c) * M.sq2g * d / pm::sqrt_rn(jmax(fabs(d), kOrificeHeadFloor));
+  } else {
+    const double H1 = Ha > Hb ? Ha : Hb;
+    if (H1 > 0) {
+      const double H2 = Ha > Hb ? Hb : Ha;
+      double f = 1;
+      if (H2 > 0) {
+        const double r = H2 / H1;
+        f = pm::pow(jmax(0.0, 1 - pm::pow(r, kWeirExponent)), kVillemonteExponent);
+      }
+      q = __ldg(M.coef + c) * __ldg(area + c) * kWeirCoefficient * M.sq2g * H1 * pm::sqrt_rn(H1) * f * (Ha >= Hb ? 1.0 : -1.0);
+    }
+  }
+  if (q == 0) { qOut = 0; return 0; }
+  double dV = q * M.dt;
+  const int src = dV > 0 ? a : b, dst = dV > 0 ? b : a;
+  const double hs = src < 0 ? 0.0 : S.hEff[src];
+  const double hd = dst < 0 ? 0.0 : S.hEff[dst];
+  const double inv = (src < 0 ? 0.0 : 1 / S.aEff[src]) + (dst < 0 ? 0.0 : 1 / S.aEff[dst]);
+  const int degRef = src < 0 ? S.deg[dst] : (dst < 0 ? S.deg[src] : (S.deg[src] > S.deg[dst] ? S.deg[src] : S.deg[dst]));
+  const double share = kLimiterShare / static_cast<double>(degRef > 1 ? degRef : 1);
+  double lim = inv > 0 ? share * (hs - jmax(hd, zo)) / inv : fabs(dV);
+  if (lim < 0) lim = 0;
+  if (fabs(dV) > lim) dV = dV > 0 ? lim : -lim;
+  qOut = dV / M.dt;
+  return dV;
+}
+
+// Scalars of one simulation: identical in every lane of its warp.
+struct SimRegs {
+  double t, zO, pitch, roll, vz, wth, wph, calm;
+  double inflow, Vb, hullTop, mw, bx, by, bz;
+  int foundered;
+  double founderT;
+  int evCount;
+};
+
+struct InstPtrs {
+  const std::uint8_t* en;
+  const double* area;
+  const double* tOn;
+  double *evT, *overT, *markT;
+  std::int32_t *evId, *evKind;
+};
+
+__device__ __forceinline__ void push_event(const DevModel& M, SimRegs& R, const InstPtrs& I, int id, int kind, int lane) {
+  if (R.evCount < M.evCap) {
+    if (lane == 0) { I.evT[R.evCount] = R.t; I.evId[R.evCount] = id; I.evKind[R.evCount] = kind; }
+    R.evCount++;
+  }
+}
+
+// ----------------------------------------------------------------------------- the step (kernel/step.hpp:41-54)
+
+template <bool MIXED>
+__device__ __forceinline__ void warp_step(const DevModel& M, const Pose& F, SimRegs& R, Slot& S, const InstPtrs& I, int lane) {
+  const Buoy hb = buoyancy<MIXED>(M, F, lane);
+  solve_levels<MIXED>(M, F, S, lane);
+  __syncwarp();
+
+  // effective heads and areas, then degrees (flows.hpp:15-35)
+  for (int n = lane; n < M.nn; n += kLanes) {
+    const double v = S.vol[n];
+    S.hEff[n] = v > kEmptyVolume ? S.level[n] : kNoHead;
+    S.aEff[n] = v >= __ldg(M.vmax + n) ? __ldg(M.aov + n) : jmax(S.area[n], __ldg(M.amin + n));
+  }
+  __syncwarp();
+  for (int n = lane; n < M.nn; n += kLanes) {
+    const int k0 = __ldg(M.incStart + n), k1 = k0 + __ldg(M.incCount + n);
+    int d = 0;
+    for (int k = k0; k < k1; ++k) {
+      const int c = __ldg(M.incConn + k);
+      if (!__ldg(I.en + c)) continue;
+      const int a = __ldg(M.ca + c), b = __ldg(M.cb + c);
+      if (a >= 0 && S.hEff[a] < kNoHeadTest && S.hEff[b] < kNoHeadTest) continue;
+      ++d;
+    }
+    S.deg[n] = d;
+  }
+  __syncwarp();
+  for (int c = lane; c < M.nc; c += kLanes) {
+    double q;
+    S.dV[c] = connection_flow(M, F, R.t, S, I.en, I.area, I.tOn, c, q);
+    S.q[c] = q;
+  }
+  __syncwarp();
+  // per-node gathers in increasing connection order, then the volume update (flows.hpp:81-111)
+  for (int n = lane; n < M.nn; n += kLanes) {
+    const int k0 = __ldg(M.incStart + n), k1 = k0 + __ldg(M.incCount + n);
+    double acc = 0;
+    for (int k = k0; k < k1; ++k) {
+      const double d = S.dV[__ldg(M.incConn + k)];
+      acc = __ldg(M.incSide + k) ? acc + d : acc - d;
+    }
+    double v = S.vol[n] + acc;
+    if (v < 0) v = 0;
+    const double vm = __ldg(M.vmax + n);
+    double excess = 0;
+    if (v > vm) {
+      const double head = jmax(0.0, -S.zmax[n]);
+      const double cap = vm + __ldg(M.aov + n) * head;
+      if (v > cap) { excess = v - cap; v = cap; }
+    }
+    S.acc[n] = excess;
+    S.vol[n] = v;
+  }
+  double seaIn = 0;
+  for (int k = 0; k < M.nsea; ++k) seaIn += S.dV[__ldg(M.sea + k)];
+  __syncwarp();
+  // the excess returns to the sea in node order (flows.hpp:114-118)
+  for (int n0 = 0; n0 < M.nn; n0 += kLanes) {
+    const int n = n0 + lane;
+    unsigned mask = __ballot_sync(kFull, n < M.nn && S.acc[n] > 0);
+    while (mask) {
+      const int b = __ffs(mask) - 1;
+      mask &= mask - 1;
+      seaIn -= S.acc[n0 + b];
+    }
+  }
+  R.inflow = seaIn / M.dt;
+
+  // loads (body.hpp:11-40): per-node terms in parallel, sums in node order
+  const double W = M.rho * M.g;
+  const double Fb = W * hb.V;
+  const double bxw = F.R00 * hb.x + F.R01 * hb.y + F.R02 * hb.z + F.tx;
+  const double byw = F.R10 * hb.x + F.R11 * hb.y + F.R12 * hb.z + F.ty;
+  double tauX = (byw - M.YO) * Fb, tauY = -(bxw - M.XO) * Fb;
+  double Fz = Fb - M.g * M.ms;
+  double mw = 0, Iw_p = 0, Iw_r = 0;
+  const int NN = M.nn;
+  for (int n = lane; n < NN; n += kLanes) {
+    const double V = S.vol[n];
+    if (V <= 0) continue;
+    const double x = S.cx[n], y = S.cy[n], z = S.cz[n];
+    const double wx = F.R00 * x + F.R01 * y + F.R02 * z + F.tx - M.XO;
+    const double wy = F.R10 * x + F.R11 * y + F.R12 * z + F.ty - M.YO;
+    const double wz = F.R20 * x + F.R21 * y + F.R22 * z + F.tz - R.zO;
+    const double f = -W * V;
+    const double m = M.rho * V;
+    S.tmp[n] = wy * f;
+    S.tmp[NN + n] = wx * f;
+    S.tmp[2 * NN + n] = f;
+    S.tmp[3 * NN + n] = m;
+    S.tmp[4 * NN + n] = m * (wx * wx + wz * wz);
+    S.tmp[5 * NN + n] = m * (wy * wy + wz * wz);
+  }
+  __syncwarp();
+  for (int n = 0; n < NN; ++n) {
+    if (S.vol[n] <= 0) continue;
+    tauX += S.tmp[n]; tauY -= S.tmp[NN + n]; Fz += S.tmp[2 * NN + n];
+    mw += S.tmp[3 * NN + n];
+    Iw_p += S.tmp[4 * NN + n];
+    Iw_r += S.tmp[5 * NN + n];
+  }
+  const double Mth = tauY, Mph = tauX * F.cth;
+  // integrate (body.hpp:42-57)
+  const double dt = M.dt;
+  const double mh = M.mh0 + mw;
+  const double Ith = M.Ith0 + Iw_p, Iph = M.Iph0 + Iw_r;
+  const double az = (Fz - M.cDz * R.vz - M.qz * fabs(R.vz) * R.vz) / mh;
+  const double ath = (Mth - M.cDth * R.wth - M.qth * fabs(R.wth) * R.wth) / Ith;
+  const double aph = (Mph - M.cDph * R.wph - M.qph * fabs(R.wph) * R.wph) / Iph;
+  R.vz += az * dt; R.wth += ath * dt; R.wph += aph * dt;
+  R.zO += R.vz * dt; R.pitch += R.wth * dt; R.roll += R.wph * dt;
+  if (R.pitch > kPitchClamp) { R.pitch = kPitchClamp; R.wth = 0; }
+  if (R.pitch < -kPitchClamp) { R.pitch = -kPitchClamp; R.wth = 0; }
+  if (R.roll > kRollClamp) { R.roll = kRollClamp; R.wph = 0; }
+  if (R.roll < -kRollClamp) { R.roll = -kRollClamp; R.wph = 0; }
+  R.t += dt;
+  R.Vb = hb.V; R.hullTop = hb.top; R.mw = mw;
+  R.bx = hb.x; R.by = hb.y; R.bz = hb.z;
+
+  // events (events.hpp:11-38): monitors in order, marks in order, then the founder rule
+  for (int m0 = 0; m0 < M.nmon; m0 += kLanes) {
+    const int m = m0 + lane;
+    bool fire = false;
+    if (m < M.nmon && I.overT[m] < 0) {
+      const int k0 = __ldg(M.monStart + m), k1 = k0 + __ldg(M.monCount + m);
+      double over = 0;
+      for (int k = k0; k < k1; ++k) {
+        const double qc = S.q[__ldg(M.monConn + k)];
+        if (qc > 0) over += qc;
+      }
+      fire = over > M.monThreshold;
+      if (fire) I.overT[m] = R.t;
+    }
+    unsigned mask = __ballot_sync(kFull, fire);
+    while (mask) {
+      const int b = __ffs(mask) - 1;
+      mask &= mask - 1;
+      push_event(M, R, I, m0 + b, 0, lane);
+    }
+  }
+  for (int i0 = 0; i0 < M.nmark; i0 += kLanes) {
+    const int i = i0 + lane;
+    bool fire = false;
+    if (i < M.nmark && I.markT[i] < 0) {
+      const double wz = world_z(F, __ldg(M.mkx + i), __ldg(M.mky + i), __ldg(M.mkz + i));
+      const bool under = __ldg(M.mkWhen + i) == 0;
+      fire = (under && wz < 0) || (!under && wz > 0);
+      if (fire) I.markT[i] = R.t;
+    }
+    unsigned mask = __ballot_sync(kFull, fire);
+    while (mask) {
+      const int b = __ffs(mask) - 1;
+      mask &= mask - 1;
+      push_event(M, R, I, i0 + b, 1, lane);
+    }
+  }
+  if (!R.foundered && (R.hullTop < M.hullTopBelow || fabs(R.pitch) > M.pitchAbsAbove || (R.Vb < M.buoyancyBelow && R.t > M.minT))) {
+    R.foundered = 1;
+    R.founderT = R.t;
+    push_event(M, R, I, -1, 2, lane);
+  }
+  __syncwarp();
+}
+
+// Readouts at the current state (kernel/readouts.hpp:20-36): t, trim, list, water (t), inflow (t/min), draftF, draftA.
+__device__ __forceinline__ void readouts(const DevModel& M, const SimRegs& R, const Slot& S, double* r7) {
+  const Pose F = make_pose(M, R.zO, R.pitch, R.roll);
+  double water = 0;
+  for (int n = 0; n < M.nn; ++n) water += S.vol[n];
+  r7[0] = R.t;
+  r7[1] = R.pitch * 180 / kPi;
+  r7[2] = R.roll * 180 / kPi;
+  r7[3] = water * M.rho / 1000;
+  r7[4] = R.inflow * M.rho / 1000 * 60;
+  r7[5] = -world_z(F, M.xFP, 0, 0);
+  r7[6] = -world_z(F, M.xAP, 0, 0);
+}
+
+}  // namespace ssb
