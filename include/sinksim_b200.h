@@ -156,6 +156,10 @@ int ssb_compare_results(const char* a_path, const char* b_path, uint64_t* compar
 int ssb_portable_math_host(int32_t op, const double* x, const double* y, double* out, int64_t n);
 int ssb_portable_math_device(int32_t op, const double* x, const double* y, double* out, int64_t n);
 
+/* Measured rate of separately rounded adds and multiplies on the device (fp64 = 1: double, 0: float), the
+ * denominator of the engine's roofline; operations per second through *ops_per_s. No counterpart in the reference. */
+int ssb_measure_add_mul_peak(int32_t fp64, int32_t device, double* ops_per_s);
+
 #ifdef __cplusplus
 }
 #endif

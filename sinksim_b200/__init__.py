@@ -88,7 +88,15 @@ _SIGNATURES = {
     "ssb_compare_results": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]),
     "ssb_portable_math_host": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64]),
     "ssb_portable_math_device": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64]),
+    "ssb_measure_add_mul_peak": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
 }
+
+
+def add_mul_peak(fp64=True, device=0):
+    """Measured separately-rounded add+multiply rate of the device (operations per second)."""
+    v = C.c_double()
+    _check(lib().ssb_measure_add_mul_peak(1 if fp64 else 0, device, C.byref(v)))
+    return v.value
 
 
 def library_path():

@@ -29,7 +29,7 @@ HOST_FLAGS = "-fPIC,-ffp-contract=off,-fno-fast-math,-fexcess-precision=standard
 NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-fmad=false", "-lineinfo", "-Xptxas", "-v", "-diag-suppress", "222",
                      "-Xcompiler", HOST_FLAGS, "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 
-SOURCES = ["batch_kernel.cu", "portable_math.cu", "batch.cpp", "model.cpp", "json.cpp", "sweep.cpp", "capi.cpp"]
+SOURCES = ["batch_kernel.cu", "portable_math.cu", "probes.cu", "batch.cpp", "model.cpp", "json.cpp", "sweep.cpp", "capi.cpp"]
 APPS = ["sinksim_cuda_run", "sinksim_sweep"]
 
 

@@ -15,6 +15,7 @@
 namespace ssb {
 void portable_math_host(int op, const double* x, const double* y, double* out, std::int64_t n);
 cudaError_t portable_math_device(int op, const double* x, const double* y, double* out, std::int64_t n);
+double measure_add_mul_peak(bool fp64, int device);
 }  // namespace ssb
 
 struct ssb_batch {
@@ -372,6 +373,16 @@ int ssb_portable_math_device(int32_t op, const double* x, const double* y, doubl
     need_device();
     const cudaError_t e = ssb::portable_math_device(op, x, y, out, n);
     if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e));
+  });
+}
+
+int ssb_measure_add_mul_peak(int32_t fp64, int32_t device, double* ops_per_s) {
+  return guard([&] {
+    need(ops_per_s, "ops_per_s");
+    need_device();
+    const double v = ssb::measure_add_mul_peak(fp64 != 0, device);
+    if (v < 0) throw std::runtime_error("the peak probe failed");
+    *ops_per_s = v;
   });
 }
 

@@ -10,9 +10,13 @@ import os
 import shutil
 import tempfile
 
+import sys
+
 import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 _CACHE = os.path.join(tempfile.gettempdir(), "sinksim_b200_fixtures")
@@ -35,57 +39,15 @@ def fixture(name):
     return dst
 
 
-def read_json(path):
-    if path.endswith(".gz"):
-        with gzip.open(path, "rt") as f:
-            return json.load(f)
-    with open(path) as f:
-        return json.load(f)
+from sinksim_b200.files import load_model, read_json  # noqa: E402,F401
 
 
 def titanic():
     return fixture("titanic64.ship.json"), fixture("titanic.sim.json")
 
 
-# ----------------------------------------------------------------------------------------------- model arrays
-
 def f64(v):
     return np.ascontiguousarray(np.asarray(v, dtype=np.float64))
-
-
-def i32(v):
-    return np.ascontiguousarray(np.asarray(v, dtype=np.int32))
-
-
-def u8(v):
-    return np.ascontiguousarray(np.asarray(v, dtype=np.uint8))
-
-
-def load_model(ship_path, sim_path):
-    """The arrays of a compiled ship and sim as numpy arrays (the members the kernel reads)."""
-    s = read_json(ship_path)
-    m = read_json(sim_path)
-    c, n, g = s["columns"], s["nodes"], s["segments"]
-    ship = dict(x=f64(c["x"]), y=f64(c["y"]), dxdy=f64(c["dxdy"]), zlo=f64(c["zlo"]), zhi=f64(c["zhi"]),
-                segCol=i32(g["col"]), segA=f64(g["a"]), segE=f64(g["e"]), mu=f64(n["mu"]), vmax=f64(n["vmax"]),
-                amin=f64(n["amin"]), aov=f64(n["aov"]), segStart=i32(n["segStart"]), segCount=i32(n["segCount"]))
-    G, K, Mo, Mk, Fo, B, R, S0 = (m[k] for k in ("groups", "connections", "monitors", "marks", "founder", "body", "readout", "state0"))
-    sim = dict(rho=float(m["constants"]["rho"]), g=float(m["constants"]["g"]), dt=float(m["scheme"]["dt"]),
-               gStart=i32(G["nodeStart"]), gCount=i32(G["nodeCount"]), gNodes=i32(G["nodes"]), gMode=u8(G["mode"]),
-               gpx=f64(G["px"]), gpy=f64(G["py"]), gpz=f64(G["pz"]), gMargin=float(G["margin"]),
-               ca=i32(K["a"]), cb=i32(K["b"]), law=u8(K["type"]), cx=f64(K["x"]), cy=f64(K["y"]), cz=f64(K["z"]),
-               area=f64(K["area"]), coef=f64(K["coef"]), kind=u8(K["kind"]), idx=i32(K["idx"]), en=u8(K["en"]),
-               tOn=f64(K["tOn"]), skipGroup=i32(K["skipGroup"]), monitor=i32(K["monitor"]),
-               kindNames=list(K.get("kindNames", [])),
-               nmon=len(Mo["id"]), monThreshold=float(Mo["threshold"]), monitorId=list(Mo["id"]), markId=list(Mk["id"]),
-               mkx=f64(Mk["x"]), mky=f64(Mk["y"]), mkz=f64(Mk["z"]), mkWhen=u8(Mk["when"]),
-               founder=[float(Fo[k]) for k in ("hullTopBelow", "pitchAbsAbove", "buoyancyBelow", "minT")],
-               body=[float(B["ms"]), float(B["KG"]), *map(float, B["g0"]), float(B["XO"]), float(B["YO"]),
-                     *(float(B[k]) for k in ("mh0", "Ith0", "Iph0", "cDz", "cDth", "cDph", "qz", "qth", "qph"))],
-               xFP=float(R["xFP"]), xAP=float(R["xAP"]),
-               state0=[float(S0[k]) for k in ("t", "zO", "pitch", "roll", "vz", "wth", "wph")],
-               vol0=f64(S0["vol"]), level0=f64(S0["level"]), cx0=f64(S0["cx"]), cy0=f64(S0["cy"]), cz0=f64(S0["cz"]))
-    return ship, sim
 
 
 def trace_records(tr, which):
