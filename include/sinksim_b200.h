@@ -45,8 +45,12 @@ typedef struct ssb_batch_options {
   double curve_every;        /* s between readout-curve records of every instance; 0: none */
   double t_max;              /* s: every instance stops here if it has not foundered */
   int64_t steps_per_launch;  /* 0: one persistent launch; > 0: bounded launches (the reference's stepsPerLaunch) */
-  int32_t warps_per_block;   /* simulations per block; 0: chosen by the engine */
-  int32_t blocks;            /* grid size; 0: persistent grid sized to the device */
+  int32_t team_warps;        /* warps stepping one simulation in the main phase: 1, 2, 4 or 8; 0: chosen */
+  int32_t tail_team_warps;   /* warps per simulation once few instances remain: 0 no tail phase, -1 chosen */
+  int32_t teams_per_block;   /* simulations per block in the main phase; 0: chosen */
+  int32_t yield_below;       /* the main phase hands its instances to the tail phase once at most this many remain;
+                                -1: the tail grid's capacity */
+  int32_t blocks;            /* main-phase grid size; 0: persistent grid sized to the device */
   int32_t device;            /* CUDA device ordinal */
   /* extra retire rule (disabled when rule_enabled == 0): an instance stops once |pitch| > rule_pitch and the deck
    * edge point (rule_x, +-rule_y, rule_z) is below the sea ("sink"), or once |pitch rate| < rule_wth has held for
@@ -73,8 +77,10 @@ typedef struct ssb_instance_summary {
   double outputs[7];    /* inflow, Vb, hullTop, mw, bx, by, bz of the last step */
 } ssb_instance_summary;
 
+/* The launch shape the engine chose: the main phase and the tail phase (tail_team_warps == 0: none). */
 typedef struct ssb_launch_info {
-  int32_t warps_per_block, blocks, blocks_per_sm;
+  int32_t team_warps, teams_per_block, blocks, blocks_per_sm, yield_below;
+  int32_t tail_team_warps, tail_teams_per_block, tail_blocks, tail_blocks_per_sm;
   uint64_t slot_bytes;  /* shared memory of one simulation */
 } ssb_launch_info;
 

@@ -32,7 +32,8 @@ class SinksimError(RuntimeError):
 class _Options(C.Structure):
     _fields_ = [("count", C.c_int32), ("numerics", C.c_int32), ("traced_instances", C.c_int32), ("dense_steps", C.c_int32),
                 ("sample_every", C.c_double), ("curve_every", C.c_double), ("t_max", C.c_double), ("steps_per_launch", C.c_int64),
-                ("warps_per_block", C.c_int32), ("blocks", C.c_int32), ("device", C.c_int32), ("rule_enabled", C.c_int32),
+                ("team_warps", C.c_int32), ("tail_team_warps", C.c_int32), ("teams_per_block", C.c_int32), ("yield_below", C.c_int32),
+                ("blocks", C.c_int32), ("device", C.c_int32), ("rule_enabled", C.c_int32),
                 ("rule_pitch", C.c_double), ("rule_x", C.c_double), ("rule_y", C.c_double), ("rule_z", C.c_double),
                 ("rule_wth", C.c_double), ("rule_settle", C.c_double)]
 
@@ -49,7 +50,8 @@ class _Summary(C.Structure):
 
 
 class _LaunchInfo(C.Structure):
-    _fields_ = [("warps_per_block", C.c_int32), ("blocks", C.c_int32), ("blocks_per_sm", C.c_int32), ("slot_bytes", C.c_uint64)]
+    _fields_ = [(k, C.c_int32) for k in ("team_warps", "teams_per_block", "blocks", "blocks_per_sm", "yield_below", "tail_team_warps",
+                                         "tail_teams_per_block", "tail_blocks", "tail_blocks_per_sm")] + [("slot_bytes", C.c_uint64)]
 
 
 _lib = None
@@ -155,14 +157,16 @@ class Batch:
     """
 
     def __init__(self, ship_path, sim_path, count=1, numerics="portable32", traced_instances=0, dense_steps=400, sample_every=60.0,
-                 curve_every=0.0, t_max=5 * 3600.0, steps_per_launch=0, warps_per_block=0, blocks=0, device=0, rule=None):
+                 curve_every=0.0, t_max=5 * 3600.0, steps_per_launch=0, team_warps=0, tail_team_warps=-1, teams_per_block=0, yield_below=-1,
+                 blocks=0, device=0, rule=None):
         if numerics not in NUMERICS:
             raise SinksimError(-4, f"numerics {numerics!r} is not available on the GPU (portable or portable32)")
         o = _Options()
         lib().ssb_batch_options_init(C.byref(o))
         o.count, o.numerics, o.traced_instances, o.dense_steps = count, NUMERICS[numerics], traced_instances, dense_steps
         o.sample_every, o.curve_every, o.t_max, o.steps_per_launch = sample_every, curve_every, t_max, steps_per_launch
-        o.warps_per_block, o.blocks, o.device = warps_per_block, blocks, device
+        o.team_warps, o.tail_team_warps, o.teams_per_block, o.yield_below = team_warps, tail_team_warps, teams_per_block, yield_below
+        o.blocks, o.device = blocks, device
         if rule:
             o.rule_enabled = 1
             o.rule_pitch, o.rule_x, o.rule_y, o.rule_z = rule["pitch"], rule["x"], rule["y"], rule["z"]
@@ -193,7 +197,7 @@ class Batch:
     def launch_info(self):
         li = _LaunchInfo()
         _check(lib().ssb_batch_launch_info(self._h, C.byref(li)))
-        return dict(warps_per_block=li.warps_per_block, blocks=li.blocks, blocks_per_sm=li.blocks_per_sm, slot_bytes=li.slot_bytes)
+        return {k: getattr(li, k) for k, _ in _LaunchInfo._fields_}
 
     # per-instance setup
     def restore(self, instance, record):

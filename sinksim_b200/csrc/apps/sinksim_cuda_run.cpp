@@ -109,8 +109,12 @@ int main(int argc, char** argv) {
                 ship->segments(), ship->nodes(), sim.id.c_str(), sim.groups(), sim.connections(), opt.count);
     Batch batch(ship, sim, opt);
     const LaunchConfig& lc = batch.launch_config();
-    std::printf("numerics %s; shared memory per simulation %zu bytes; %d simulations per block, %d blocks\n",
-                opt.mixedPrecision ? "portable32 (mixed precision)" : "portable (double precision)", batch.slot_bytes(), lc.warpsPerBlock, lc.blocks);
+    std::printf("numerics %s; shared memory per simulation %zu bytes; %d-warp simulations, %d per block, %d blocks",
+                opt.mixedPrecision ? "portable32 (mixed precision)" : "portable (double precision)", batch.slot_bytes(), lc.main().teamWarps,
+                lc.main().teamsPerBlock, lc.main().blocks);
+    for (std::size_t k = 1; k < lc.phases.size(); ++k)
+      std::printf("; the last %d in %d-warp simulations", lc.phases[k - 1].yieldBelow, lc.phases[k].teamWarps);
+    std::printf("\n");
     if (args.flag("perturb")) {
       const std::int32_t breachKind = sim.kindIndex("breach");
       for (std::int32_t i = 1; i < opt.count; ++i) {

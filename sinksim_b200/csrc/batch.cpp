@@ -108,7 +108,10 @@ struct Batch::Impl {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
   // model
-  DevBuf<double> colX, colY, colA, colLo, colHi, segX, segY, segAr, segLo, segHi, mu, vmax, amin, aov;
+  DevBuf<double2> colXY, colLH, segXY, segLH;
+  DevBuf<float2> colXYf, colLHf, segXYf, segLHf;
+  DevBuf<float> colAf, segArf;
+  DevBuf<double> colA, segAr, mu, vmax, amin, aov;
   DevBuf<std::int32_t> segStart, segCount, gStart, gCount, gNodes, ca, cb, skip, incStart, incCount, incConn, sea, monStart, monCount, monConn;
   DevBuf<std::uint8_t> gMode, law, incSide, mkWhen;
   DevBuf<double> gpx, gpy, gpz, kx, ky, kz, coef, mkx, mky, mkz;
@@ -118,7 +121,7 @@ struct Batch::Impl {
   DevBuf<std::uint8_t> en;
   DevBuf<double> area, tOn, st, out, vol, level, cx, cy, cz, evT, overT, markT, founderT, curveRec, nextCurve, finalRec, denseRec,
       sampleRec, nextSample;
-  DevBuf<std::int32_t> evId, evKind, evCount, foundered, stop, curveCount, denseCount, sampleCount, queue, error;
+  DevBuf<std::int32_t> evId, evKind, evCount, foundered, stop, curveCount, denseCount, sampleCount, queue, error, remaining;
   DevBuf<long long> steps;
 
   // host staging
@@ -154,6 +157,8 @@ struct Batch::Impl {
     b.rule = opt.rule;
     b.queue = queue.get();
     b.error = error.get();
+    b.remaining = remaining.get();
+    b.yieldBelow = 0;
     return b;
   }
 };
@@ -191,32 +196,52 @@ Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, c
   L.dV = take(off, sizeof(double) * static_cast<std::size_t>(std::max(I.NC, 1)));
   L.q = take(off, sizeof(double) * static_cast<std::size_t>(std::max(I.NC, 1)));
   L.tmp = take(off, 6 * nb);
-  L.passes = take(off, 7 * sizeof(double) * static_cast<std::size_t>(I.maxGroup));
+  L.passes = take(off, 7 * sizeof(double) * static_cast<std::size_t>(I.maxGroup) * 8);  // per warp of a team of up to 8
+  L.hydro = take(off, 8 * 5 * sizeof(double));
+  L.misc = take(off, 2 * sizeof(std::int32_t));
   L.merged = take(off, static_cast<std::size_t>(std::max(I.NG, 1)));
   L.bytes = off;
-
-  // launch shape: warps (simulations) per block from the slot size and the batch size; a persistent grid
-  const std::size_t optin = I.info.sharedPerBlockOptIn;
-  const int maxBySmem = static_cast<int>(optin / L.bytes);
-  if (maxBySmem < 1)
-    throw std::runtime_error("Batch: one simulation needs " + std::to_string(L.bytes) + " bytes of shared memory, the device allows " + std::to_string(optin) + " per block");
-  int W = opt_.warpsPerBlock;
-  if (W <= 0) {
-    const int sms = I.info.multiprocessors;
-    W = static_cast<int>((opt_.count + sms - 1) / sms);
-    W = std::max(1, std::min(W, kMaxWarpsPerBlock));
-  }
-  W = std::min({W, maxBySmem, kMaxWarpsPerBlock});
-  cfg_.warpsPerBlock = W;
   cfg_.slotBytes = L.bytes;
-  const std::size_t smem = static_cast<std::size_t>(W) * L.bytes;
-  check(configure_batch_kernel(opt_.mixedPrecision, smem), "cudaFuncSetAttribute");
-  int perSM = 0;
-  check(batch_kernel_occupancy(opt_.mixedPrecision, W, smem, &perSM), "occupancy");
-  if (perSM < 1) throw std::runtime_error("Batch: the kernel cannot be resident with " + std::to_string(W) + " simulations per block");
-  cfg_.blocksPerSM = perSM;
-  const int needed = static_cast<int>((opt_.count + W - 1) / W);
-  cfg_.blocks = opt_.blocks > 0 ? opt_.blocks : std::min(needed, perSM * I.info.multiprocessors);
+
+  // launch shape. Teams of W warps; a slot of shared memory per team; persistent grids sized to the device.
+  // Main phase: single-warp teams when the batch fills the device (the most simulations per SM), larger teams when it
+  // does not. Tail phase: when at most one tail grid's worth of instances remains, they resume in 8-warp teams.
+  const std::size_t optin = I.info.sharedPerBlockOptIn;
+  const int sms = I.info.multiprocessors;
+  if (L.bytes > optin)
+    throw std::runtime_error("Batch: one simulation needs " + std::to_string(L.bytes) + " bytes of shared memory, the device allows " + std::to_string(optin) + " per block");
+  auto plan = [&](int W, int teamsReq, int count) {
+    PhaseConfig p;
+    if (!valid_team_size(W)) throw std::invalid_argument("Batch: warps per simulation must be 1, 2, 4 or 8");
+    p.teamWarps = W;
+    const int maxTeams = std::min(static_cast<int>(optin / L.bytes), kMaxWarpsPerBlock / W);
+    int tpb = teamsReq > 0 ? teamsReq : std::max(1, std::min(maxTeams, (count + sms - 1) / sms));
+    tpb = std::max(1, std::min(tpb, maxTeams));
+    p.teamsPerBlock = tpb;
+    const std::size_t smem = static_cast<std::size_t>(tpb) * L.bytes;
+    check(configure_batch_kernel(opt_.mixedPrecision, W, smem), "cudaFuncSetAttribute");
+    check(batch_kernel_occupancy(opt_.mixedPrecision, W, tpb, smem, &p.blocksPerSM), "occupancy");
+    if (p.blocksPerSM < 1) throw std::runtime_error("Batch: the kernel cannot be resident with " + std::to_string(tpb) + " simulations per block");
+    p.blocks = std::min((count + tpb - 1) / tpb, p.blocksPerSM * sms);
+    return p;
+  };
+  int W1 = opt_.teamWarps;
+  if (W1 <= 0) {
+    const int fit = std::max(1, (sms * 16) / std::max(opt_.count, 1));  // about 16 warps per SM in all
+    W1 = fit >= 8 ? 8 : fit >= 4 ? 4 : fit >= 2 ? 2 : 1;
+  }
+  cfg_.phases.push_back(plan(W1, opt_.teamsPerBlock, opt_.count));
+  if (opt_.blocks > 0) cfg_.phases[0].blocks = opt_.blocks;
+  const int Wlast = opt_.tailTeamWarps < 0 ? 8 : opt_.tailTeamWarps;
+  if (Wlast > W1 && opt_.stepsPerLaunch <= 0) {
+    for (int W = W1 * 2; W <= Wlast; W *= 2) {
+      PhaseConfig p = plan(W, 0, opt_.count);
+      p.blocks = p.blocksPerSM * sms;  // any instance may be left for it
+      cfg_.phases.back().yieldBelow = std::min(opt_.count - 1, p.blocks * p.teamsPerBlock);
+      cfg_.phases.push_back(p);
+    }
+    if (opt_.yieldBelow >= 0) cfg_.phases[0].yieldBelow = opt_.yieldBelow;
+  }
 
   // model upload
   check(cudaStreamCreateWithFlags(&I.stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -225,18 +250,35 @@ Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, c
   const CompiledShip& S = *I.ship;
   const CompiledSim& M = I.sim;
   cudaStream_t s = I.stream;
-  I.colX.upload(S.x, s); I.colY.upload(S.y, s); I.colA.upload(S.dxdy, s); I.colLo.upload(S.zlo, s); I.colHi.upload(S.zhi, s);
   {
-    const std::size_t ns = S.segCol.size();
-    std::vector<double> sx(ns), sy(ns), sa(ns);
+    // geometry in the kernel's layout: paired fields, the segment -> column gather resolved, float copies
+    const std::size_t nc = S.x.size(), ns = S.segCol.size();
+    std::vector<double2> cxy(nc), clh(nc), sxy(ns), slh(ns);
+    std::vector<float2> cxyf(nc), clhf(nc), sxyf(ns), slhf(ns);
+    std::vector<double> sa(ns);
+    std::vector<float> caf(nc), saf(ns);
+    for (std::size_t i = 0; i < nc; ++i) {
+      cxy[i] = double2{S.x[i], S.y[i]};
+      clh[i] = double2{S.zlo[i], S.zhi[i]};
+      cxyf[i] = float2{static_cast<float>(S.x[i]), static_cast<float>(S.y[i])};
+      clhf[i] = float2{static_cast<float>(S.zlo[i]), static_cast<float>(S.zhi[i])};
+      caf[i] = static_cast<float>(S.dxdy[i]);
+    }
     for (std::size_t j = 0; j < ns; ++j) {
       const auto c = static_cast<std::size_t>(S.segCol[j]);
-      sx[j] = S.x[c]; sy[j] = S.y[c]; sa[j] = S.dxdy[c];
+      sxy[j] = double2{S.x[c], S.y[c]};
+      slh[j] = double2{S.segA[j], S.segE[j]};
+      sa[j] = S.dxdy[c];
+      sxyf[j] = float2{static_cast<float>(S.x[c]), static_cast<float>(S.y[c])};
+      slhf[j] = float2{static_cast<float>(S.segA[j]), static_cast<float>(S.segE[j])};
+      saf[j] = static_cast<float>(S.dxdy[c]);
     }
-    I.segX.upload(sx, s); I.segY.upload(sy, s); I.segAr.upload(sa, s);
+    I.colXY.upload(cxy, s); I.colLH.upload(clh, s); I.colA.upload(S.dxdy, s);
+    I.colXYf.upload(cxyf, s); I.colLHf.upload(clhf, s); I.colAf.upload(caf, s);
+    I.segXY.upload(sxy, s); I.segLH.upload(slh, s); I.segAr.upload(sa, s);
+    I.segXYf.upload(sxyf, s); I.segLHf.upload(slhf, s); I.segArf.upload(saf, s);
     check(cudaStreamSynchronize(s), "stream sync");
   }
-  I.segLo.upload(S.segA, s); I.segHi.upload(S.segE, s);
   I.mu.upload(S.mu, s); I.vmax.upload(S.vmax, s); I.amin.upload(S.amin, s); I.aov.upload(S.aov, s);
   I.segStart.upload(S.segStart, s); I.segCount.upload(S.segCount, s);
   I.gStart.upload(M.gNodeStart, s); I.gCount.upload(M.gNodeCount, s); I.gNodes.upload(M.gNodes, s); I.gMode.upload(M.gMode, s);
@@ -256,9 +298,11 @@ Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, c
 
   DevModel& d = I.dm;
   d.ncol = S.columns();
-  d.colX = I.colX.get(); d.colY = I.colY.get(); d.colA = I.colA.get(); d.colLo = I.colLo.get(); d.colHi = I.colHi.get();
+  d.colXY = I.colXY.get(); d.colLH = I.colLH.get(); d.colA = I.colA.get();
+  d.colXYf = I.colXYf.get(); d.colLHf = I.colLHf.get(); d.colAf = I.colAf.get();
   d.nseg = S.segments();
-  d.segX = I.segX.get(); d.segY = I.segY.get(); d.segAr = I.segAr.get(); d.segLo = I.segLo.get(); d.segHi = I.segHi.get();
+  d.segXY = I.segXY.get(); d.segLH = I.segLH.get(); d.segAr = I.segAr.get();
+  d.segXYf = I.segXYf.get(); d.segLHf = I.segLHf.get(); d.segArf = I.segArf.get();
   d.nn = I.NN;
   d.mu = I.mu.get(); d.vmax = I.vmax.get(); d.amin = I.amin.get(); d.aov = I.aov.get();
   d.segStart = I.segStart.get(); d.segCount = I.segCount.get();
@@ -391,6 +435,7 @@ void Batch::upload() {
   I.curveCount.alloc(count); check(cudaMemsetAsync(I.curveCount.get(), 0, I.curveCount.bytes(), s), "memset");
   I.nextCurve.alloc(count); check(cudaMemsetAsync(I.nextCurve.get(), 0, I.nextCurve.bytes(), s), "memset");
   I.queue.alloc(1);
+  I.remaining.alloc(1);
   I.error.alloc(1); check(cudaMemsetAsync(I.error.get(), 0, I.error.bytes(), s), "memset");
 }
 
@@ -402,13 +447,18 @@ float Batch::launch() {
   check(cudaSetDevice(opt_.device), "cudaSetDevice");
   cudaStream_t s = I.stream;
   const long long maxSteps = opt_.stepsPerLaunch > 0 ? opt_.stepsPerLaunch : LLONG_MAX;
+  check(cudaMemcpyAsync(I.remaining.get(), &opt_.count, sizeof(std::int32_t), cudaMemcpyHostToDevice, s), "copy to device");
   check(cudaEventRecord(I.ev0, s), "cudaEventRecord");
   int first = 1;
   for (;;) {
-    check(cudaMemsetAsync(I.queue.get(), 0, sizeof(std::int32_t), s), "memset");
-    check(launch_batch_kernel(opt_.mixedPrecision, I.dm, I.devBatch(opt_, maxSteps, first), I.layout, cfg_.blocks, cfg_.warpsPerBlock, s),
-          "kernel launch");
-    first = 0;
+    // phase by phase: the instances a phase paused (and any it did not reach) resume in the next phase's larger teams
+    for (const PhaseConfig& p : cfg_.phases) {
+      check(cudaMemsetAsync(I.queue.get(), 0, sizeof(std::int32_t), s), "memset");
+      DevBatch db = I.devBatch(opt_, maxSteps, first);
+      db.yieldBelow = p.yieldBelow;
+      check(launch_batch_kernel(opt_.mixedPrecision, p.teamWarps, I.dm, db, I.layout, p.blocks, p.teamsPerBlock, s), "kernel launch");
+      first = 0;
+    }
     if (opt_.stepsPerLaunch <= 0) break;
     std::vector<std::int32_t> stops;
     I.stop.download(stops, s);

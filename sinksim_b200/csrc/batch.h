@@ -23,7 +23,10 @@ struct BatchOptions {
   double curveEvery = 0;           // s between readout-curve records (0: none)
   double tMax = 5 * 3600;
   std::int64_t stepsPerLaunch = 0; // 0: one launch runs every instance to its end; > 0: bounded launches
-  std::int32_t warpsPerBlock = 0;  // 0: chosen from the slot size and the batch size
+  std::int32_t teamWarps = 0;      // warps per simulation in the main phase (1, 2, 4, 8); 0: chosen from the batch size
+  std::int32_t tailTeamWarps = -1; // warps per simulation once few instances remain; 0: no tail phase; -1: chosen
+  std::int32_t teamsPerBlock = 0;  // simulations per block in the main phase; 0: chosen from the slot size
+  std::int32_t yieldBelow = -1;    // main phase pauses once at most this many instances remain; -1: the tail grid's size
   std::int32_t blocks = 0;         // 0: persistent grid sized to the device
   RetireRule rule{};
   int device = 0;
@@ -39,9 +42,19 @@ struct DeviceInfo {
 bool cuda_available(std::string* why);
 DeviceInfo device_info(int device);
 
+// One launch phase: teams of teamWarps warps, teamsPerBlock per block, a persistent grid of `blocks`.
+struct PhaseConfig {
+  int teamWarps = 0, teamsPerBlock = 0, blocks = 0, blocksPerSM = 0;
+  int yieldBelow = 0;  // the phase pauses its instances once at most this many remain (0: never)
+};
+
+// Launch phases in order. Each phase's teams are twice the size of the previous phase's; a phase hands its
+// unfinished instances to the next once they fit in the next phase's resident teams.
 struct LaunchConfig {
-  int warpsPerBlock = 0, blocks = 0, blocksPerSM = 0;
+  std::vector<PhaseConfig> phases;
   std::size_t slotBytes = 0;
+  const PhaseConfig& main() const { return phases.front(); }
+  PhaseConfig tail() const { return phases.size() > 1 ? phases.back() : PhaseConfig{}; }
 };
 
 class Batch {

@@ -1,11 +1,16 @@
-// The batch kernel: a persistent grid whose warps each run one simulation at a time. A warp takes the next
-// instance index from a device work queue (one atomicAdd), loads that instance's state into its shared-memory
-// slot and registers, steps it until it founders, reaches tMax, meets the optional retire rule or uses up the
-// launch's step budget, stores the state back and takes the next instance. Instances of uneven run length thus
-// retire and admit new ones without any host round trip; the reference instead launched one 256-thread block per
-// instance in fixed-size chunks (engine/cuda/device_step.cuh:323-434, engine/cuda/batch.cu:287-302).
+// The batch kernel: a persistent grid whose teams (W warps each) run one simulation at a time. A team takes the
+// next instance index from a device work queue (one atomicAdd), loads that instance into its shared-memory slot and
+// registers, steps it until it founders, reaches tMax, meets the optional retire rule or uses up the launch's step
+// budget, stores it back and takes the next one. Instances of uneven run length thus retire and admit new ones
+// without a host round trip; the reference instead launched one 256-thread block per instance in fixed-size chunks
+// (engine/cuda/device_step.cuh:323-434, engine/cuda/batch.cu:287-302).
 //
-// There are no waits between warps: the only inter-warp operation is the queue's atomicAdd.
+// Adaptive team size: a launch of single-warp teams gives the most simulations per SM, but a lone simulation then
+// steps slowly. When at most `yieldBelow` instances remain unfinished, the teams pause their instances and stop
+// claiming; the next launch resumes them with larger teams, whose steps are several times shorter.
+//
+// Teams never wait on each other: the only inter-team operations are the queue's atomicAdd and the count of
+// unfinished instances (atomicSub when one stops, a plain load every 64 steps).
 #include <cuda_runtime.h>
 
 #include "batch_kernel.h"
@@ -15,7 +20,12 @@ namespace ssb {
 
 namespace {
 
-__device__ __forceinline__ void write_record(double* rec, const SimRegs& R, const Slot& S, int nn, int lane) {
+constexpr int kYieldCheckEvery = 64;
+
+template <int W>
+__device__ __forceinline__ void write_record(double* rec, const SimRegs& R, const Slot& S, int nn, const Team<W>& T) {
+  if (T.warp != 0) return;
+  const int lane = T.lane;
   if (lane == 0) {
     rec[0] = R.t; rec[1] = R.zO; rec[2] = R.pitch; rec[3] = R.roll; rec[4] = R.vz; rec[5] = R.wth; rec[6] = R.wph;
     rec[7] = R.inflow; rec[8] = R.Vb; rec[9] = R.hullTop;
@@ -30,9 +40,12 @@ __device__ __forceinline__ void write_record(double* rec, const SimRegs& R, cons
   }
 }
 
-template <bool MIXED>
-__device__ void run_instance(const DevModel& M, const DevBatch& B, Slot& S, int inst, int lane) {
-  if (B.stop[inst] != kRunning) return;
+// Runs one instance; returns true when the team paused it (yield) and must stop claiming.
+template <bool MIXED, int W>
+__device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int inst, const Team<W>& T) {
+  constexpr int kStride = 32 * W;
+  if (B.stop[inst] != kRunning) return false;
+  const int rank = T.rank;
   const std::size_t iN = static_cast<std::size_t>(inst) * M.nn;
   const std::size_t iC = static_cast<std::size_t>(inst) * M.nc;
   SimRegs R;
@@ -52,14 +65,14 @@ __device__ void run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
   I.evKind = B.evKind + static_cast<std::size_t>(inst) * M.evCap;
   I.overT = B.overT + static_cast<std::size_t>(inst) * M.nmon;
   I.markT = B.markT + static_cast<std::size_t>(inst) * M.nmark;
-  for (int n = lane; n < M.nn; n += kLanes) {
+  for (int n = rank; n < M.nn; n += kStride) {
     S.vol[n] = B.vol[iN + n]; S.level[n] = B.level[iN + n];
     S.cx[n] = B.cx[iN + n]; S.cy[n] = B.cy[iN + n]; S.cz[n] = B.cz[iN + n];
     S.area[n] = 0; S.zmax[n] = 0; S.hEff[n] = 0; S.aEff[n] = 0; S.acc[n] = 0; S.deg[n] = 0;
   }
-  for (int g = lane; g < M.ng; g += kLanes) S.merged[g] = 0;
-  for (int c = lane; c < M.nc; c += kLanes) { S.dV[c] = 0; S.q[c] = 0; }
-  __syncwarp();
+  for (int g = rank; g < M.ng; g += kStride) S.merged[g] = 0;
+  for (int c = rank; c < M.nc; c += kStride) { S.dV[c] = 0; S.q[c] = 0; }
+  T.sync();
 
   long long done = B.steps[inst];
   const bool traced = inst < B.traced;
@@ -74,37 +87,48 @@ __device__ void run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
   }
   if (B.curveEvery > 0) { curveCount = B.curveCount[inst]; nextCurve = B.nextCurve[inst]; }
 
-  if (B.firstLaunch && traced && done == 0) {
+  if (traced && done == 0 && denseCount == 0) {
     // the initial record: buoyancy at the initial pose and no inflow (the reference's Simulation::record_trace)
     const Pose F0 = make_pose(M, R.zO, R.pitch, R.roll);
-    const Buoy hb = buoyancy<MIXED>(M, F0, lane);
+    const Buoy hb = buoyancy<MIXED, W>(M, F0, T, S.hydro);
     R.inflow = 0; R.Vb = hb.V; R.hullTop = hb.top; R.bx = hb.x; R.by = hb.y; R.bz = hb.z;
-    write_record(denseBase, R, S, M.nn, lane);
-    write_record(sampleBase, R, S, M.nn, lane);
+    write_record(denseBase, R, S, M.nn, T);
+    write_record(sampleBase, R, S, M.nn, T);
     denseCount = 1; sampleCount = 1; nextSample = B.sampleEvery;
+    T.sync();
   }
 
   int stop = kRunning;
+  bool paused = false;
   Pose F = make_pose(M, R.zO, R.pitch, R.roll);
   for (long long s = 0; s < B.maxSteps; ++s) {
     if (R.foundered || R.t >= B.tMax) break;
+    if (B.yieldBelow > 0 && s > 0 && (s % kYieldCheckEvery) == 0) {
+      if (T.leader()) S.misc[1] = *reinterpret_cast<volatile int*>(B.remaining) <= B.yieldBelow ? 1 : 0;
+      T.sync();
+      const bool y = S.misc[1] != 0;
+      T.sync();
+      if (y) { paused = true; break; }
+    }
     if (B.curveEvery > 0 && R.t >= nextCurve && curveCount < B.curveMax) {
-      double r7[7];
-      readouts(M, R, S, r7);
-      if (lane == 0) {
-        double* rec = B.curveRec + (static_cast<std::size_t>(inst) * B.curveMax + curveCount) * 7;
-        for (int k = 0; k < 7; ++k) rec[k] = r7[k];
+      if (T.warp == 0) {
+        double r7[7];
+        readouts(M, R, S, r7);
+        if (T.lane == 0) {
+          double* rec = B.curveRec + (static_cast<std::size_t>(inst) * B.curveMax + curveCount) * 7;
+          for (int k = 0; k < 7; ++k) rec[k] = r7[k];
+        }
       }
       ++curveCount;
       nextCurve += B.curveEvery;
     }
-    warp_step<MIXED>(M, F, R, S, I, lane);
+    team_step<MIXED, W>(M, F, R, S, I, T);
     ++done;
     F = make_pose(M, R.zO, R.pitch, R.roll);
     if (traced) {
-      if (done <= B.denseSteps) write_record(denseBase + static_cast<std::size_t>(denseCount++) * B.recSize, R, S, M.nn, lane);
+      if (done <= B.denseSteps) write_record(denseBase + static_cast<std::size_t>(denseCount++) * B.recSize, R, S, M.nn, T);
       if (R.t >= nextSample - 1e-9 && sampleCount < B.maxSamples) {
-        write_record(sampleBase + static_cast<std::size_t>(sampleCount++) * B.recSize, R, S, M.nn, lane);
+        write_record(sampleBase + static_cast<std::size_t>(sampleCount++) * B.recSize, R, S, M.nn, T);
         nextSample += B.sampleEvery;
       }
     }
@@ -116,71 +140,118 @@ __device__ void run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
       if (R.calm >= B.rule.settleTime) { stop = kSettleRule; break; }
     }
   }
-  if (stop == kRunning) {
+  if (stop == kRunning && !paused) {
     if (R.foundered) stop = kFoundered;
     else if (R.t >= B.tMax) stop = kTimeLimit;
   }
 
   // store the instance
-  __syncwarp();
-  for (int n = lane; n < M.nn; n += kLanes) {
+  T.sync();
+  for (int n = rank; n < M.nn; n += kStride) {
     B.vol[iN + n] = S.vol[n]; B.level[iN + n] = S.level[n];
     B.cx[iN + n] = S.cx[n]; B.cy[iN + n] = S.cy[n]; B.cz[iN + n] = S.cz[n];
   }
-  if (lane == 0) {
+  if (T.leader()) {
     double* st = B.st + static_cast<std::size_t>(inst) * 8;
     st[0] = R.t; st[1] = R.zO; st[2] = R.pitch; st[3] = R.roll; st[4] = R.vz; st[5] = R.wth; st[6] = R.wph; st[7] = R.calm;
     double* o = B.out + static_cast<std::size_t>(inst) * 7;
     o[0] = R.inflow; o[1] = R.Vb; o[2] = R.hullTop; o[3] = R.mw; o[4] = R.bx; o[5] = R.by; o[6] = R.bz;
     B.foundered[inst] = R.foundered;
     B.founderT[inst] = R.founderT;
-    B.evCount[inst] = R.evCount;
+    B.evCount[inst] = R.evCount;  // the leader is lane 0 of warp 0, which keeps the event log
     B.steps[inst] = done;
     B.stop[inst] = stop;
     if (traced) { B.denseCount[inst] = denseCount; B.sampleCount[inst] = sampleCount; B.nextSample[inst] = nextSample; }
     if (B.curveEvery > 0) { B.curveCount[inst] = curveCount; B.nextCurve[inst] = nextCurve; }
+    if (stop != kRunning) atomicSub(B.remaining, 1);
   }
-  if (stop != kRunning) {
+  if (stop != kRunning && T.warp == 0) {
     double r7[7];
     readouts(M, R, S, r7);
-    if (lane == 0)
+    if (T.lane == 0)
       for (int k = 0; k < 7; ++k) B.finalRec[static_cast<std::size_t>(inst) * 7 + k] = r7[k];
   }
-  __syncwarp();
+  T.sync();
+  return paused;
+}
+
+template <bool MIXED, int W>
+__global__ void __launch_bounds__(kMaxWarpsPerBlock * 32, 1) run_batch(DevModel M, DevBatch B, SlotLayout L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warpInBlock = threadIdx.x >> 5;
+  const int team = warpInBlock / W;
+  Team<W> T;
+  T.warp = warpInBlock % W;
+  T.lane = threadIdx.x & 31;
+  T.rank = T.warp * 32 + T.lane;
+  T.bar = team + 1;
+  Slot S = carve_slot(smem + static_cast<std::size_t>(team) * L.bytes, L);
+  for (;;) {
+    if (T.leader()) S.misc[0] = atomicAdd(B.queue, 1);
+    T.sync();
+    const int inst = S.misc[0];
+    T.sync();
+    if (inst >= B.count) return;
+    if (run_instance<MIXED, W>(M, B, S, inst, T)) return;
+  }
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kMaxWarpsPerBlock * 32) run_batch(DevModel M, DevBatch B, SlotLayout L) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  Slot S = carve_slot(smem + static_cast<std::size_t>(warp) * L.bytes, L);
-  for (;;) {
-    int inst = 0;
-    if (lane == 0) inst = atomicAdd(B.queue, 1);
-    inst = __shfl_sync(kFull, inst, 0);
-    if (inst >= B.count) return;
-    run_instance<MIXED>(M, B, S, inst, lane);
+cudaError_t set_smem(int W, std::size_t bytes) {
+  const int b = static_cast<int>(bytes);
+  switch (W) {
+    case 1: return cudaFuncSetAttribute(run_batch<MIXED, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    case 2: return cudaFuncSetAttribute(run_batch<MIXED, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    case 4: return cudaFuncSetAttribute(run_batch<MIXED, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    case 8: return cudaFuncSetAttribute(run_batch<MIXED, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <bool MIXED>
+cudaError_t occupancy(int W, int threads, std::size_t bytes, int* perSM) {
+  switch (W) {
+    case 1: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 1>, threads, bytes);
+    case 2: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 2>, threads, bytes);
+    case 4: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 4>, threads, bytes);
+    case 8: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 8>, threads, bytes);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <bool MIXED>
+void launch(int W, const DevModel& M, const DevBatch& B, const SlotLayout& L, int grid, int threads, std::size_t smem, cudaStream_t s) {
+  switch (W) {
+    case 1: run_batch<MIXED, 1><<<grid, threads, smem, s>>>(M, B, L); break;
+    case 2: run_batch<MIXED, 2><<<grid, threads, smem, s>>>(M, B, L); break;
+    case 4: run_batch<MIXED, 4><<<grid, threads, smem, s>>>(M, B, L); break;
+    case 8: run_batch<MIXED, 8><<<grid, threads, smem, s>>>(M, B, L); break;
   }
 }
 
 }  // namespace
 
-cudaError_t configure_batch_kernel(bool mixed, std::size_t smemBytes) {
-  if (mixed) return cudaFuncSetAttribute(run_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemBytes));
-  return cudaFuncSetAttribute(run_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemBytes));
+bool valid_team_size(int W) { return W == 1 || W == 2 || W == 4 || W == 8; }
+
+cudaError_t configure_batch_kernel(bool mixed, int teamWarps, std::size_t smemBytes) {
+  if (!valid_team_size(teamWarps)) return cudaErrorInvalidValue;
+  return mixed ? set_smem<true>(teamWarps, smemBytes) : set_smem<false>(teamWarps, smemBytes);
 }
 
-cudaError_t launch_batch_kernel(bool mixed, const DevModel& M, const DevBatch& B, const SlotLayout& L, int grid, int warpsPerBlock,
-                                cudaStream_t stream) {
-  const std::size_t smem = static_cast<std::size_t>(warpsPerBlock) * L.bytes;
-  if (mixed) run_batch<true><<<grid, warpsPerBlock * 32, smem, stream>>>(M, B, L);
-  else run_batch<false><<<grid, warpsPerBlock * 32, smem, stream>>>(M, B, L);
+cudaError_t launch_batch_kernel(bool mixed, int teamWarps, const DevModel& M, const DevBatch& B, const SlotLayout& L, int grid,
+                                int teamsPerBlock, cudaStream_t stream) {
+  if (!valid_team_size(teamWarps) || teamsPerBlock * teamWarps > kMaxWarpsPerBlock) return cudaErrorInvalidValue;
+  const std::size_t smem = static_cast<std::size_t>(teamsPerBlock) * L.bytes;
+  const int threads = teamsPerBlock * teamWarps * 32;
+  if (mixed) launch<true>(teamWarps, M, B, L, grid, threads, smem, stream);
+  else launch<false>(teamWarps, M, B, L, grid, threads, smem, stream);
   return cudaGetLastError();
 }
 
-cudaError_t batch_kernel_occupancy(bool mixed, int warpsPerBlock, std::size_t smemBytes, int* blocksPerSM) {
-  if (mixed) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSM, run_batch<true>, warpsPerBlock * 32, smemBytes);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSM, run_batch<false>, warpsPerBlock * 32, smemBytes);
+cudaError_t batch_kernel_occupancy(bool mixed, int teamWarps, int teamsPerBlock, std::size_t smemBytes, int* blocksPerSM) {
+  if (!valid_team_size(teamWarps)) return cudaErrorInvalidValue;
+  const int threads = teamsPerBlock * teamWarps * 32;
+  return mixed ? occupancy<true>(teamWarps, threads, smemBytes, blocksPerSM) : occupancy<false>(teamWarps, threads, smemBytes, blocksPerSM);
 }
 
 }  // namespace ssb

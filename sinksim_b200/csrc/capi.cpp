@@ -78,7 +78,10 @@ ssb::BatchOptions to_options(const ssb_batch_options& o) {
   b.curveEvery = o.curve_every;
   b.tMax = o.t_max;
   b.stepsPerLaunch = o.steps_per_launch;
-  b.warpsPerBlock = o.warps_per_block;
+  b.teamWarps = o.team_warps;
+  b.tailTeamWarps = o.tail_team_warps;
+  b.teamsPerBlock = o.teams_per_block;
+  b.yieldBelow = o.yield_below;
   b.blocks = o.blocks;
   b.device = o.device;
   b.rule.enabled = o.rule_enabled;
@@ -134,6 +137,8 @@ void ssb_batch_options_init(ssb_batch_options* o) {
   o->sample_every = 60;
   o->curve_every = 0;
   o->t_max = 5 * 3600;
+  o->tail_team_warps = -1;
+  o->yield_below = -1;
 }
 
 int ssb_batch_create(const char* ship_path, const char* sim_path, const ssb_batch_options* opt, ssb_batch** out) {
@@ -165,7 +170,12 @@ int ssb_batch_launch_info(const ssb_batch* b, ssb_launch_info* out) {
   return guard([&] {
     need(b, "batch"); need(out, "out");
     const ssb::LaunchConfig& c = b->batch->launch_config();
-    out->warps_per_block = c.warpsPerBlock; out->blocks = c.blocks; out->blocks_per_sm = c.blocksPerSM; out->slot_bytes = c.slotBytes;
+    const ssb::PhaseConfig m = c.main(), t = c.tail();
+    out->team_warps = m.teamWarps; out->teams_per_block = m.teamsPerBlock; out->blocks = m.blocks;
+    out->blocks_per_sm = m.blocksPerSM; out->yield_below = m.yieldBelow;
+    out->tail_team_warps = t.teamWarps; out->tail_teams_per_block = t.teamsPerBlock; out->tail_blocks = t.blocks;
+    out->tail_blocks_per_sm = t.blocksPerSM;
+    out->slot_bytes = c.slotBytes;
   });
 }
 

@@ -16,15 +16,25 @@
 
 #include <cstdint>
 
+#include <vector_types.h>
+
 namespace ssb {
 
 struct DevModel {
-  // columns
+  // columns: (x, y) and (zlo, zhi) pairs, so one 16-byte load fetches two fields, and the footprint dxdy; the float
+  // copies are the same values rounded to single precision once on the host (the portable32 column arithmetic
+  // rounds every geometry value to float before using it, kernel/reduce.hpp:131-164)
   std::int32_t ncol;
-  const double *colX, *colY, *colA, *colLo, *colHi;
-  // segments (column gather resolved)
+  const double2 *colXY, *colLH;
+  const double* colA;
+  const float2 *colXYf, *colLHf;
+  const float* colAf;
+  // segments with the column gather resolved: (x, y) of the column, (a, e) of the segment, the column's dxdy
   std::int32_t nseg;
-  const double *segX, *segY, *segAr, *segLo, *segHi;
+  const double2 *segXY, *segLH;
+  const double* segAr;
+  const float2 *segXYf, *segLHf;
+  const float* segArf;
   // nodes
   std::int32_t nn;
   const double *mu, *vmax, *amin, *aov;
@@ -119,11 +129,18 @@ struct DevBatch {
   RetireRule rule;
   std::int32_t* queue;         // work-queue head (atomic), reset to 0 before each launch
   std::int32_t* error;         // first error code seen by any warp (0 = none)
+  // adaptive team size: instances not yet stopped (atomic, set to count before the first launch); a launch with
+  // yieldBelow > 0 pauses its instances and stops claiming new ones once at most yieldBelow remain, so that the
+  // next launch resumes them with larger teams (shorter steps)
+  std::int32_t* remaining;
+  std::int32_t yieldBelow;
 };
 
-// Byte offsets of one simulation slot (one warp) in dynamic shared memory; `bytes` is the slot stride.
+// Byte offsets of one simulation slot (one team of warps) in dynamic shared memory; `bytes` is the slot stride.
+// passes holds maxGroup node-pass results per warp of the team; hydro the eight buoyancy tree results; misc two
+// ints the team broadcasts (the claimed instance, the yield decision).
 struct SlotLayout {
-  std::uint32_t vol, level, cx, cy, cz, area, zmax, hEff, aEff, acc, deg, dV, q, tmp, passes, merged, bytes;
+  std::uint32_t vol, level, cx, cy, cz, area, zmax, hEff, aEff, acc, deg, dV, q, tmp, passes, hydro, misc, merged, bytes;
 };
 
 }  // namespace ssb

@@ -100,64 +100,129 @@ __device__ __forceinline__ T bmax(T v, int off, int lane) {
   return (b > a) ? b : a;
 }
 
+// ----------------------------------------------------------------------------- a team of W warps stepping one simulation
+
+// Thread `rank` of the team (0 .. 32 W - 1), its warp and lane. Teams of more than one warp synchronise on their own
+// named barrier (ids 1..15; 0 is __syncthreads), so teams in one block never wait on each other.
+template <int W>
+struct Team {
+  int rank, warp, lane, bar;
+  __device__ __forceinline__ void sync() const {
+    if constexpr (W == 1) __syncwarp();
+    else asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(W * 32) : "memory");
+  }
+  __device__ __forceinline__ bool leader() const { return rank == 0; }
+};
+
 // ----------------------------------------------------------------------------- buoyancy (hydro pass, tree order)
 
 struct Buoy {
   double V, x, y, z, top;
 };
 
-template <bool MIXED>
-__device__ __forceinline__ Buoy buoyancy(const DevModel& M, const Pose& F, int lane) {
-  double V = 0, Mx = 0, My = 0, Mz = 0, top = -1e9;
-  for (int w = 0; w < 8; ++w) {
-    double gV, gMx, gMy, gMz, gTop;
+// One column into a buoyancy partial (kernel/reduce.hpp:39-49 in double, :131-142 in float): the same expressions in
+// the same order for T = double (portable) and T = float (portable32).
+template <class T>
+struct ColPartial {
+  T V, Mx, My, Mz, top;
+};
+
+template <class T>
+__device__ __forceinline__ void clip_column(T x, T y, T lo, T hi, T A, T R20, T R21, T R22, T tz, T iR, ColPartial<T>& p) {
+  const T base = R20 * x + R21 * y + tz;
+  const T wt = base + R22 * hi;
+  if (wt > p.top) p.top = wt;
+  const T zp = -base * iR;
+  if (zp <= lo) return;
+  const T s = zp >= hi ? hi - lo : zp - lo;
+  const T v = A * s;
+  p.V += v; p.Mx += v * x; p.My += v * y; p.Mz += v * (lo + T(0.5) * s);
+}
+
+// One segment into a node-pass partial (kernel/reduce.hpp:52-71 in double, :144-164 in float).
+template <class T>
+struct SegPartial {
+  T vol, dv, mx, my, mz, zmin, zmax;
+};
+
+template <class T>
+__device__ __forceinline__ void clip_segment(T x, T y, T a, T b, T A, T R20, T R21, T R22, T tz, T iR, T h, SegPartial<T>& p) {
+  const T base = R20 * x + R21 * y + tz;
+  const T wa = base + R22 * a, wb = base + R22 * b;
+  if (wa < p.zmin) p.zmin = wa;
+  if (wb > p.zmax) p.zmax = wb;
+  const T zp = (h - base) * iR;
+  if (zp <= a) return;
+  T L;
+  if (zp >= b) {
+    L = b - a;
+  } else {
+    L = zp - a;
+    p.dv += A;
+  }
+  const T v = A * L;
+  p.vol += v; p.mx += v * x; p.my += v * y; p.mz += v * (a + T(0.5) * L);
+}
+
+template <class T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+// Lane `lane`'s partial of tree w: columns w*32 + lane + 256 k in increasing k, two at a time (loads of the second
+// column issue before the first is clipped; the clips stay in order).
+template <class T>
+__device__ __forceinline__ ColPartial<T> column_partial(const typename Vec2<T>::type* xy, const typename Vec2<T>::type* lh, const T* area,
+                                                        int ncol, int first, T R20, T R21, T R22, T tz, T iR) {
+  ColPartial<T> p{T(0), T(0), T(0), T(0), T(-1e9)};
+  int i = first;
+  for (; i + 256 < ncol; i += 512) {
+    const auto a0 = __ldg(xy + i), b0 = __ldg(lh + i), a1 = __ldg(xy + i + 256), b1 = __ldg(lh + i + 256);
+    const T A0 = __ldg(area + i), A1 = __ldg(area + i + 256);
+    clip_column<T>(a0.x, a0.y, b0.x, b0.y, A0, R20, R21, R22, tz, iR, p);
+    clip_column<T>(a1.x, a1.y, b1.x, b1.y, A1, R20, R21, R22, tz, iR, p);
+  }
+  if (i < ncol) {
+    const auto a0 = __ldg(xy + i), b0 = __ldg(lh + i);
+    clip_column<T>(a0.x, a0.y, b0.x, b0.y, __ldg(area + i), R20, R21, R22, tz, iR, p);
+  }
+  return p;
+}
+
+// The eight trees are spread over the team's warps (warp v computes trees v, v + W, ...); the tree results meet in
+// shared memory and every thread adds them in the reference's order (trees 0..7).
+template <bool MIXED, int W>
+__device__ __forceinline__ Buoy buoyancy(const DevModel& M, const Pose& F, const Team<W>& T, double* trees) {
+  const int lane = T.lane;
+  for (int w = T.warp; w < 8; w += W) {
+    double g[5];
     if constexpr (!MIXED) {
-      double pV = 0, pMx = 0, pMy = 0, pMz = 0, pTop = -1e9;
-      for (int i = w * kLanes + lane; i < M.ncol; i += 256) {
-        const double x = __ldg(M.colX + i), y = __ldg(M.colY + i), lo = __ldg(M.colLo + i), hi = __ldg(M.colHi + i);
-        const double base = F.R20 * x + F.R21 * y + F.tz;
-        const double wt = base + F.R22 * hi;
-        if (wt > pTop) pTop = wt;
-        const double zp = -base * F.iR;
-        if (zp <= lo) continue;
-        const double s = zp >= hi ? hi - lo : zp - lo;
-        const double v = __ldg(M.colA + i) * s;
-        pV += v; pMx += v * x; pMy += v * y; pMz += v * (lo + 0.5 * s);
-      }
+      ColPartial<double> p = column_partial<double>(M.colXY, M.colLH, M.colA, M.ncol, w * kLanes + lane, F.R20, F.R21, F.R22, F.tz, F.iR);
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
-        pV = bsum(pV, off); pMx = bsum(pMx, off); pMy = bsum(pMy, off); pMz = bsum(pMz, off);
-        pTop = bmax(pTop, off, lane);
+        p.V = bsum(p.V, off); p.Mx = bsum(p.Mx, off); p.My = bsum(p.My, off); p.Mz = bsum(p.Mz, off);
+        p.top = bmax(p.top, off, lane);
       }
-      gV = pV; gMx = pMx; gMy = pMy; gMz = pMz; gTop = pTop;
+      g[0] = p.V; g[1] = p.Mx; g[2] = p.My; g[3] = p.Mz; g[4] = p.top;
     } else {
-      float pV = 0.0f, pMx = 0.0f, pMy = 0.0f, pMz = 0.0f, pTop = -1e9f;
-      for (int i = w * kLanes + lane; i < M.ncol; i += 256) {
-        const float x = static_cast<float>(__ldg(M.colX + i)), y = static_cast<float>(__ldg(M.colY + i));
-        const float lo = static_cast<float>(__ldg(M.colLo + i)), hi = static_cast<float>(__ldg(M.colHi + i));
-        const float base = F.fR20 * x + F.fR21 * y + F.ftz;
-        const float wt = base + F.fR22 * hi;
-        if (wt > pTop) pTop = wt;
-        const float zp = -base * F.fiR;
-        if (zp <= lo) continue;
-        const float s = zp >= hi ? hi - lo : zp - lo;
-        const float v = static_cast<float>(__ldg(M.colA + i)) * s;
-        pV += v; pMx += v * x; pMy += v * y; pMz += v * (lo + 0.5f * s);
-      }
+      ColPartial<float> p = column_partial<float>(M.colXYf, M.colLHf, M.colAf, M.ncol, w * kLanes + lane, F.fR20, F.fR21, F.fR22, F.ftz, F.fiR);
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
-        pV = bsum(pV, off); pMx = bsum(pMx, off); pMy = bsum(pMy, off); pMz = bsum(pMz, off);
-        pTop = bmax(pTop, off, lane);
+        p.V = bsum(p.V, off); p.Mx = bsum(p.Mx, off); p.My = bsum(p.My, off); p.Mz = bsum(p.Mz, off);
+        p.top = bmax(p.top, off, lane);
       }
-      gV = static_cast<double>(pV); gMx = static_cast<double>(pMx); gMy = static_cast<double>(pMy);
-      gMz = static_cast<double>(pMz); gTop = static_cast<double>(pTop);
+      g[0] = p.V; g[1] = p.Mx; g[2] = p.My; g[3] = p.Mz; g[4] = p.top;
     }
-    if (w == 0) {
-      V = gV; Mx = gMx; My = gMy; Mz = gMz; top = gTop;
-    } else {
-      V += gV; Mx += gMx; My += gMy; Mz += gMz;
-      if (gTop > top) top = gTop;
+    if (lane == 0) {
+      double* t = trees + 5 * w;
+      for (int k = 0; k < 5; ++k) t[k] = g[k];
     }
+  }
+  T.sync();
+  double V = trees[0], Mx = trees[1], My = trees[2], Mz = trees[3], top = trees[4];
+  for (int w = 1; w < 8; ++w) {
+    const double* t = trees + 5 * w;
+    V += t[0]; Mx += t[1]; My += t[2]; Mz += t[3];
+    if (t[4] > top) top = t[4];
   }
   Buoy b;
   b.V = V;
@@ -174,65 +239,46 @@ struct PassR {
   double vol, dv, mx, my, mz, zmin, zmax;
 };
 
+// Lane `lane`'s partial of a node pass: segments s0 + lane + 32 k in increasing k, two at a time.
+template <class T>
+__device__ __forceinline__ SegPartial<T> segment_partial(const typename Vec2<T>::type* xy, const typename Vec2<T>::type* ab, const T* area,
+                                                         int first, int end, T R20, T R21, T R22, T tz, T iR, T h) {
+  SegPartial<T> p{T(0), T(0), T(0), T(0), T(0), T(1e9), T(-1e9)};
+  int j = first;
+  for (; j + kLanes < end; j += 2 * kLanes) {
+    const auto a0 = __ldg(xy + j), b0 = __ldg(ab + j), a1 = __ldg(xy + j + kLanes), b1 = __ldg(ab + j + kLanes);
+    const T A0 = __ldg(area + j), A1 = __ldg(area + j + kLanes);
+    clip_segment<T>(a0.x, a0.y, b0.x, b0.y, A0, R20, R21, R22, tz, iR, h, p);
+    clip_segment<T>(a1.x, a1.y, b1.x, b1.y, A1, R20, R21, R22, tz, iR, h, p);
+  }
+  if (j < end) {
+    const auto a0 = __ldg(xy + j), b0 = __ldg(ab + j);
+    clip_segment<T>(a0.x, a0.y, b0.x, b0.y, __ldg(area + j), R20, R21, R22, tz, iR, h, p);
+  }
+  return p;
+}
+
 template <bool MIXED>
 __device__ __forceinline__ PassR node_pass(const DevModel& M, const Pose& F, int n, double h, int lane) {
   const int s0 = __ldg(M.segStart + n), s1 = s0 + __ldg(M.segCount + n);
   double vol, dv, mx, my, mz, zmin, zmax;
   if constexpr (!MIXED) {
-    vol = 0; dv = 0; mx = 0; my = 0; mz = 0; zmin = 1e9; zmax = -1e9;
-    for (int j = s0 + lane; j < s1; j += kLanes) {
-      const double x = __ldg(M.segX + j), y = __ldg(M.segY + j), a = __ldg(M.segLo + j), b = __ldg(M.segHi + j);
-      const double base = F.R20 * x + F.R21 * y + F.tz;
-      const double wa = base + F.R22 * a, wb = base + F.R22 * b;
-      if (wa < zmin) zmin = wa;
-      if (wb > zmax) zmax = wb;
-      const double zp = (h - base) * F.iR;
-      if (zp <= a) continue;
-      const double A = __ldg(M.segAr + j);
-      double L;
-      if (zp >= b) {
-        L = b - a;
-      } else {
-        L = zp - a;
-        dv += A;
-      }
-      const double v = A * L;
-      vol += v; mx += v * x; my += v * y; mz += v * (a + 0.5 * L);
-    }
+    SegPartial<double> p = segment_partial<double>(M.segXY, M.segLH, M.segAr, s0 + lane, s1, F.R20, F.R21, F.R22, F.tz, F.iR, h);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
-      vol = bsum(vol, off); dv = bsum(dv, off); mx = bsum(mx, off); my = bsum(my, off); mz = bsum(mz, off);
-      zmin = bmin(zmin, off, lane); zmax = bmax(zmax, off, lane);
+      p.vol = bsum(p.vol, off); p.dv = bsum(p.dv, off); p.mx = bsum(p.mx, off); p.my = bsum(p.my, off); p.mz = bsum(p.mz, off);
+      p.zmin = bmin(p.zmin, off, lane); p.zmax = bmax(p.zmax, off, lane);
     }
+    vol = p.vol; dv = p.dv; mx = p.mx; my = p.my; mz = p.mz; zmin = p.zmin; zmax = p.zmax;
   } else {
-    const float hf = static_cast<float>(h);
-    float fvol = 0.0f, fdv = 0.0f, fmx = 0.0f, fmy = 0.0f, fmz = 0.0f, fzmin = 1e9f, fzmax = -1e9f;
-    for (int j = s0 + lane; j < s1; j += kLanes) {
-      const float x = static_cast<float>(__ldg(M.segX + j)), y = static_cast<float>(__ldg(M.segY + j));
-      const float a = static_cast<float>(__ldg(M.segLo + j)), b = static_cast<float>(__ldg(M.segHi + j));
-      const float base = F.fR20 * x + F.fR21 * y + F.ftz;
-      const float wa = base + F.fR22 * a, wb = base + F.fR22 * b;
-      if (wa < fzmin) fzmin = wa;
-      if (wb > fzmax) fzmax = wb;
-      const float zp = (hf - base) * F.fiR;
-      if (zp <= a) continue;
-      const float A = static_cast<float>(__ldg(M.segAr + j));
-      float L;
-      if (zp >= b) {
-        L = b - a;
-      } else {
-        L = zp - a;
-        fdv += A;
-      }
-      const float v = A * L;
-      fvol += v; fmx += v * x; fmy += v * y; fmz += v * (a + 0.5f * L);
-    }
+    SegPartial<float> p = segment_partial<float>(M.segXYf, M.segLHf, M.segArf, s0 + lane, s1, F.fR20, F.fR21, F.fR22, F.ftz, F.fiR,
+                                                 static_cast<float>(h));
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
-      fvol = bsum(fvol, off); fdv = bsum(fdv, off); fmx = bsum(fmx, off); fmy = bsum(fmy, off); fmz = bsum(fmz, off);
-      fzmin = bmin(fzmin, off, lane); fzmax = bmax(fzmax, off, lane);
+      p.vol = bsum(p.vol, off); p.dv = bsum(p.dv, off); p.mx = bsum(p.mx, off); p.my = bsum(p.my, off); p.mz = bsum(p.mz, off);
+      p.zmin = bmin(p.zmin, off, lane); p.zmax = bmax(p.zmax, off, lane);
     }
-    vol = fvol; dv = fdv; mx = fmx; my = fmy; mz = fmz; zmin = fzmin; zmax = fzmax;
+    vol = p.vol; dv = p.dv; mx = p.mx; my = p.my; mz = p.mz; zmin = p.zmin; zmax = p.zmax;
   }
   const double mu = __ldg(M.mu + n);
   PassR r;
@@ -246,8 +292,9 @@ __device__ __forceinline__ PassR node_pass(const DevModel& M, const Pose& F, int
 // ----------------------------------------------------------------------------- per-warp view of the slot in shared memory
 
 struct Slot {
-  double *vol, *level, *cx, *cy, *cz, *area, *zmax, *hEff, *aEff, *acc, *dV, *q, *tmp;
+  double *vol, *level, *cx, *cy, *cz, *area, *zmax, *hEff, *aEff, *acc, *dV, *q, *tmp, *hydro;
   int* deg;
+  int* misc;
   PassR* passes;
   std::uint8_t* merged;
 };
@@ -268,6 +315,8 @@ __device__ __forceinline__ Slot carve_slot(unsigned char* base, const SlotLayout
   s.q = reinterpret_cast<double*>(base + L.q);
   s.tmp = reinterpret_cast<double*>(base + L.tmp);
   s.deg = reinterpret_cast<int*>(base + L.deg);
+  s.hydro = reinterpret_cast<double*>(base + L.hydro);
+  s.misc = reinterpret_cast<int*>(base + L.misc);
   s.passes = reinterpret_cast<PassR*>(base + L.passes);
   s.merged = base + L.merged;
   return s;
@@ -316,8 +365,7 @@ __device__ __forceinline__ void solve_single(const DevModel& M, const Pose& F, S
 }
 
 template <bool MIXED>
-__device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Slot& S, const int* m, int N, int lane) {
-  PassR* P = S.passes;
+__device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Slot& S, PassR* P, const int* m, int N, int lane) {
   double V = 0, Vmax = 0;
   for (int k = 0; k < N; ++k) { V += S.vol[__ldg(m + k)]; Vmax += __ldg(M.vmax + __ldg(m + k)); }
   bool allWet = true;
@@ -424,9 +472,13 @@ __device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Sl
   }
 }
 
-template <bool MIXED>
-__device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, Slot& S, int lane) {
-  for (int g = 0; g < M.ng; ++g) {
+// Groups are independent (a group's solve reads and writes only its members), so the team's warps take them in turn:
+// warp v solves groups v, v + W, ... (the reference's block did the same with its eight warps, device_step.cuh:270-281).
+template <bool MIXED, int W>
+__device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, Slot& S, const Team<W>& T) {
+  const int lane = T.lane;
+  PassR* P = S.passes + static_cast<std::size_t>(T.warp) * M.maxGroup;
+  for (int g = T.warp; g < M.ng; g += W) {
     const int N = __ldg(M.gCount + g);
     const int* m = M.gNodes + __ldg(M.gStart + g);
     const int mode = __ldg(M.gMode + g);
@@ -444,7 +496,7 @@ __device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, S
       }
     }
     S.merged[g] = merged ? 1 : 0;
-    if (merged) solve_group<MIXED>(M, F, S, m, N, lane);
+    if (merged) solve_group<MIXED>(M, F, S, P, m, N, lane);
     else for (int k = 0; k < N; ++k) solve_single<MIXED>(M, F, S, __ldg(m + k), lane);
   }
 }
@@ -508,6 +560,7 @@ struct InstPtrs {
   std::int32_t *evId, *evKind;
 };
 
+// The event log belongs to warp 0 of the team: only its lane 0 writes, only its count is stored.
 __device__ __forceinline__ void push_event(const DevModel& M, SimRegs& R, const InstPtrs& I, int id, int kind, int lane) {
   if (R.evCount < M.evCap) {
     if (lane == 0) { I.evT[R.evCount] = R.t; I.evId[R.evCount] = id; I.evKind[R.evCount] = kind; }
@@ -516,21 +569,26 @@ __device__ __forceinline__ void push_event(const DevModel& M, SimRegs& R, const 
 }
 
 // ----------------------------------------------------------------------------- the step (kernel/step.hpp:41-54)
+// Phases that exchange per-node or per-connection arrays are separated by team barriers; per-node and
+// per-connection work is spread over all 32 W threads of the team; scalars are computed redundantly and identically
+// by every thread, so every decision is uniform across the team.
 
-template <bool MIXED>
-__device__ __forceinline__ void warp_step(const DevModel& M, const Pose& F, SimRegs& R, Slot& S, const InstPtrs& I, int lane) {
-  const Buoy hb = buoyancy<MIXED>(M, F, lane);
-  solve_levels<MIXED>(M, F, S, lane);
-  __syncwarp();
+template <bool MIXED, int W>
+__device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimRegs& R, Slot& S, const InstPtrs& I, const Team<W>& T) {
+  constexpr int kStride = 32 * W;
+  const int lane = T.lane, rank = T.rank;
+  const Buoy hb = buoyancy<MIXED, W>(M, F, T, S.hydro);
+  solve_levels<MIXED, W>(M, F, S, T);
+  T.sync();
 
   // effective heads and areas, then degrees (flows.hpp:15-35)
-  for (int n = lane; n < M.nn; n += kLanes) {
+  for (int n = rank; n < M.nn; n += kStride) {
     const double v = S.vol[n];
     S.hEff[n] = v > kEmptyVolume ? S.level[n] : kNoHead;
     S.aEff[n] = v >= __ldg(M.vmax + n) ? __ldg(M.aov + n) : jmax(S.area[n], __ldg(M.amin + n));
   }
-  __syncwarp();
-  for (int n = lane; n < M.nn; n += kLanes) {
+  T.sync();
+  for (int n = rank; n < M.nn; n += kStride) {
     const int k0 = __ldg(M.incStart + n), k1 = k0 + __ldg(M.incCount + n);
     int d = 0;
     for (int k = k0; k < k1; ++k) {
@@ -542,15 +600,15 @@ __device__ __forceinline__ void warp_step(const DevModel& M, const Pose& F, SimR
     }
     S.deg[n] = d;
   }
-  __syncwarp();
-  for (int c = lane; c < M.nc; c += kLanes) {
+  T.sync();
+  for (int c = rank; c < M.nc; c += kStride) {
     double q;
     S.dV[c] = connection_flow(M, F, R.t, S, I.en, I.area, I.tOn, c, q);
     S.q[c] = q;
   }
-  __syncwarp();
+  T.sync();
   // per-node gathers in increasing connection order, then the volume update (flows.hpp:81-111)
-  for (int n = lane; n < M.nn; n += kLanes) {
+  for (int n = rank; n < M.nn; n += kStride) {
     const int k0 = __ldg(M.incStart + n), k1 = k0 + __ldg(M.incCount + n);
     double acc = 0;
     for (int k = k0; k < k1; ++k) {
@@ -571,7 +629,7 @@ __device__ __forceinline__ void warp_step(const DevModel& M, const Pose& F, SimR
   }
   double seaIn = 0;
   for (int k = 0; k < M.nsea; ++k) seaIn += S.dV[__ldg(M.sea + k)];
-  __syncwarp();
+  T.sync();
   // the excess returns to the sea in node order (flows.hpp:114-118)
   for (int n0 = 0; n0 < M.nn; n0 += kLanes) {
     const int n = n0 + lane;
@@ -585,22 +643,22 @@ __device__ __forceinline__ void warp_step(const DevModel& M, const Pose& F, SimR
   R.inflow = seaIn / M.dt;
 
   // loads (body.hpp:11-40): per-node terms in parallel, sums in node order
-  const double W = M.rho * M.g;
-  const double Fb = W * hb.V;
+  const double Wg = M.rho * M.g;
+  const double Fb = Wg * hb.V;
   const double bxw = F.R00 * hb.x + F.R01 * hb.y + F.R02 * hb.z + F.tx;
   const double byw = F.R10 * hb.x + F.R11 * hb.y + F.R12 * hb.z + F.ty;
   double tauX = (byw - M.YO) * Fb, tauY = -(bxw - M.XO) * Fb;
   double Fz = Fb - M.g * M.ms;
   double mw = 0, Iw_p = 0, Iw_r = 0;
   const int NN = M.nn;
-  for (int n = lane; n < NN; n += kLanes) {
+  for (int n = rank; n < NN; n += kStride) {
     const double V = S.vol[n];
     if (V <= 0) continue;
     const double x = S.cx[n], y = S.cy[n], z = S.cz[n];
     const double wx = F.R00 * x + F.R01 * y + F.R02 * z + F.tx - M.XO;
     const double wy = F.R10 * x + F.R11 * y + F.R12 * z + F.ty - M.YO;
     const double wz = F.R20 * x + F.R21 * y + F.R22 * z + F.tz - R.zO;
-    const double f = -W * V;
+    const double f = -Wg * V;
     const double m = M.rho * V;
     S.tmp[n] = wy * f;
     S.tmp[NN + n] = wx * f;
@@ -609,7 +667,7 @@ __device__ __forceinline__ void warp_step(const DevModel& M, const Pose& F, SimR
     S.tmp[4 * NN + n] = m * (wx * wx + wz * wz);
     S.tmp[5 * NN + n] = m * (wy * wy + wz * wz);
   }
-  __syncwarp();
+  T.sync();
   for (int n = 0; n < NN; ++n) {
     if (S.vol[n] <= 0) continue;
     tauX += S.tmp[n]; tauY -= S.tmp[NN + n]; Fz += S.tmp[2 * NN + n];
@@ -635,7 +693,8 @@ __device__ __forceinline__ void warp_step(const DevModel& M, const Pose& F, SimR
   R.Vb = hb.V; R.hullTop = hb.top; R.mw = mw;
   R.bx = hb.x; R.by = hb.y; R.bz = hb.z;
 
-  // events (events.hpp:11-38): monitors in order, marks in order, then the founder rule
+  // events (events.hpp:11-38): monitors in order, marks in order, then the founder rule; warp 0 keeps the log
+  if (T.warp == 0) {
   for (int m0 = 0; m0 < M.nmon; m0 += kLanes) {
     const int m = m0 + lane;
     bool fire = false;
@@ -672,12 +731,13 @@ __device__ __forceinline__ void warp_step(const DevModel& M, const Pose& F, SimR
       push_event(M, R, I, i0 + b, 1, lane);
     }
   }
+  }
   if (!R.foundered && (R.hullTop < M.hullTopBelow || fabs(R.pitch) > M.pitchAbsAbove || (R.Vb < M.buoyancyBelow && R.t > M.minT))) {
     R.foundered = 1;
     R.founderT = R.t;
-    push_event(M, R, I, -1, 2, lane);
+    if (T.warp == 0) push_event(M, R, I, -1, 2, lane);
   }
-  __syncwarp();
+  T.sync();
 }
 
 // Readouts at the current state (kernel/readouts.hpp:20-36): t, trim, list, water (t), inflow (t/min), draftF, draftA.

@@ -115,7 +115,10 @@ def test_perturbed_batch_equals_oracle(model, numerics, mixed):
 def test_launch_shape_does_not_change_bits(model):
     ship_p, sim_p, _, sim = model
     ref = None
-    for kw in (dict(), dict(warps_per_block=1), dict(warps_per_block=16, blocks=1), dict(steps_per_launch=777)):
+    shapes = [dict(), dict(team_warps=1, tail_team_warps=0, teams_per_block=1), dict(team_warps=1, teams_per_block=16, blocks=1),
+              dict(steps_per_launch=777), dict(team_warps=2), dict(team_warps=4), dict(team_warps=8),
+              dict(team_warps=1, tail_team_warps=4, yield_below=20), dict(team_warps=2, tail_team_warps=8, yield_below=20)]
+    for kw in shapes:
         b, _ = _perturbed_batch(ship_p, sim_p, sim, 20, "portable", 1800.0, **kw)
         b.run()
         states = np.stack([b.state(i) for i in range(20)])
