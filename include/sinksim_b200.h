@@ -162,6 +162,29 @@ int ssb_compare_results(const char* a_path, const char* b_path, uint64_t* compar
 int ssb_portable_math_host(int32_t op, const double* x, const double* y, double* out, int64_t n);
 int ssb_portable_math_device(int32_t op, const double* x, const double* y, double* out, int64_t n);
 
+/* Runs `count` instances of the batch's model without allocating any device memory, for callers that cannot call
+ * cudaMalloc at run time: a host application that owns every device allocation through its own memory pool (a
+ * calibration or control loop embedded in a larger program), or code that must not allocate once it is running.
+ * No counterpart in the reference, whose cuda::Batch allocates everything itself (engine/cuda/batch.cu:23-59).
+ *
+ * All pointers are the caller's device memory: state (count x 8 doubles: t, zO, pitch, roll, vz, wth, wph, then a
+ * 0 for the settle timer of the retire rule), vol, level, cx, cy, cz (count x N each) are read as the initial states
+ * and overwritten with the final ones; en (bytes), area, t_on (count x connections each) are the connection fields;
+ * final_readouts (count x 7) receives each instance's final readouts, steps (int64) its step count and stop_reason its
+ * stop (1 foundered, 2 t_max, 3 sink rule, 4 settle rule). Numerics, t_max and the retire rule are the batch's options;
+ * curves and traces are not recorded. `stream` is a cudaStream_t (NULL: the default stream); the call returns once the
+ * work is queued on it.
+ *
+ * The kernel's scratch (the work-queue head, the count of unfinished instances, each instance's outputs, event log,
+ * overflow and mark times) lives in a fixed 4 MiB device array of the library, which every GPU that loads the library
+ * holds until the process exits; a count whose scratch does not fit returns SSB_EINVAL with the largest count that
+ * would. The first call on a device looks up that array's device address (cudaGetSymbolAddress) and sets kernel
+ * attributes, so make it before any stream capture. Every call shares the array and clears what must start at zero;
+ * calls that overlap on the GPU race on it. The batch handle must have been created beforehand (which allocates). */
+int ssb_batch_run_noalloc(const ssb_batch* b, int32_t count, const uint8_t* en, const double* area, const double* t_on, double* state,
+                          double* vol, double* level, double* cx, double* cy, double* cz, double* final_readouts, int64_t* steps,
+                          int32_t* stop_reason, void* stream);
+
 /* Measured rate of separately rounded adds and multiplies on the device (fp64 = 1: double, 0: float), the
  * denominator of the engine's roofline; operations per second through *ops_per_s. No counterpart in the reference. */
 int ssb_measure_add_mul_peak(int32_t fp64, int32_t device, double* ops_per_s);

@@ -91,6 +91,7 @@ _SIGNATURES = {
     "ssb_portable_math_host": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64]),
     "ssb_portable_math_device": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64]),
     "ssb_measure_add_mul_peak": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+    "ssb_batch_run_noalloc": (C.c_int, [C.c_void_p, C.c_int32] + [C.c_void_p] * 13),
 }
 
 
@@ -288,6 +289,13 @@ class Batch:
 
     def save_results(self, path, sweep_path=None):
         _check(lib().ssb_batch_save_results(self._h, _b(sweep_path), _b(path)))
+
+    def run_noalloc(self, count, en, area, t_on, state, vol, level, cx, cy, cz, final_readouts, steps, stop_reason, stream=None):
+        """Runs `count` instances of this batch's model in the caller's device memory without allocating any (see
+        ssb_batch_run_noalloc in include/sinksim_b200.h). Every buffer argument is a device address (int); returns
+        once the work is queued on `stream` (a cudaStream_t as int, or None for the default stream)."""
+        _check(lib().ssb_batch_run_noalloc(self._h, count, en, area, t_on, state, vol, level, cx, cy, cz, final_readouts, steps, stop_reason,
+                                           stream))
 
 
 def run_sweep(ship_path, sim_path, sweep_path, numerics="portable32", results_path=None):

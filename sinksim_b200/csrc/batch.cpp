@@ -582,6 +582,36 @@ std::vector<int> Batch::event_ids(std::int32_t inst) const {
 
 const CompiledSim& Batch::sim() const { return I_->sim; }
 
+void Batch::run_noalloc(const NoAllocRun& run, cudaStream_t stream) const {
+  const Impl& I = *I_;
+  if (run.count < 1) throw std::invalid_argument("run_noalloc: count must be at least 1");
+  const std::size_t need = noalloc_scratch_bytes(I.dm, run.count), cap = noalloc_scratch_capacity();
+  if (need > cap)
+    throw std::invalid_argument("run_noalloc: " + std::to_string(run.count) + " instances of this model need " + std::to_string(need) +
+                                " bytes of scratch; the fixed scratch array holds " + std::to_string(cap) + " (at most " +
+                                std::to_string(run.count * (cap / need)) + " instances)");
+  if (!run.en || !run.area || !run.tOn || !run.state || !run.vol || !run.level || !run.cx || !run.cy || !run.cz || !run.finalRec || !run.steps ||
+      !run.stop)
+    throw std::invalid_argument("run_noalloc: a device pointer is NULL");
+  check(cudaSetDevice(opt_.device), "cudaSetDevice");
+  NoAllocRun r = run;
+  r.tMax = opt_.tMax;
+  r.rule = opt_.rule;
+  // one launch, teams sized so that about 16 warps per SM carry the instances
+  const int sms = I.info.multiprocessors;
+  const int fit = std::max(1, (sms * 16) / r.count);
+  r.teamWarps = fit >= 8 ? 8 : fit >= 4 ? 4 : fit >= 2 ? 2 : 1;
+  const int maxTeams = std::min(static_cast<int>(I.info.sharedPerBlockOptIn / I.layout.bytes), kMaxWarpsPerBlock / r.teamWarps);
+  r.teamsPerBlock = std::max(1, std::min(maxTeams, (r.count + sms - 1) / sms));
+  const std::size_t smem = static_cast<std::size_t>(r.teamsPerBlock) * I.layout.bytes;
+  check(configure_batch_kernel(opt_.mixedPrecision, r.teamWarps, smem), "cudaFuncSetAttribute");
+  int perSM = 0;
+  check(batch_kernel_occupancy(opt_.mixedPrecision, r.teamWarps, r.teamsPerBlock, smem, &perSM), "occupancy");
+  if (perSM < 1) throw std::runtime_error("run_noalloc: the kernel cannot be resident");
+  r.blocks = std::min((r.count + r.teamsPerBlock - 1) / r.teamsPerBlock, perSM * sms);
+  check(run_batch_noalloc(opt_.mixedPrecision, I.dm, I.layout, r, stream), "kernel launch");
+}
+
 std::vector<EventRecord> Batch::events(std::int32_t inst) const {
   const Impl& I = *I_;
   if (!I.downloaded) throw std::logic_error("Batch: result before run");

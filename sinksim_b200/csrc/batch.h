@@ -8,6 +8,9 @@
 #include <string>
 #include <vector>
 
+#include <cuda_runtime.h>
+
+#include "batch_kernel.h"
 #include "device_model.h"
 #include "model.h"
 #include "sweep.h"
@@ -105,6 +108,11 @@ class Batch {
   std::vector<int> event_kinds(std::int32_t inst) const;
   std::vector<int> event_ids(std::int32_t inst) const;  // monitor or mark index, -1 for the founder
   const CompiledSim& sim() const;
+
+  // Runs `count` instances of this batch's model with the caller's device buffers and the library's fixed scratch
+  // array: nothing is allocated on the device (see run_batch_noalloc). Numerics, tMax and the retire rule are the
+  // batch's; one launch of single- or multi-warp teams chosen from count, no curves or traces.
+  void run_noalloc(const NoAllocRun& run, cudaStream_t stream) const;
   std::vector<CurveRecord> curve(std::int32_t inst) const;  // the device records closed by the final readouts
   CurveRecord final_readouts(std::int32_t inst) const;
   Trace trace(std::int32_t inst) const;

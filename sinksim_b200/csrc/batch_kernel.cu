@@ -13,6 +13,9 @@
 // unfinished instances (atomicSub when one stops, a plain load every 64 steps).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <climits>
+
 #include "batch_kernel.h"
 #include "warp_step.cuh"
 
@@ -252,6 +255,106 @@ cudaError_t batch_kernel_occupancy(bool mixed, int teamWarps, int teamsPerBlock,
   if (!valid_team_size(teamWarps)) return cudaErrorInvalidValue;
   const int threads = teamsPerBlock * teamWarps * 32;
   return mixed ? occupancy<true>(teamWarps, threads, smemBytes, blocksPerSM) : occupancy<false>(teamWarps, threads, smemBytes, blocksPerSM);
+}
+
+// ----------------------------------------------------------------------------- the batch run without device allocation
+// Some callers cannot call cudaMalloc when they run a batch: a host application that owns every device allocation
+// through its own pool (a calibration or control loop embedded in a larger program), or code that must not allocate
+// once it is running. For them the batch kernel's scratch, the memory it needs beyond the caller's inputs and outputs
+// (the work-queue head, the count of unfinished instances, and each instance's outputs, event log, overflow and mark
+// times), lives in this fixed array instead of in buffers the engine allocates. Every GPU that loads the library
+// holds it until the process exits. All calls share it and it keeps the last call's contents, so each call clears
+// what must start at zero; two calls that overlap on the GPU (on different streams) would race on it.
+
+namespace {
+
+constexpr std::size_t kNoAllocScratchBytes = std::size_t(4) << 20;
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+void* g_scratch_address[kMaxDevices] = {};
+
+// The per-instance fields the batch kernel expects to find set before its first launch.
+__global__ void clear_noalloc_scratch(DevBatch B, int nmon, int nmark) {
+  const std::int32_t stride = gridDim.x * blockDim.x;
+  for (std::int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < B.count; i += stride) {
+    for (int k = 0; k < 7; ++k) B.out[static_cast<std::size_t>(i) * 7 + k] = 0;
+    B.evCount[i] = 0;
+    B.foundered[i] = 0;
+    B.founderT[i] = -1;
+    B.steps[i] = 0;
+    B.stop[i] = kRunning;
+    for (int m = 0; m < nmon; ++m) B.overT[static_cast<std::size_t>(i) * nmon + m] = -1;
+    for (int m = 0; m < nmark; ++m) B.markT[static_cast<std::size_t>(i) * nmark + m] = -1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *B.queue = 0;
+    *B.remaining = B.count;
+    *B.error = 0;
+  }
+}
+
+std::size_t align256(std::size_t x) { return (x + 255) & ~static_cast<std::size_t>(255); }
+
+}  // namespace
+
+std::size_t noalloc_scratch_capacity() { return kNoAllocScratchBytes; }
+
+std::size_t noalloc_scratch_bytes(const DevModel& M, int count) {
+  const auto c = static_cast<std::size_t>(count);
+  std::size_t b = align256(3 * sizeof(std::int32_t));                         // queue, remaining, error
+  b += align256(c * 7 * sizeof(double));                                        // outputs
+  b += 2 * align256(c * sizeof(std::int32_t)) + align256(c * sizeof(double));   // evCount, foundered, founderT
+  b += align256(c * M.evCap * sizeof(double)) + 2 * align256(c * M.evCap * sizeof(std::int32_t));  // event log
+  b += align256(c * std::max(M.nmon, 1) * sizeof(double)) + align256(c * std::max(M.nmark, 1) * sizeof(double));
+  return b;
+}
+
+cudaError_t run_batch_noalloc(bool mixed, const DevModel& M, const SlotLayout& L, const NoAllocRun& r, cudaStream_t stream) {
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return e;
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (!g_scratch_address[device]) {
+    // set-up, once per device with that device current: the host-side name of the array is not a device address
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_scratch_address[device] = p;
+  }
+  if (noalloc_scratch_bytes(M, r.count) > kNoAllocScratchBytes) return cudaErrorMemoryAllocation;
+  auto* base = static_cast<unsigned char*>(g_scratch_address[device]);
+  std::size_t off = 0;
+  auto carve = [&](std::size_t bytes) { unsigned char* p = base + off; off += align256(bytes); return p; };
+  const auto c = static_cast<std::size_t>(r.count);
+  DevBatch B{};
+  B.count = r.count;
+  B.queue = reinterpret_cast<std::int32_t*>(carve(3 * sizeof(std::int32_t)));
+  B.remaining = B.queue + 1;
+  B.error = B.queue + 2;
+  B.out = reinterpret_cast<double*>(carve(c * 7 * sizeof(double)));
+  B.evCount = reinterpret_cast<std::int32_t*>(carve(c * sizeof(std::int32_t)));
+  B.foundered = reinterpret_cast<std::int32_t*>(carve(c * sizeof(std::int32_t)));
+  B.founderT = reinterpret_cast<double*>(carve(c * sizeof(double)));
+  B.evT = reinterpret_cast<double*>(carve(c * M.evCap * sizeof(double)));
+  B.evId = reinterpret_cast<std::int32_t*>(carve(c * M.evCap * sizeof(std::int32_t)));
+  B.evKind = reinterpret_cast<std::int32_t*>(carve(c * M.evCap * sizeof(std::int32_t)));
+  B.overT = reinterpret_cast<double*>(carve(c * std::max(M.nmon, 1) * sizeof(double)));
+  B.markT = reinterpret_cast<double*>(carve(c * std::max(M.nmark, 1) * sizeof(double)));
+  // the caller's inputs and outputs
+  B.en = r.en; B.area = r.area; B.tOn = r.tOn;
+  B.st = r.state; B.vol = r.vol; B.level = r.level; B.cx = r.cx; B.cy = r.cy; B.cz = r.cz;
+  B.finalRec = r.finalRec; B.steps = r.steps; B.stop = r.stop;
+  B.curveEvery = 0; B.traced = 0;
+  B.tMax = r.tMax;
+  B.maxSteps = LLONG_MAX;
+  B.firstLaunch = 1;
+  B.rule = r.rule;
+  B.yieldBelow = 0;
+  clear_noalloc_scratch<<<64, 256, 0, stream>>>(B, M.nmon, M.nmark);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_batch_kernel(mixed, r.teamWarps, M, B, L, r.blocks, r.teamsPerBlock, stream);
 }
 
 }  // namespace ssb

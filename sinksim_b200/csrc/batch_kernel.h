@@ -18,4 +18,24 @@ cudaError_t launch_batch_kernel(bool mixed, int teamWarps, const DevModel& M, co
                                 int teamsPerBlock, cudaStream_t stream);
 cudaError_t batch_kernel_occupancy(bool mixed, int teamWarps, int teamsPerBlock, std::size_t smemBytes, int* blocksPerSM);
 
+// A batch run whose scratch lives in a fixed device array of the library (see batch_kernel.cu); every pointer here
+// is the caller's device memory. state is count x 8 (t, zO, pitch, roll, vz, wth, wph, and the settle timer, which
+// must start at 0); vol .. cz are count x nodes; en, area, tOn count x connections; finalRec count x 7; steps and
+// stop count (cleared by the call). In and out: state, vol, level, cx, cy, cz.
+struct NoAllocRun {
+  std::int32_t count;
+  const std::uint8_t* en;
+  const double *area, *tOn;
+  double *state, *vol, *level, *cx, *cy, *cz, *finalRec;
+  long long* steps;
+  std::int32_t* stop;
+  double tMax;
+  RetireRule rule;
+  int teamWarps, teamsPerBlock, blocks;
+};
+std::size_t noalloc_scratch_capacity();
+std::size_t noalloc_scratch_bytes(const DevModel& M, int count);
+// cudaErrorMemoryAllocation when count instances need more scratch than the fixed array holds.
+cudaError_t run_batch_noalloc(bool mixed, const DevModel& M, const SlotLayout& L, const NoAllocRun& run, cudaStream_t stream);
+
 }  // namespace ssb

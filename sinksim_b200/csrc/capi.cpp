@@ -386,6 +386,22 @@ int ssb_portable_math_device(int32_t op, const double* x, const double* y, doubl
   });
 }
 
+int ssb_batch_run_noalloc(const ssb_batch* b, int32_t count, const uint8_t* en, const double* area, const double* t_on, double* state,
+                          double* vol, double* level, double* cx, double* cy, double* cz, double* final_readouts, int64_t* steps,
+                          int32_t* stop_reason, void* stream) {
+  return guard([&] {
+    need(b, "batch");
+    ssb::NoAllocRun r{};
+    r.count = count;
+    r.en = en; r.area = area; r.tOn = t_on;
+    r.state = state; r.vol = vol; r.level = level; r.cx = cx; r.cy = cy; r.cz = cz;
+    r.finalRec = final_readouts;
+    r.steps = reinterpret_cast<long long*>(steps);
+    r.stop = stop_reason;
+    b->batch->run_noalloc(r, static_cast<cudaStream_t>(stream));
+  });
+}
+
 int ssb_measure_add_mul_peak(int32_t fp64, int32_t device, double* ops_per_s) {
   return guard([&] {
     need(ops_per_s, "ops_per_s");
