@@ -57,6 +57,10 @@ typedef struct ssb_batch_options {
    * rule_settle seconds ("settle"). It never changes the physics. */
   int32_t rule_enabled;
   double rule_pitch, rule_x, rule_y, rule_z, rule_wth, rule_settle;
+  /* the reference's calm rule of Simulation::run (engine/src/simulation.cpp:179-182), a sweep's "stopWhenStable":
+   * after 1,800 s an instance stops once |inflow| < 0.02, |pitch rate| < 1e-5 and |heave rate| < 1e-3 have held for
+   * more than 1,200 s (stop reason 5). Exclusive with the retire rule. */
+  int32_t stop_when_stable;
 } ssb_batch_options;
 
 typedef struct ssb_device_info {
@@ -69,7 +73,7 @@ typedef struct ssb_device_info {
 /* Summary of one instance after a run: engine/include/sinksim/cuda/batch.hpp:45-54 (InstanceResult). */
 typedef struct ssb_instance_summary {
   int32_t foundered;
-  int32_t stop_reason; /* 1 foundered, 2 tMax, 3 sink rule, 4 settle rule, 0 still running */
+  int32_t stop_reason; /* 1 foundered, 2 tMax, 3 sink rule, 4 settle rule, 5 stable (calm rule), 0 still running */
   double founder_t, t_end;
   int64_t steps;
   int32_t event_count;

@@ -22,9 +22,9 @@ namespace {
 
 int run_sweep(const cli::Args& args, std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, bool mixed, const DeviceInfo& info) {
   const Sweep sw = load_sweep(args.get("sweep", ""), sim);
-  if (sw.stopWhenStable) throw std::runtime_error("stopWhenStable is not supported on the GPU; run the sweep with the CPU engine");
   if (sw.instances.empty()) throw std::runtime_error("the sweep has no instances");
   BatchOptions opt;
+  opt.stopWhenStable = sw.stopWhenStable;  // the reference's GPU runner refused these sweeps; this engine runs them
   opt.count = static_cast<std::int32_t>(sw.instances.size());
   opt.mixedPrecision = mixed;
   opt.tracedInstances = 0;

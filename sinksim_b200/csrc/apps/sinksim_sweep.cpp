@@ -51,7 +51,6 @@ int main(int argc, char** argv) {
     const CompiledSim sim = load_sim(args.positional[1]);
     check_pairing(*ship, sim);
     const Sweep sw = load_sweep(args.positional[2], sim);
-    if (sw.stopWhenStable) throw std::runtime_error("stopWhenStable is not supported on the GPU engine");
     if (sw.instances.empty()) throw std::runtime_error("the sweep has no instances");
     std::printf("sweep of %zu instances on %s / %s, numerics %s, tMax %s, curve every %g s, GPU\n", sw.instances.size(), ship->id.c_str(), sim.id.c_str(),
                 numerics.c_str(), cli::minutes(sw.tMax).c_str(), sw.every);
@@ -61,6 +60,7 @@ int main(int argc, char** argv) {
     opt.tracedInstances = 0;
     opt.tMax = sw.tMax;
     opt.curveEvery = sw.every;
+    opt.stopWhenStable = sw.stopWhenStable;
     Batch batch(ship, sim, opt);
     batch.apply_sweep(sw);
     const double s = batch.run();

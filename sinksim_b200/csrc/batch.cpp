@@ -155,6 +155,7 @@ struct Batch::Impl {
     b.maxSteps = maxSteps;
     b.firstLaunch = firstLaunch;
     b.rule = opt.rule;
+    b.stopWhenStable = opt.stopWhenStable ? 1 : 0;
     b.queue = queue.get();
     b.error = error.get();
     b.remaining = remaining.get();
@@ -171,6 +172,7 @@ Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, c
   if (opt_.tracedInstances > opt_.count) opt_.tracedInstances = opt_.count;
   if (opt_.tracedInstances < 0) opt_.tracedInstances = 0;
   if (opt_.tracedInstances > 0 && !(opt_.sampleEvery > 0)) throw std::invalid_argument("Batch: sampleEvery must be positive");
+  if (opt_.stopWhenStable && opt_.rule.enabled) throw std::invalid_argument("Batch: stopWhenStable and the retire rule are exclusive");
   std::string why;
   if (!cuda_available(&why)) throw std::runtime_error("Batch: " + why);
   check(cudaSetDevice(opt_.device), "cudaSetDevice");

@@ -32,6 +32,7 @@ struct BatchOptions {
   std::int32_t yieldBelow = -1;    // main phase pauses once at most this many instances remain; -1: the tail grid's size
   std::int32_t blocks = 0;         // 0: persistent grid sized to the device
   RetireRule rule{};
+  bool stopWhenStable = false;     // the reference's calm rule (a sweep's "stopWhenStable"); exclusive with `rule`
   int device = 0;
 };
 

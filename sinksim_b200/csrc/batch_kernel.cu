@@ -135,6 +135,10 @@ __device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
         nextSample += B.sampleEvery;
       }
     }
+    if (B.stopWhenStable && R.t > 1800) {
+      R.calm = (fabs(R.inflow) < 0.02 && fabs(R.wth) < 1e-5 && fabs(R.vz) < 1e-3) ? R.calm + M.dt : 0;
+      if (R.calm > 1200) { stop = kStable; break; }
+    }
     if (B.rule.enabled) {
       const double zp = world_z(F, B.rule.xDeck, B.rule.yDeck, B.rule.zDeck);
       const double zs = world_z(F, B.rule.xDeck, -B.rule.yDeck, B.rule.zDeck);

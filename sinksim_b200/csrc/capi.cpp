@@ -89,6 +89,7 @@ ssb::BatchOptions to_options(const ssb_batch_options& o) {
   b.rule.xDeck = o.rule_x; b.rule.yDeck = o.rule_y; b.rule.zDeck = o.rule_z;
   b.rule.wthLimit = o.rule_wth;
   b.rule.settleTime = o.rule_settle;
+  b.stopWhenStable = o.stop_when_stable != 0;
   return b;
 }
 
@@ -333,9 +334,9 @@ int ssb_run_sweep(const char* ship_path, const char* sim_path, const char* sweep
     const ssb::CompiledSim sim = ssb::load_sim(sim_path);
     ssb::check_pairing(*ship, sim);
     const ssb::Sweep sw = ssb::load_sweep(sweep_path, sim);
-    if (sw.stopWhenStable) throw Unsupported("stopWhenStable is not supported on the GPU; run the sweep with sinksim_sweep");
     if (sw.instances.empty()) throw std::invalid_argument("the sweep has no instances");
     ssb::BatchOptions opt;
+    opt.stopWhenStable = sw.stopWhenStable;
     opt.count = static_cast<std::int32_t>(sw.instances.size());
     opt.mixedPrecision = nm == "portable32";
     opt.tracedInstances = 0;

@@ -84,8 +84,9 @@ struct RetireRule {
   double settleTime;           // s: ... for this long
 };
 
-// Why an instance stopped.
-enum StopReason : std::int32_t { kRunning = 0, kFoundered = 1, kTimeLimit = 2, kSinkRule = 3, kSettleRule = 4 };
+// Why an instance stopped. kStable: the reference's "stop when stable" calm rule of Simulation::run
+// (engine/src/simulation.cpp:179-182), which its GPU runner refused (apps/sinksim_cuda_run.cpp:28).
+enum StopReason : std::int32_t { kRunning = 0, kFoundered = 1, kTimeLimit = 2, kSinkRule = 3, kSettleRule = 4, kStable = 5 };
 
 struct DevBatch {
   std::int32_t count;
@@ -127,6 +128,9 @@ struct DevBatch {
   long long maxSteps;          // steps per instance per launch
   std::int32_t firstLaunch;
   RetireRule rule;
+  // the reference's calm rule: after 1,800 s, stop once |inflow| < 0.02, |pitch rate| < 1e-5 and |heave rate| < 1e-3
+  // have held for more than 1,200 s; exclusive with `rule` (both keep their timer in state slot 7)
+  std::int32_t stopWhenStable;
   std::int32_t* queue;         // work-queue head (atomic), reset to 0 before each launch
   std::int32_t* error;         // first error code seen by any warp (0 = none)
   // adaptive team size: instances not yet stopped (atomic, set to count before the first launch); a launch with
