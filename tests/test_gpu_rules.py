@@ -61,7 +61,8 @@ def test_stop_when_stable_sweep_equals_reference_sweep(tmp_path):
     ship_p, sim_p = titanic()
     sweep = {"format": "sinksim.sweep", "formatVersion": 1, "ship": "titanic64", "sim": "titanic", "tMax": 5 * 3600, "every": 30,
              "stopWhenStable": True,
-             "instances": [{"id": f"breach-{f}", "scale": {"breach": f}} for f in (0.02, 0.05, 0.1, 0.3, 1.0)]}
+             "instances": [{"id": f"breach-{f}", "scale": {"breach": f}} for f in (0.0, 0.001, 0.005, 0.3, 1.0)] +
+                          [{"id": "breaches-closed", "connections": [{"kind": "breach", "enabled": False}]}]}
     sp = tmp_path / "stable.sweep.json"
     sp.write_text(json.dumps(sweep))
     cpu, gpu = str(tmp_path / "cpu.json"), str(tmp_path / "gpu.json")
