@@ -103,7 +103,26 @@ struct Batch::Impl {
   MonitorLists mons;
   DeviceInfo info;
   std::int32_t NN = 0, NC = 0, NG = 0, nmon = 0, nmark = 0, evCap = 0, maxGroup = 0, recSize = 0, maxSamples = 0, curveMax = 0;
-  SlotLayout layout{};
+  // The shared-memory slot of one simulation stepped by a team of W warps: per-node state and scratch, per-connection
+  // dV and q, one group-pass buffer per warp, the buoyancy tree results. The loads' sixth scratch column reuses dV
+  // when there are at least as many connections as nodes.
+  SlotLayout layout_for(int W) const {
+    SlotLayout L{};
+    std::uint32_t off = 0;
+    const std::size_t nb = sizeof(double) * static_cast<std::size_t>(NN);
+    L.vol = take(off, nb); L.level = take(off, nb); L.cx = take(off, nb); L.cy = take(off, nb); L.cz = take(off, nb);
+    L.area = take(off, nb); L.zmax = take(off, nb); L.hEff = take(off, nb); L.aEff = take(off, nb); L.acc = take(off, nb);
+    L.deg = take(off, sizeof(std::int32_t) * static_cast<std::size_t>(NN));
+    L.dV = take(off, sizeof(double) * static_cast<std::size_t>(std::max(NC, 1)));
+    L.q = take(off, sizeof(double) * static_cast<std::size_t>(std::max(NC, 1)));
+    L.tmp = NC >= NN ? kSlotAliasDV : take(off, nb);
+    L.passes = take(off, 7 * sizeof(double) * static_cast<std::size_t>(maxGroup) * static_cast<std::size_t>(W));
+    L.hydro = take(off, 8 * 5 * sizeof(double));
+    L.misc = take(off, 2 * sizeof(std::int32_t));
+    L.merged = take(off, static_cast<std::size_t>(std::max(NG, 1)));
+    L.bytes = off;
+    return L;
+  }
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
@@ -188,34 +207,22 @@ Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, c
   I.maxSamples = opt_.tracedInstances > 0 ? static_cast<std::int32_t>(std::floor(opt_.tMax / opt_.sampleEvery)) + 2 : 0;
   I.curveMax = opt_.curveEvery > 0 ? static_cast<std::int32_t>(std::floor(opt_.tMax / opt_.curveEvery)) + 2 : 0;
 
-  // shared-memory slot of one simulation
-  SlotLayout& L = I.layout;
-  std::uint32_t off = 0;
-  const std::size_t nb = sizeof(double) * static_cast<std::size_t>(I.NN);
-  L.vol = take(off, nb); L.level = take(off, nb); L.cx = take(off, nb); L.cy = take(off, nb); L.cz = take(off, nb);
-  L.area = take(off, nb); L.zmax = take(off, nb); L.hEff = take(off, nb); L.aEff = take(off, nb); L.acc = take(off, nb);
-  L.deg = take(off, sizeof(std::int32_t) * static_cast<std::size_t>(I.NN));
-  L.dV = take(off, sizeof(double) * static_cast<std::size_t>(std::max(I.NC, 1)));
-  L.q = take(off, sizeof(double) * static_cast<std::size_t>(std::max(I.NC, 1)));
-  L.tmp = take(off, 6 * nb);
-  L.passes = take(off, 7 * sizeof(double) * static_cast<std::size_t>(I.maxGroup) * 8);  // per warp of a team of up to 8
-  L.hydro = take(off, 8 * 5 * sizeof(double));
-  L.misc = take(off, 2 * sizeof(std::int32_t));
-  L.merged = take(off, static_cast<std::size_t>(std::max(I.NG, 1)));
-  L.bytes = off;
-  cfg_.slotBytes = L.bytes;
-
   // launch shape. Teams of W warps; a slot of shared memory per team; persistent grids sized to the device.
   // Main phase: single-warp teams when the batch fills the device (the most simulations per SM), larger teams when it
-  // does not. Tail phase: when at most one tail grid's worth of instances remains, they resume in 8-warp teams.
+  // does not. Later phases: when the unfinished instances fit the resident teams of twice the size, they resume there.
   const std::size_t optin = I.info.sharedPerBlockOptIn;
   const int sms = I.info.multiprocessors;
-  if (L.bytes > optin)
-    throw std::runtime_error("Batch: one simulation needs " + std::to_string(L.bytes) + " bytes of shared memory, the device allows " + std::to_string(optin) + " per block");
+  cfg_.slotBytes = I.layout_for(1).bytes;
+  if (cfg_.slotBytes > optin)
+    throw std::runtime_error("Batch: one simulation needs " + std::to_string(cfg_.slotBytes) + " bytes of shared memory, the device allows " +
+                             std::to_string(optin) + " per block");
   auto plan = [&](int W, int teamsReq, int count) {
     PhaseConfig p;
     if (!valid_team_size(W)) throw std::invalid_argument("Batch: warps per simulation must be 1, 2, 4 or 8");
     p.teamWarps = W;
+    p.layout = I.layout_for(W);
+    const SlotLayout& L = p.layout;
+    if (L.bytes > optin) throw std::runtime_error("Batch: a " + std::to_string(W) + "-warp simulation needs more shared memory than a block has");
     const int maxTeams = std::min(static_cast<int>(optin / L.bytes), kMaxWarpsPerBlock / W);
     int tpb = teamsReq > 0 ? teamsReq : std::max(1, std::min(maxTeams, (count + sms - 1) / sms));
     tpb = std::max(1, std::min(tpb, maxTeams));
@@ -350,7 +357,7 @@ Batch::~Batch() {
 
 std::int32_t Batch::nodes() const { return I_->NN; }
 std::int32_t Batch::connections() const { return I_->NC; }
-std::size_t Batch::slot_bytes() const { return I_->layout.bytes; }
+std::size_t Batch::slot_bytes() const { return cfg_.slotBytes; }
 
 static void check_inst(const BatchOptions& o, std::int32_t inst) {
   if (inst < 0 || inst >= o.count) throw std::out_of_range("Batch: instance " + std::to_string(inst) + " out of range");
@@ -458,7 +465,7 @@ float Batch::launch() {
       check(cudaMemsetAsync(I.queue.get(), 0, sizeof(std::int32_t), s), "memset");
       DevBatch db = I.devBatch(opt_, maxSteps, first);
       db.yieldBelow = p.yieldBelow;
-      check(launch_batch_kernel(opt_.mixedPrecision, p.teamWarps, I.dm, db, I.layout, p.blocks, p.teamsPerBlock, s), "kernel launch");
+      check(launch_batch_kernel(opt_.mixedPrecision, p.teamWarps, I.dm, db, p.layout, p.blocks, p.teamsPerBlock, s), "kernel launch");
       first = 0;
     }
     if (opt_.stepsPerLaunch <= 0) break;
@@ -603,15 +610,16 @@ void Batch::run_noalloc(const NoAllocRun& run, cudaStream_t stream) const {
   const int sms = I.info.multiprocessors;
   const int fit = std::max(1, (sms * 16) / r.count);
   r.teamWarps = fit >= 8 ? 8 : fit >= 4 ? 4 : fit >= 2 ? 2 : 1;
-  const int maxTeams = std::min(static_cast<int>(I.info.sharedPerBlockOptIn / I.layout.bytes), kMaxWarpsPerBlock / r.teamWarps);
+  const SlotLayout L = I.layout_for(r.teamWarps);
+  const int maxTeams = std::min(static_cast<int>(I.info.sharedPerBlockOptIn / L.bytes), kMaxWarpsPerBlock / r.teamWarps);
   r.teamsPerBlock = std::max(1, std::min(maxTeams, (r.count + sms - 1) / sms));
-  const std::size_t smem = static_cast<std::size_t>(r.teamsPerBlock) * I.layout.bytes;
+  const std::size_t smem = static_cast<std::size_t>(r.teamsPerBlock) * L.bytes;
   check(configure_batch_kernel(opt_.mixedPrecision, r.teamWarps, smem), "cudaFuncSetAttribute");
   int perSM = 0;
   check(batch_kernel_occupancy(opt_.mixedPrecision, r.teamWarps, r.teamsPerBlock, smem, &perSM), "occupancy");
   if (perSM < 1) throw std::runtime_error("run_noalloc: the kernel cannot be resident");
   r.blocks = std::min((r.count + r.teamsPerBlock - 1) / r.teamsPerBlock, perSM * sms);
-  check(run_batch_noalloc(opt_.mixedPrecision, I.dm, I.layout, r, stream), "kernel launch");
+  check(run_batch_noalloc(opt_.mixedPrecision, I.dm, L, r, stream), "kernel launch");
 }
 
 std::vector<EventRecord> Batch::events(std::int32_t inst) const {

@@ -50,6 +50,7 @@ DeviceInfo device_info(int device);
 struct PhaseConfig {
   int teamWarps = 0, teamsPerBlock = 0, blocks = 0, blocksPerSM = 0;
   int yieldBelow = 0;  // the phase pauses its instances once at most this many remain (0: never)
+  SlotLayout layout{};
 };
 
 // Launch phases in order. Each phase's teams are twice the size of the previous phase's; a phase hands its

@@ -143,8 +143,11 @@ struct DevBatch {
 // Byte offsets of one simulation slot (one team of warps) in dynamic shared memory; `bytes` is the slot stride.
 // passes holds maxGroup node-pass results per warp of the team; hydro the eight buoyancy tree results; misc two
 // ints the team broadcasts (the claimed instance, the yield decision).
+// tmp is the sixth column of the loads' per-node terms (the other five reuse area, zmax, hEff, aEff and acc, which
+// are dead by then); kSlotAliasDV places it on dV when there are at least as many connections as nodes.
 struct SlotLayout {
   std::uint32_t vol, level, cx, cy, cz, area, zmax, hEff, aEff, acc, deg, dV, q, tmp, passes, hydro, misc, merged, bytes;
 };
+constexpr std::uint32_t kSlotAliasDV = 0xFFFFFFFFu;
 
 }  // namespace ssb

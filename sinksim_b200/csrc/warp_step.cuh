@@ -245,6 +245,12 @@ __device__ __forceinline__ SegPartial<T> segment_partial(const typename Vec2<T>:
                                                          int first, int end, T R20, T R21, T R22, T tz, T iR, T h) {
   SegPartial<T> p{T(0), T(0), T(0), T(0), T(0), T(1e9), T(-1e9)};
   int j = first;
+#if defined(SSB_SEGMENTS_ONE_AT_A_TIME)
+  for (; j < end; j += kLanes) {
+    const auto a0 = __ldg(xy + j), b0 = __ldg(ab + j);
+    clip_segment<T>(a0.x, a0.y, b0.x, b0.y, __ldg(area + j), R20, R21, R22, tz, iR, h, p);
+  }
+#endif
   for (; j + kLanes < end; j += 2 * kLanes) {
     const auto a0 = __ldg(xy + j), b0 = __ldg(ab + j), a1 = __ldg(xy + j + kLanes), b1 = __ldg(ab + j + kLanes);
     const T A0 = __ldg(area + j), A1 = __ldg(area + j + kLanes);
@@ -258,35 +264,40 @@ __device__ __forceinline__ SegPartial<T> segment_partial(const typename Vec2<T>:
   return p;
 }
 
+// The node pass of node n at world level h: the lane partials, the butterfly tree and the permeability scaling
+// (hydro.hpp:295-316 / 338-349). The level solvers call it from seven places: inlined, the copies crowd the
+// instruction cache; out of line, the caller's live registers spill around each call. Measured on B200 (2,368
+// titanic64 instances, single-warp teams): inlined 9.4 M steps/s, out of line 8.1 M.
+#ifndef SSB_NODE_PASS_LINKAGE
+#define SSB_NODE_PASS_LINKAGE __forceinline__
+#endif
+template <class T>
+__device__ SSB_NODE_PASS_LINKAGE PassR node_pass_body(const int* segStart, const int* segCount, const double* muArr, const typename Vec2<T>::type* xy,
+                                             const typename Vec2<T>::type* ab, const T* area, T R20, T R21, T R22, T tz, T iR, double iRd,
+                                             int n, double h, int lane) {
+  const int s0 = __ldg(segStart + n), s1 = s0 + __ldg(segCount + n);
+  SegPartial<T> p = segment_partial<T>(xy, ab, area, s0 + lane, s1, R20, R21, R22, tz, iR, static_cast<T>(h));
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    p.vol = bsum(p.vol, off); p.dv = bsum(p.dv, off); p.mx = bsum(p.mx, off); p.my = bsum(p.my, off); p.mz = bsum(p.mz, off);
+    p.zmin = bmin(p.zmin, off, lane); p.zmax = bmax(p.zmax, off, lane);
+  }
+  const double mu = __ldg(muArr + n);
+  PassR r;
+  r.vol = static_cast<double>(p.vol) * mu;
+  r.dv = static_cast<double>(p.dv) * mu * iRd;
+  r.mx = static_cast<double>(p.mx) * mu; r.my = static_cast<double>(p.my) * mu; r.mz = static_cast<double>(p.mz) * mu;
+  r.zmin = static_cast<double>(p.zmin); r.zmax = static_cast<double>(p.zmax);
+  return r;
+}
+
 template <bool MIXED>
 __device__ __forceinline__ PassR node_pass(const DevModel& M, const Pose& F, int n, double h, int lane) {
-  const int s0 = __ldg(M.segStart + n), s1 = s0 + __ldg(M.segCount + n);
-  double vol, dv, mx, my, mz, zmin, zmax;
-  if constexpr (!MIXED) {
-    SegPartial<double> p = segment_partial<double>(M.segXY, M.segLH, M.segAr, s0 + lane, s1, F.R20, F.R21, F.R22, F.tz, F.iR, h);
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      p.vol = bsum(p.vol, off); p.dv = bsum(p.dv, off); p.mx = bsum(p.mx, off); p.my = bsum(p.my, off); p.mz = bsum(p.mz, off);
-      p.zmin = bmin(p.zmin, off, lane); p.zmax = bmax(p.zmax, off, lane);
-    }
-    vol = p.vol; dv = p.dv; mx = p.mx; my = p.my; mz = p.mz; zmin = p.zmin; zmax = p.zmax;
-  } else {
-    SegPartial<float> p = segment_partial<float>(M.segXYf, M.segLHf, M.segArf, s0 + lane, s1, F.fR20, F.fR21, F.fR22, F.ftz, F.fiR,
-                                                 static_cast<float>(h));
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      p.vol = bsum(p.vol, off); p.dv = bsum(p.dv, off); p.mx = bsum(p.mx, off); p.my = bsum(p.my, off); p.mz = bsum(p.mz, off);
-      p.zmin = bmin(p.zmin, off, lane); p.zmax = bmax(p.zmax, off, lane);
-    }
-    vol = p.vol; dv = p.dv; mx = p.mx; my = p.my; mz = p.mz; zmin = p.zmin; zmax = p.zmax;
-  }
-  const double mu = __ldg(M.mu + n);
-  PassR r;
-  r.vol = vol * mu;
-  r.dv = dv * mu * F.iR;
-  r.mx = mx * mu; r.my = my * mu; r.mz = mz * mu;
-  r.zmin = zmin; r.zmax = zmax;
-  return r;
+  if constexpr (!MIXED)
+    return node_pass_body<double>(M.segStart, M.segCount, M.mu, M.segXY, M.segLH, M.segAr, F.R20, F.R21, F.R22, F.tz, F.iR, F.iR, n, h, lane);
+  else
+    return node_pass_body<float>(M.segStart, M.segCount, M.mu, M.segXYf, M.segLHf, M.segArf, F.fR20, F.fR21, F.fR22, F.ftz, F.fiR, F.iR, n, h,
+                                 lane);
 }
 
 // ----------------------------------------------------------------------------- per-warp view of the slot in shared memory
@@ -313,7 +324,7 @@ __device__ __forceinline__ Slot carve_slot(unsigned char* base, const SlotLayout
   s.acc = reinterpret_cast<double*>(base + L.acc);
   s.dV = reinterpret_cast<double*>(base + L.dV);
   s.q = reinterpret_cast<double*>(base + L.q);
-  s.tmp = reinterpret_cast<double*>(base + L.tmp);
+  s.tmp = L.tmp == kSlotAliasDV ? s.dV : reinterpret_cast<double*>(base + L.tmp);
   s.deg = reinterpret_cast<int*>(base + L.deg);
   s.hydro = reinterpret_cast<double*>(base + L.hydro);
   s.misc = reinterpret_cast<int*>(base + L.misc);
@@ -641,8 +652,16 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
     }
   }
   R.inflow = seaIn / M.dt;
+  // the loads' per-node terms overwrite area, zmax, hEff, aEff, acc and dV, all read for the last time above
+  T.sync();
 
   // loads (body.hpp:11-40): per-node terms in parallel, sums in node order
+  double* const t0 = S.area;
+  double* const t1 = S.zmax;
+  double* const t2 = S.hEff;
+  double* const t3 = S.aEff;
+  double* const t4 = S.acc;
+  double* const t5 = S.tmp;
   const double Wg = M.rho * M.g;
   const double Fb = Wg * hb.V;
   const double bxw = F.R00 * hb.x + F.R01 * hb.y + F.R02 * hb.z + F.tx;
@@ -660,20 +679,20 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
     const double wz = F.R20 * x + F.R21 * y + F.R22 * z + F.tz - R.zO;
     const double f = -Wg * V;
     const double m = M.rho * V;
-    S.tmp[n] = wy * f;
-    S.tmp[NN + n] = wx * f;
-    S.tmp[2 * NN + n] = f;
-    S.tmp[3 * NN + n] = m;
-    S.tmp[4 * NN + n] = m * (wx * wx + wz * wz);
-    S.tmp[5 * NN + n] = m * (wy * wy + wz * wz);
+    t0[n] = wy * f;
+    t1[n] = wx * f;
+    t2[n] = f;
+    t3[n] = m;
+    t4[n] = m * (wx * wx + wz * wz);
+    t5[n] = m * (wy * wy + wz * wz);
   }
   T.sync();
   for (int n = 0; n < NN; ++n) {
     if (S.vol[n] <= 0) continue;
-    tauX += S.tmp[n]; tauY -= S.tmp[NN + n]; Fz += S.tmp[2 * NN + n];
-    mw += S.tmp[3 * NN + n];
-    Iw_p += S.tmp[4 * NN + n];
-    Iw_r += S.tmp[5 * NN + n];
+    tauX += t0[n]; tauY -= t1[n]; Fz += t2[n];
+    mw += t3[n];
+    Iw_p += t4[n];
+    Iw_r += t5[n];
   }
   const double Mth = tauY, Mph = tauX * F.cth;
   // integrate (body.hpp:42-57)
