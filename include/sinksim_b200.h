@@ -49,7 +49,7 @@ typedef struct ssb_batch_options {
   int32_t tail_team_warps;   /* warps per simulation once few instances remain: 0 no tail phase, -1 chosen */
   int32_t teams_per_block;   /* simulations per block in the main phase; 0: chosen */
   int32_t yield_below;       /* the main phase hands its instances to the tail phase once at most this many remain;
-                                -1: the tail grid's capacity */
+                                -1: from handover_factor */
   int32_t blocks;            /* main-phase grid size; 0: persistent grid sized to the device */
   int32_t device;            /* CUDA device ordinal */
   /* extra retire rule (disabled when rule_enabled == 0): an instance stops once |pitch| > rule_pitch and the deck
@@ -61,6 +61,9 @@ typedef struct ssb_batch_options {
    * after 1,800 s an instance stops once |inflow| < 0.02, |pitch rate| < 1e-5 and |heave rate| < 1e-3 have held for
    * more than 1,200 s (stop reason 5). Exclusive with the retire rule. */
   int32_t stop_when_stable;
+  /* a launch phase hands its unfinished instances to the next (twice the warps per simulation) once they number at
+   * most this multiple of the next phase's resident simulations; 0: the default (2) */
+  double handover_factor;
 } ssb_batch_options;
 
 typedef struct ssb_device_info {

@@ -35,7 +35,7 @@ class _Options(C.Structure):
                 ("team_warps", C.c_int32), ("tail_team_warps", C.c_int32), ("teams_per_block", C.c_int32), ("yield_below", C.c_int32),
                 ("blocks", C.c_int32), ("device", C.c_int32), ("rule_enabled", C.c_int32),
                 ("rule_pitch", C.c_double), ("rule_x", C.c_double), ("rule_y", C.c_double), ("rule_z", C.c_double),
-                ("rule_wth", C.c_double), ("rule_settle", C.c_double), ("stop_when_stable", C.c_int32)]
+                ("rule_wth", C.c_double), ("rule_settle", C.c_double), ("stop_when_stable", C.c_int32), ("handover_factor", C.c_double)]
 
 
 class _DeviceInfo(C.Structure):
@@ -159,7 +159,7 @@ class Batch:
 
     def __init__(self, ship_path, sim_path, count=1, numerics="portable32", traced_instances=0, dense_steps=400, sample_every=60.0,
                  curve_every=0.0, t_max=5 * 3600.0, steps_per_launch=0, team_warps=0, tail_team_warps=-1, teams_per_block=0, yield_below=-1,
-                 blocks=0, device=0, rule=None, stop_when_stable=False):
+                 blocks=0, device=0, rule=None, stop_when_stable=False, handover_factor=0.0):
         if numerics not in NUMERICS:
             raise SinksimError(-4, f"numerics {numerics!r} is not available on the GPU (portable or portable32)")
         o = _Options()
@@ -169,6 +169,7 @@ class Batch:
         o.team_warps, o.tail_team_warps, o.teams_per_block, o.yield_below = team_warps, tail_team_warps, teams_per_block, yield_below
         o.blocks, o.device = blocks, device
         o.stop_when_stable = 1 if stop_when_stable else 0
+        o.handover_factor = handover_factor
         if rule:
             o.rule_enabled = 1
             o.rule_pitch, o.rule_x, o.rule_y, o.rule_z = rule["pitch"], rule["x"], rule["y"], rule["z"]

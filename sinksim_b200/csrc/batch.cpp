@@ -236,8 +236,12 @@ Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, c
   };
   int W1 = opt_.teamWarps;
   if (W1 <= 0) {
-    const int fit = std::max(1, (sms * 16) / std::max(opt_.count, 1));  // about 16 warps per SM in all
-    W1 = fit >= 8 ? 8 : fit >= 4 ? 4 : fit >= 2 ? 2 : 1;
+    // About 16 warps per SM in all. A batch that all fits at once in single-warp teams runs there; a larger one
+    // starts in two-warp teams: with 16 slots per SM the slots leave too little of the SM's shared storage to L1 for
+    // the geometry that every simulation reads (uneven titanic64 batches of 4096 and 8192 instances on B200: 7.3 and
+    // 7.8 M steps/s in two-warp teams, 6.4 and 5.5 M in single-warp teams).
+    const int fit = (sms * 16) / std::max(opt_.count, 1);
+    W1 = fit >= 8 ? 8 : fit >= 4 ? 4 : fit >= 2 ? 2 : fit >= 1 ? 1 : 2;
   }
   cfg_.phases.push_back(plan(W1, opt_.teamsPerBlock, opt_.count));
   if (opt_.blocks > 0) cfg_.phases[0].blocks = opt_.blocks;
@@ -246,7 +250,8 @@ Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, c
     for (int W = W1 * 2; W <= Wlast; W *= 2) {
       PhaseConfig p = plan(W, 0, opt_.count);
       p.blocks = p.blocksPerSM * sms;  // any instance may be left for it
-      cfg_.phases.back().yieldBelow = std::min(opt_.count - 1, p.blocks * p.teamsPerBlock);
+      const double capacity = static_cast<double>(p.blocks) * p.teamsPerBlock;
+      cfg_.phases.back().yieldBelow = static_cast<int>(std::min<double>(opt_.count - 1, std::ceil(opt_.handoverFactor * capacity)));
       cfg_.phases.push_back(p);
     }
     if (opt_.yieldBelow >= 0) cfg_.phases[0].yieldBelow = opt_.yieldBelow;

@@ -29,7 +29,9 @@ struct BatchOptions {
   std::int32_t teamWarps = 0;      // warps per simulation in the main phase (1, 2, 4, 8); 0: chosen from the batch size
   std::int32_t tailTeamWarps = -1; // warps per simulation once few instances remain; 0: no tail phase; -1: chosen
   std::int32_t teamsPerBlock = 0;  // simulations per block in the main phase; 0: chosen from the slot size
-  std::int32_t yieldBelow = -1;    // main phase pauses once at most this many instances remain; -1: the tail grid's size
+  std::int32_t yieldBelow = -1;    // main phase pauses once at most this many instances remain; -1: from handoverFactor
+  double handoverFactor = 2.0;     // a phase hands over once the unfinished instances number at most this multiple of
+                                   // the next phase's resident teams (the surplus waits in the next phase's queue)
   std::int32_t blocks = 0;         // 0: persistent grid sized to the device
   RetireRule rule{};
   bool stopWhenStable = false;     // the reference's calm rule (a sweep's "stopWhenStable"); exclusive with `rule`

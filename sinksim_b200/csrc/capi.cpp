@@ -90,6 +90,7 @@ ssb::BatchOptions to_options(const ssb_batch_options& o) {
   b.rule.wthLimit = o.rule_wth;
   b.rule.settleTime = o.rule_settle;
   b.stopWhenStable = o.stop_when_stable != 0;
+  if (o.handover_factor > 0) b.handoverFactor = o.handover_factor;
   return b;
 }
 
