@@ -103,7 +103,9 @@ __device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
 
   int stop = kRunning;
   bool paused = false;
-  Pose F = make_pose(M, R.zO, R.pitch, R.roll);
+  // every thread of the team stores the same pose; no thread reads the previous one after the step's last barrier
+  Pose& F = *S.pose;
+  F = make_pose(M, R.zO, R.pitch, R.roll);
   for (long long s = 0; s < B.maxSteps; ++s) {
     if (R.foundered || R.t >= B.tMax) break;
     if (B.yieldBelow > 0 && s > 0 && (s % kYieldCheckEvery) == 0) {

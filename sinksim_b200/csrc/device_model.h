@@ -140,13 +140,36 @@ struct DevBatch {
   std::int32_t yieldBelow;
 };
 
+// Pose R = Ry(pitch) Rx(roll) and translation (kernel/frame.hpp:9-21), with the single-precision copies the
+// portable32 column arithmetic uses (kernel/reduce.hpp:86-98). A team keeps the pose of its current step in its slot.
+struct Pose {
+  double R00, R01, R02, R10, R11, R12, R20, R21, R22, tx, ty, tz, cth, iR;
+  float fR20, fR21, fR22, ftz, fiR;
+};
+
+// The buoyancy pass's result: displaced volume, its centroid in the ship frame, the highest hull point in the world.
+struct Buoy {
+  double V, x, y, z, top;
+};
+
+// Lanes that solve one group of nodes' free-surface levels together (8, 16 or 32): a warp works on 32 / kLevelLanes
+// groups at once. Each lane forms the partials of 32 / kLevelLanes lanes of the 32-lane node-pass tree and combines
+// them in the tree's order, so the results do not depend on this choice.
+#ifndef SSB_LEVEL_LANES
+#define SSB_LEVEL_LANES 16
+#endif
+constexpr int kLevelLanes = SSB_LEVEL_LANES;
+static_assert(kLevelLanes == 8 || kLevelLanes == 16 || kLevelLanes == 32, "kLevelLanes must be 8, 16 or 32");
+constexpr int kLevelGroupsPerWarp = 32 / kLevelLanes;
+
 // Byte offsets of one simulation slot (one team of warps) in dynamic shared memory; `bytes` is the slot stride.
-// passes holds maxGroup node-pass results per warp of the team; hydro the eight buoyancy tree results; misc two
-// ints the team broadcasts (the claimed instance, the yield decision).
+// passes holds maxGroup node-pass results per level lane group of the team (kLevelGroupsPerWarp per warp); hydro the
+// eight buoyancy tree results; misc two ints the team broadcasts (the claimed instance, the yield decision); pose and
+// buoy the step's pose and buoyancy result, which every phase reads (kept here rather than in each thread's registers).
 // tmp is the sixth column of the loads' per-node terms (the other five reuse area, zmax, hEff, aEff and acc, which
 // are dead by then); kSlotAliasDV places it on dV when there are at least as many connections as nodes.
 struct SlotLayout {
-  std::uint32_t vol, level, cx, cy, cz, area, zmax, hEff, aEff, acc, deg, dV, q, tmp, passes, hydro, misc, merged, bytes;
+  std::uint32_t vol, level, cx, cy, cz, area, zmax, hEff, aEff, acc, deg, dV, q, tmp, passes, hydro, misc, merged, pose, buoy, bytes;
 };
 constexpr std::uint32_t kSlotAliasDV = 0xFFFFFFFFu;
 

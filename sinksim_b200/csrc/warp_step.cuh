@@ -46,13 +46,6 @@ constexpr double kPi = 3.141592653589793;
 __device__ __forceinline__ double jmax(double a, double b) { return (b > a) ? b : a; }
 __device__ __forceinline__ double jmin(double a, double b) { return (b < a) ? b : a; }
 
-// Pose R = Ry(pitch) Rx(roll) and translation (kernel/frame.hpp:9-21), with the single-precision copies the
-// portable32 column arithmetic uses (kernel/reduce.hpp:86-98).
-struct Pose {
-  double R00, R01, R02, R10, R11, R12, R20, R21, R22, tx, ty, tz, cth, iR;
-  float fR20, fR21, fR22, ftz, fiR;
-};
-
 __device__ __forceinline__ Pose make_pose(const DevModel& M, double zO, double th, double ph) {
   const double cth = pm::cos(th), sth = pm::sin(th), cph = pm::cos(ph), sph = pm::sin(ph);
   Pose F;
@@ -82,19 +75,19 @@ __device__ __forceinline__ double world_z(const Pose& F, double x, double y, dou
 // operand order (lower partner first), so every lane ends with the bits of the tree's lane 0.
 
 template <class T>
-__device__ __forceinline__ T bsum(T v, int off) { return v + __shfl_xor_sync(kFull, v, off); }
+__device__ __forceinline__ T bsum(T v, int off, unsigned mask = kFull) { return v + __shfl_xor_sync(mask, v, off); }
 
 template <class T>
-__device__ __forceinline__ T bmin(T v, int off, int lane) {
-  const T o = __shfl_xor_sync(kFull, v, off);
+__device__ __forceinline__ T bmin(T v, int off, int lane, unsigned mask = kFull) {
+  const T o = __shfl_xor_sync(mask, v, off);
   const bool lower = (lane & off) == 0;
   const T a = lower ? v : o, b = lower ? o : v;
   return (b < a) ? b : a;
 }
 
 template <class T>
-__device__ __forceinline__ T bmax(T v, int off, int lane) {
-  const T o = __shfl_xor_sync(kFull, v, off);
+__device__ __forceinline__ T bmax(T v, int off, int lane, unsigned mask = kFull) {
+  const T o = __shfl_xor_sync(mask, v, off);
   const bool lower = (lane & off) == 0;
   const T a = lower ? v : o, b = lower ? o : v;
   return (b > a) ? b : a;
@@ -115,10 +108,6 @@ struct Team {
 };
 
 // ----------------------------------------------------------------------------- buoyancy (hydro pass, tree order)
-
-struct Buoy {
-  double V, x, y, z, top;
-};
 
 // One column into a buoyancy partial (kernel/reduce.hpp:39-49 in double, :131-142 in float): the same expressions in
 // the same order for T = double (portable) and T = float (portable32).
@@ -239,18 +228,20 @@ struct PassR {
   double vol, dv, mx, my, mz, zmin, zmax;
 };
 
-// Lane `lane`'s partial of a node pass: segments s0 + lane + 32 k in increasing k, two at a time.
+// The kLevelLanes consecutive lanes of a warp that solve one group of nodes: `lane` is the lane in the warp, `sub` the
+// lane in the group, `mask` the group's lanes.
+struct LevelLanes {
+  int lane, sub;
+  unsigned mask;
+};
+
+// The partial of one lane of the 32-lane tree (the lane whose first segment is `first`): segments first + 32 k in
+// increasing k, two at a time.
 template <class T>
 __device__ __forceinline__ SegPartial<T> segment_partial(const typename Vec2<T>::type* xy, const typename Vec2<T>::type* ab, const T* area,
                                                          int first, int end, T R20, T R21, T R22, T tz, T iR, T h) {
   SegPartial<T> p{T(0), T(0), T(0), T(0), T(0), T(1e9), T(-1e9)};
   int j = first;
-#if defined(SSB_SEGMENTS_ONE_AT_A_TIME)
-  for (; j < end; j += kLanes) {
-    const auto a0 = __ldg(xy + j), b0 = __ldg(ab + j);
-    clip_segment<T>(a0.x, a0.y, b0.x, b0.y, __ldg(area + j), R20, R21, R22, tz, iR, h, p);
-  }
-#endif
   for (; j + kLanes < end; j += 2 * kLanes) {
     const auto a0 = __ldg(xy + j), b0 = __ldg(ab + j), a1 = __ldg(xy + j + kLanes), b1 = __ldg(ab + j + kLanes);
     const T A0 = __ldg(area + j), A1 = __ldg(area + j + kLanes);
@@ -264,23 +255,40 @@ __device__ __forceinline__ SegPartial<T> segment_partial(const typename Vec2<T>:
   return p;
 }
 
-// The node pass of node n at world level h: the lane partials, the butterfly tree and the permeability scaling
-// (hydro.hpp:295-316 / 338-349). The level solvers call it from seven places: inlined, the copies crowd the
-// instruction cache; out of line, the caller's live registers spill around each call. Measured on B200 (2,368
-// titanic64 instances, single-warp teams): inlined 9.4 M steps/s, out of line 8.1 M.
-#ifndef SSB_NODE_PASS_LINKAGE
-#define SSB_NODE_PASS_LINKAGE __forceinline__
-#endif
+// One level of the tree inside a lane: the lower tree lane's partial `lo` takes in the upper one's, with the operand
+// order of the butterfly steps.
 template <class T>
-__device__ SSB_NODE_PASS_LINKAGE PassR node_pass_body(const int* segStart, const int* segCount, const double* muArr, const typename Vec2<T>::type* xy,
-                                             const typename Vec2<T>::type* ab, const T* area, T R20, T R21, T R22, T tz, T iR, double iRd,
-                                             int n, double h, int lane) {
+__device__ __forceinline__ void tree_pair(SegPartial<T>& lo, const SegPartial<T>& up) {
+  lo.vol = lo.vol + up.vol; lo.dv = lo.dv + up.dv; lo.mx = lo.mx + up.mx; lo.my = lo.my + up.my; lo.mz = lo.mz + up.mz;
+  lo.zmin = (up.zmin < lo.zmin) ? up.zmin : lo.zmin;
+  lo.zmax = (up.zmax > lo.zmax) ? up.zmax : lo.zmax;
+}
+
+// The node pass of node n at world level h: the 32 lane partials, the halving tree and the permeability scaling
+// (hydro.hpp:295-316 / 338-349). Lane `sub` of a level lane group forms the partials of tree lanes sub + kLevelLanes j
+// and combines them over the tree's upper levels (offsets 16 down to kLevelLanes) in registers; the lower levels are
+// shuffles inside the group. Every lane of the group ends with the bits of tree lane 0.
+template <class T>
+__device__ __forceinline__ PassR node_pass_body(const int* segStart, const int* segCount, const double* muArr, const typename Vec2<T>::type* xy,
+                                                const typename Vec2<T>::type* ab, const T* area, T R20, T R21, T R22, T tz, T iR, double iRd,
+                                                int n, double h, const LevelLanes& L) {
   const int s0 = __ldg(segStart + n), s1 = s0 + __ldg(segCount + n);
-  SegPartial<T> p = segment_partial<T>(xy, ab, area, s0 + lane, s1, R20, R21, R22, tz, iR, static_cast<T>(h));
+  const T hT = static_cast<T>(h);
+  const int f = s0 + L.sub;
+  SegPartial<T> p = segment_partial<T>(xy, ab, area, f, s1, R20, R21, R22, tz, iR, hT);
+  if constexpr (kLevelLanes == 16) {
+    tree_pair(p, segment_partial<T>(xy, ab, area, f + 16, s1, R20, R21, R22, tz, iR, hT));
+  } else if constexpr (kLevelLanes == 8) {
+    tree_pair(p, segment_partial<T>(xy, ab, area, f + 16, s1, R20, R21, R22, tz, iR, hT));
+    SegPartial<T> q = segment_partial<T>(xy, ab, area, f + 8, s1, R20, R21, R22, tz, iR, hT);
+    tree_pair(q, segment_partial<T>(xy, ab, area, f + 24, s1, R20, R21, R22, tz, iR, hT));
+    tree_pair(p, q);
+  }
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    p.vol = bsum(p.vol, off); p.dv = bsum(p.dv, off); p.mx = bsum(p.mx, off); p.my = bsum(p.my, off); p.mz = bsum(p.mz, off);
-    p.zmin = bmin(p.zmin, off, lane); p.zmax = bmax(p.zmax, off, lane);
+  for (int off = kLevelLanes / 2; off > 0; off >>= 1) {
+    p.vol = bsum(p.vol, off, L.mask); p.dv = bsum(p.dv, off, L.mask); p.mx = bsum(p.mx, off, L.mask);
+    p.my = bsum(p.my, off, L.mask); p.mz = bsum(p.mz, off, L.mask);
+    p.zmin = bmin(p.zmin, off, L.lane, L.mask); p.zmax = bmax(p.zmax, off, L.lane, L.mask);
   }
   const double mu = __ldg(muArr + n);
   PassR r;
@@ -292,12 +300,12 @@ __device__ SSB_NODE_PASS_LINKAGE PassR node_pass_body(const int* segStart, const
 }
 
 template <bool MIXED>
-__device__ __forceinline__ PassR node_pass(const DevModel& M, const Pose& F, int n, double h, int lane) {
+__device__ __forceinline__ PassR node_pass(const DevModel& M, const Pose& F, int n, double h, const LevelLanes& L) {
   if constexpr (!MIXED)
-    return node_pass_body<double>(M.segStart, M.segCount, M.mu, M.segXY, M.segLH, M.segAr, F.R20, F.R21, F.R22, F.tz, F.iR, F.iR, n, h, lane);
+    return node_pass_body<double>(M.segStart, M.segCount, M.mu, M.segXY, M.segLH, M.segAr, F.R20, F.R21, F.R22, F.tz, F.iR, F.iR, n, h, L);
   else
     return node_pass_body<float>(M.segStart, M.segCount, M.mu, M.segXYf, M.segLHf, M.segArf, F.fR20, F.fR21, F.fR22, F.ftz, F.fiR, F.iR, n, h,
-                                 lane);
+                                 L);
 }
 
 // ----------------------------------------------------------------------------- per-warp view of the slot in shared memory
@@ -308,6 +316,8 @@ struct Slot {
   int* misc;
   PassR* passes;
   std::uint8_t* merged;
+  Pose* pose;
+  Buoy* buoy;
 };
 
 __device__ __forceinline__ Slot carve_slot(unsigned char* base, const SlotLayout& L) {
@@ -330,53 +340,66 @@ __device__ __forceinline__ Slot carve_slot(unsigned char* base, const SlotLayout
   s.misc = reinterpret_cast<int*>(base + L.misc);
   s.passes = reinterpret_cast<PassR*>(base + L.passes);
   s.merged = base + L.merged;
+  s.pose = reinterpret_cast<Pose*>(base + L.pose);
+  s.buoy = reinterpret_cast<Buoy*>(base + L.buoy);
   return s;
 }
 
 // ----------------------------------------------------------------------------- free-surface levels (kernel/levels.hpp)
-// Warp-uniform: every lane runs the solver on identical pass results and stores identical values.
+// Group-uniform: the lanes of a level lane group run the solver on identical pass results and store identical values.
+// Each solver is a loop around its one node-pass call site, in stages: the passes at the starting level, then either
+// the passes at the top of a full node or group (for the centroids) or the passes of the bracketed Newton iteration.
 
 __device__ __forceinline__ void set_centroid(Slot& S, int n, const PassR& p) {
   if (p.vol > kCentroidMinVolume) { S.cx[n] = p.mx / p.vol; S.cy[n] = p.my / p.vol; S.cz[n] = p.mz / p.vol; }
 }
 
+enum SolveStage { kStageFirst, kStageFull, kStageNewton };
+
+// One node (levels.hpp:13-49).
 template <bool MIXED>
-__device__ __forceinline__ void solve_single(const DevModel& M, const Pose& F, Slot& S, int n, int lane) {
+__device__ __forceinline__ void solve_single(const DevModel& M, const Pose& F, Slot& S, int n, const LevelLanes& L) {
   const double V = S.vol[n], Vmax = __ldg(M.vmax + n);
-  double h = S.level[n];
-  PassR p = node_pass<MIXED>(M, F, n, h, lane);
-  const double lo = p.zmin, hi = p.zmax;
-  S.zmax[n] = hi;
-  if (V <= kEmptyVolume) { S.level[n] = lo; S.area[n] = 0; return; }
-  if (V >= Vmax * kFullFraction) {
-    p = node_pass<MIXED>(M, F, n, hi, lane);
-    const double aov = __ldg(M.aov + n);
-    S.level[n] = hi + jmax(0.0, V - Vmax) / aov;
-    S.area[n] = aov;
-    set_centroid(S, n, p);
-    return;
-  }
-  if (h < lo || h > hi) {
-    h = jmin(hi, jmax(lo, h));
-    p = node_pass<MIXED>(M, F, n, h, lane);
-  }
   const double tol = jmax(1e-3 * Vmax, 0.5);
-  double a = lo, b = hi;
-  for (int it = 0; it < kNewtonFast; ++it) {
+  double h = S.level[n];
+  double hi = 0, a = 0, b = 0;
+  int stage = kStageFirst, it = 0;
+  PassR p;
+  for (;;) {
+    p = node_pass<MIXED>(M, F, n, h, L);
+    if (stage == kStageFirst) {
+      const double lo = p.zmin;
+      hi = p.zmax;
+      S.zmax[n] = hi;
+      if (V <= kEmptyVolume) { S.level[n] = lo; S.area[n] = 0; return; }
+      if (V >= Vmax * kFullFraction) { stage = kStageFull; h = hi; continue; }
+      stage = kStageNewton;
+      a = lo; b = hi;
+      if (h < lo || h > hi) { h = jmin(hi, jmax(lo, h)); continue; }
+    } else if (stage == kStageFull) {
+      const double aov = __ldg(M.aov + n);
+      S.level[n] = hi + jmax(0.0, V - Vmax) / aov;
+      S.area[n] = aov;
+      set_centroid(S, n, p);
+      return;
+    }
+    // Newton: p is the pass at h, the it-th of at most kNewtonFast after the starting one
+    if (it == kNewtonFast) break;
     const double err = p.vol - V;
     if (fabs(err) < tol) break;
     if (err > 0) b = h; else a = h;
     double hn = p.dv > kSlopeMin ? h - err / p.dv : 0.5 * (a + b);
     if (!(hn > a && hn < b)) hn = 0.5 * (a + b);
     h = hn;
-    p = node_pass<MIXED>(M, F, n, h, lane);
+    ++it;
   }
   S.level[n] = h; S.area[n] = p.dv;
   set_centroid(S, n, p);
 }
 
+// A merged group of N nodes at one common level (levels.hpp:54-162); P holds the members' passes.
 template <bool MIXED>
-__device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Slot& S, PassR* P, const int* m, int N, int lane) {
+__device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Slot& S, PassR* P, const int* m, int N, const LevelLanes& L) {
   double V = 0, Vmax = 0;
   for (int k = 0; k < N; ++k) { V += S.vol[__ldg(m + k)]; Vmax += __ldg(M.vmax + __ldg(m + k)); }
   bool allWet = true;
@@ -393,43 +416,50 @@ __device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Sl
   } else {
     h = S.level[__ldg(m + (firstWet >= 0 ? firstWet : N - 1))];
   }
-  for (int k = 0; k < N; ++k) P[k] = node_pass<MIXED>(M, F, __ldg(m + k), h, lane);
-  for (int k = 0; k < N; ++k) S.zmax[__ldg(m + k)] = P[k].zmax;
-  double lo = P[0].zmin, hi = P[0].zmax;
-  for (int k = 1; k < N; ++k) { if (P[k].zmin < lo) lo = P[k].zmin; if (P[k].zmax > hi) hi = P[k].zmax; }
-
-  if (V <= kEmptyVolume) {
-    for (int k = 0; k < N; ++k) { const int n = __ldg(m + k); S.vol[n] = 0; S.level[n] = P[k].zmin; S.area[n] = 0; }
-    return;
-  }
-  if (V >= Vmax * kFullFraction) {
-    const double over = jmax(0.0, V - Vmax);
-    double aSum = 0;
-    for (int k = 0; k < N; ++k) aSum += __ldg(M.aov + __ldg(m + k));
-    const double dh = over / aSum;
-    double assigned = 0;
-    for (int k = 0; k < N - 1; ++k) {
-      const int n = __ldg(m + k);
-      const double v = __ldg(M.vmax + n) + dh * __ldg(M.aov + n);
-      S.vol[n] = v;
-      assigned += v;
-    }
-    S.vol[__ldg(m + N - 1)] = V - assigned;
-    for (int k = 0; k < N; ++k) {
-      const int n = __ldg(m + k);
-      P[k] = node_pass<MIXED>(M, F, n, hi, lane);
-      S.level[n] = hi + dh; S.area[n] = __ldg(M.aov + n);
-      set_centroid(S, n, P[k]);
-    }
-    return;
-  }
-  if (!(h >= lo && h <= hi)) {
-    h = jmin(hi, jmax(lo, h));
-    for (int k = 0; k < N; ++k) P[k] = node_pass<MIXED>(M, F, __ldg(m + k), h, lane);
-  }
   const double tol = jmax(1e-3 * Vmax, 0.5);
-  double a = lo, b = hi;
-  for (int it = 0; it < kNewtonFast; ++it) {
+  double hi = 0, a = 0, b = 0, dh = 0;
+  int stage = kStageFirst, it = 0;
+  for (;;) {
+    for (int k = 0; k < N; ++k) P[k] = node_pass<MIXED>(M, F, __ldg(m + k), h, L);
+    if (stage == kStageFirst) {
+      for (int k = 0; k < N; ++k) S.zmax[__ldg(m + k)] = P[k].zmax;
+      double lo = P[0].zmin;
+      hi = P[0].zmax;
+      for (int k = 1; k < N; ++k) { if (P[k].zmin < lo) lo = P[k].zmin; if (P[k].zmax > hi) hi = P[k].zmax; }
+      if (V <= kEmptyVolume) {
+        for (int k = 0; k < N; ++k) { const int n = __ldg(m + k); S.vol[n] = 0; S.level[n] = P[k].zmin; S.area[n] = 0; }
+        return;
+      }
+      if (V >= Vmax * kFullFraction) {
+        const double over = jmax(0.0, V - Vmax);
+        double aSum = 0;
+        for (int k = 0; k < N; ++k) aSum += __ldg(M.aov + __ldg(m + k));
+        dh = over / aSum;
+        double assigned = 0;
+        for (int k = 0; k < N - 1; ++k) {
+          const int n = __ldg(m + k);
+          const double v = __ldg(M.vmax + n) + dh * __ldg(M.aov + n);
+          S.vol[n] = v;
+          assigned += v;
+        }
+        S.vol[__ldg(m + N - 1)] = V - assigned;
+        stage = kStageFull;
+        h = hi;
+        continue;
+      }
+      stage = kStageNewton;
+      a = lo; b = hi;
+      if (!(h >= lo && h <= hi)) { h = jmin(hi, jmax(lo, h)); continue; }
+    } else if (stage == kStageFull) {
+      for (int k = 0; k < N; ++k) {
+        const int n = __ldg(m + k);
+        S.level[n] = hi + dh; S.area[n] = __ldg(M.aov + n);
+        set_centroid(S, n, P[k]);
+      }
+      return;
+    }
+    // Newton on the members' summed volume: P holds the passes at h
+    if (it == kNewtonFast) break;
     double sum = 0;
     for (int k = 0; k < N; ++k) sum += P[k].vol;
     const double err = sum - V;
@@ -440,7 +470,7 @@ __device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Sl
     double hn = dvs > kSlopeMin ? h - err / dvs : 0.5 * (a + b);
     if (!(hn > a && hn < b)) hn = 0.5 * (a + b);
     h = hn;
-    for (int k = 0; k < N; ++k) P[k] = node_pass<MIXED>(M, F, __ldg(m + k), h, lane);
+    ++it;
   }
   double tot = 0;
   for (int k = 0; k < N; ++k) tot += P[k].vol;
@@ -483,13 +513,20 @@ __device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Sl
   }
 }
 
-// Groups are independent (a group's solve reads and writes only its members), so the team's warps take them in turn:
-// warp v solves groups v, v + W, ... (the reference's block did the same with its eight warps, device_step.cuh:270-281).
+// Groups are independent (a group's solve reads and writes only its members), so the team's level lane groups take
+// them in turn: lane group u of the team (kLevelGroupsPerWarp per warp) solves groups u, u + W kLevelGroupsPerWarp, ...
+// (the reference's block gave them to its eight warps, device_step.cuh:270-281).
 template <bool MIXED, int W>
 __device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, Slot& S, const Team<W>& T) {
-  const int lane = T.lane;
-  PassR* P = S.passes + static_cast<std::size_t>(T.warp) * M.maxGroup;
-  for (int g = T.warp; g < M.ng; g += W) {
+  LevelLanes L;
+  L.lane = T.lane;
+  L.sub = T.lane % kLevelLanes;
+  const int grp = T.lane / kLevelLanes;
+  if constexpr (kLevelLanes == 32) L.mask = kFull;
+  else L.mask = ((1u << kLevelLanes) - 1u) << (grp * kLevelLanes);
+  const int unit = T.warp * kLevelGroupsPerWarp + grp;
+  PassR* P = S.passes + static_cast<std::size_t>(unit) * M.maxGroup;
+  for (int g = unit; g < M.ng; g += W * kLevelGroupsPerWarp) {
     const int N = __ldg(M.gCount + g);
     const int* m = M.gNodes + __ldg(M.gStart + g);
     const int mode = __ldg(M.gMode + g);
@@ -507,9 +544,10 @@ __device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, S
       }
     }
     S.merged[g] = merged ? 1 : 0;
-    if (merged) solve_group<MIXED>(M, F, S, P, m, N, lane);
-    else for (int k = 0; k < N; ++k) solve_single<MIXED>(M, F, S, __ldg(m + k), lane);
+    if (merged) solve_group<MIXED>(M, F, S, P, m, N, L);
+    else for (int k = 0; k < N; ++k) solve_single<MIXED>(M, F, S, __ldg(m + k), L);
   }
+  __syncwarp();  // the lane groups leave the loop after different numbers of groups
 }
 
 // ----------------------------------------------------------------------------- flows (kernel/flows.hpp:38-78)
@@ -588,7 +626,7 @@ template <bool MIXED, int W>
 __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimRegs& R, Slot& S, const InstPtrs& I, const Team<W>& T) {
   constexpr int kStride = 32 * W;
   const int lane = T.lane, rank = T.rank;
-  const Buoy hb = buoyancy<MIXED, W>(M, F, T, S.hydro);
+  *S.buoy = buoyancy<MIXED, W>(M, F, T, S.hydro);  // every thread stores the same values
   solve_levels<MIXED, W>(M, F, S, T);
   T.sync();
 
@@ -662,6 +700,7 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
   double* const t3 = S.aEff;
   double* const t4 = S.acc;
   double* const t5 = S.tmp;
+  const Buoy hb = *S.buoy;
   const double Wg = M.rho * M.g;
   const double Fb = Wg * hb.V;
   const double bxw = F.R00 * hb.x + F.R01 * hb.y + F.R02 * hb.z + F.tx;
