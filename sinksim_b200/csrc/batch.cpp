@@ -122,6 +122,7 @@ struct Batch::Impl {
     L.merged = take(off, static_cast<std::size_t>(std::max(NG, 1)));
     L.pose = take(off, sizeof(Pose));
     L.buoy = take(off, sizeof(Buoy));
+    L.parked = take(off, sizeof(Parked));
     L.bytes = off;
     return L;
   }

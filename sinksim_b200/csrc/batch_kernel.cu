@@ -50,7 +50,6 @@ __device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
   if (B.stop[inst] != kRunning) return false;
   const int rank = T.rank;
   const std::size_t iN = static_cast<std::size_t>(inst) * M.nn;
-  const std::size_t iC = static_cast<std::size_t>(inst) * M.nc;
   SimRegs R;
   {
     const double* st = B.st + static_cast<std::size_t>(inst) * 8;
@@ -61,13 +60,7 @@ __device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
     R.founderT = B.founderT[inst];
     R.evCount = B.evCount[inst];
   }
-  InstPtrs I;
-  I.en = B.en + iC; I.area = B.area + iC; I.tOn = B.tOn + iC;
-  I.evT = B.evT + static_cast<std::size_t>(inst) * M.evCap;
-  I.evId = B.evId + static_cast<std::size_t>(inst) * M.evCap;
-  I.evKind = B.evKind + static_cast<std::size_t>(inst) * M.evCap;
-  I.overT = B.overT + static_cast<std::size_t>(inst) * M.nmon;
-  I.markT = B.markT + static_cast<std::size_t>(inst) * M.nmark;
+  const InstPtrs I{M, B, inst};
   for (int n = rank; n < M.nn; n += kStride) {
     S.vol[n] = B.vol[iN + n]; S.level[n] = B.level[iN + n];
     S.cx[n] = B.cx[iN + n]; S.cy[n] = B.cy[iN + n]; S.cz[n] = B.cz[iN + n];

@@ -152,6 +152,13 @@ struct Buoy {
   double V, x, y, z, top;
 };
 
+// The run's values that the hydrostatic phases of a step do not read: a team parks them in its slot while those
+// phases run, so that their registers serve the level solve (every thread of the team holds the same values).
+struct Parked {
+  double t, zO, pitch, roll, vz, wth, wph, calm, inflow, Vb, hullTop, mw, bx, by, bz, founderT;
+  int foundered;
+};
+
 // Lanes that solve one group of nodes' free-surface levels together (8, 16 or 32): a warp works on 32 / kLevelLanes
 // groups at once. Each lane forms the partials of 32 / kLevelLanes lanes of the 32-lane node-pass tree and combines
 // them in the tree's order, so the results do not depend on this choice.
@@ -165,11 +172,12 @@ constexpr int kLevelGroupsPerWarp = 32 / kLevelLanes;
 // Byte offsets of one simulation slot (one team of warps) in dynamic shared memory; `bytes` is the slot stride.
 // passes holds maxGroup node-pass results per level lane group of the team (kLevelGroupsPerWarp per warp); hydro the
 // eight buoyancy tree results; misc two ints the team broadcasts (the claimed instance, the yield decision); pose and
-// buoy the step's pose and buoyancy result, which every phase reads (kept here rather than in each thread's registers).
+// buoy the step's pose and buoyancy result, which every phase reads (kept here rather than in each thread's registers);
+// parked the run's values during the hydrostatic phases.
 // tmp is the sixth column of the loads' per-node terms (the other five reuse area, zmax, hEff, aEff and acc, which
 // are dead by then); kSlotAliasDV places it on dV when there are at least as many connections as nodes.
 struct SlotLayout {
-  std::uint32_t vol, level, cx, cy, cz, area, zmax, hEff, aEff, acc, deg, dV, q, tmp, passes, hydro, misc, merged, pose, buoy, bytes;
+  std::uint32_t vol, level, cx, cy, cz, area, zmax, hEff, aEff, acc, deg, dV, q, tmp, passes, hydro, misc, merged, pose, buoy, parked, bytes;
 };
 constexpr std::uint32_t kSlotAliasDV = 0xFFFFFFFFu;
 

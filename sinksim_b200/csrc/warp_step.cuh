@@ -318,6 +318,7 @@ struct Slot {
   std::uint8_t* merged;
   Pose* pose;
   Buoy* buoy;
+  Parked* parked;
 };
 
 __device__ __forceinline__ Slot carve_slot(unsigned char* base, const SlotLayout& L) {
@@ -342,6 +343,7 @@ __device__ __forceinline__ Slot carve_slot(unsigned char* base, const SlotLayout
   s.merged = base + L.merged;
   s.pose = reinterpret_cast<Pose*>(base + L.pose);
   s.buoy = reinterpret_cast<Buoy*>(base + L.buoy);
+  s.parked = reinterpret_cast<Parked*>(base + L.parked);
   return s;
 }
 
@@ -598,21 +600,44 @@ struct SimRegs {
   double inflow, Vb, hullTop, mw, bx, by, bz;
   int foundered;
   double founderT;
-  int evCount;
+  int evCount;  // warp 0's count is the log's; the other warps' lag
 };
 
+// Every thread stores the same values (evCount, which differs between warps, stays in registers).
+__device__ __forceinline__ void park(Parked* P, const SimRegs& R) {
+  P->t = R.t; P->zO = R.zO; P->pitch = R.pitch; P->roll = R.roll; P->vz = R.vz; P->wth = R.wth; P->wph = R.wph;
+  P->calm = R.calm; P->inflow = R.inflow; P->Vb = R.Vb; P->hullTop = R.hullTop; P->mw = R.mw; P->bx = R.bx;
+  P->by = R.by; P->bz = R.bz; P->founderT = R.founderT; P->foundered = R.foundered;
+}
+
+__device__ __forceinline__ void unpark(const Parked* P, SimRegs& R) {
+  R.t = P->t; R.zO = P->zO; R.pitch = P->pitch; R.roll = P->roll; R.vz = P->vz; R.wth = P->wth; R.wph = P->wph;
+  R.calm = P->calm; R.inflow = P->inflow; R.Vb = P->Vb; R.hullTop = P->hullTop; R.mw = P->mw; R.bx = P->bx;
+  R.by = P->by; R.bz = P->bz; R.founderT = P->founderT; R.foundered = P->foundered;
+}
+
+// Instance `inst`'s per-instance arrays: each pointer is formed where it is used from the batch's base pointers (kernel
+// parameters), so a thread holds one index rather than eight pointers through the step.
 struct InstPtrs {
-  const std::uint8_t* en;
-  const double* area;
-  const double* tOn;
-  double *evT, *overT, *markT;
-  std::int32_t *evId, *evKind;
+  const DevModel& M;
+  const DevBatch& B;
+  int inst;
+  __device__ __forceinline__ std::size_t perConn() const { return static_cast<std::size_t>(inst) * M.nc; }
+  __device__ __forceinline__ std::size_t perEvent() const { return static_cast<std::size_t>(inst) * M.evCap; }
+  __device__ __forceinline__ const std::uint8_t* en() const { return B.en + perConn(); }
+  __device__ __forceinline__ const double* area() const { return B.area + perConn(); }
+  __device__ __forceinline__ const double* tOn() const { return B.tOn + perConn(); }
+  __device__ __forceinline__ double* evT() const { return B.evT + perEvent(); }
+  __device__ __forceinline__ std::int32_t* evId() const { return B.evId + perEvent(); }
+  __device__ __forceinline__ std::int32_t* evKind() const { return B.evKind + perEvent(); }
+  __device__ __forceinline__ double* overT() const { return B.overT + static_cast<std::size_t>(inst) * M.nmon; }
+  __device__ __forceinline__ double* markT() const { return B.markT + static_cast<std::size_t>(inst) * M.nmark; }
 };
 
 // The event log belongs to warp 0 of the team: only its lane 0 writes, only its count is stored.
 __device__ __forceinline__ void push_event(const DevModel& M, SimRegs& R, const InstPtrs& I, int id, int kind, int lane) {
   if (R.evCount < M.evCap) {
-    if (lane == 0) { I.evT[R.evCount] = R.t; I.evId[R.evCount] = id; I.evKind[R.evCount] = kind; }
+    if (lane == 0) { I.evT()[R.evCount] = R.t; I.evId()[R.evCount] = id; I.evKind()[R.evCount] = kind; }
     R.evCount++;
   }
 }
@@ -626,6 +651,8 @@ template <bool MIXED, int W>
 __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimRegs& R, Slot& S, const InstPtrs& I, const Team<W>& T) {
   constexpr int kStride = 32 * W;
   const int lane = T.lane, rank = T.rank;
+  const double tNow = R.t;
+  park(S.parked, R);  // until the volume update; no thread reads it before the barrier that ends that phase
   *S.buoy = buoyancy<MIXED, W>(M, F, T, S.hydro);  // every thread stores the same values
   solve_levels<MIXED, W>(M, F, S, T);
   T.sync();
@@ -642,7 +669,7 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
     int d = 0;
     for (int k = k0; k < k1; ++k) {
       const int c = __ldg(M.incConn + k);
-      if (!__ldg(I.en + c)) continue;
+      if (!__ldg(I.en() + c)) continue;
       const int a = __ldg(M.ca + c), b = __ldg(M.cb + c);
       if (a >= 0 && S.hEff[a] < kNoHeadTest && S.hEff[b] < kNoHeadTest) continue;
       ++d;
@@ -652,7 +679,7 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
   T.sync();
   for (int c = rank; c < M.nc; c += kStride) {
     double q;
-    S.dV[c] = connection_flow(M, F, R.t, S, I.en, I.area, I.tOn, c, q);
+    S.dV[c] = connection_flow(M, F, tNow, S, I.en(), I.area(), I.tOn(), c, q);
     S.q[c] = q;
   }
   T.sync();
@@ -679,6 +706,7 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
   double seaIn = 0;
   for (int k = 0; k < M.nsea; ++k) seaIn += S.dV[__ldg(M.sea + k)];
   T.sync();
+  unpark(S.parked, R);
   // the excess returns to the sea in node order (flows.hpp:114-118)
   for (int n0 = 0; n0 < M.nn; n0 += kLanes) {
     const int n = n0 + lane;
@@ -756,7 +784,7 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
   for (int m0 = 0; m0 < M.nmon; m0 += kLanes) {
     const int m = m0 + lane;
     bool fire = false;
-    if (m < M.nmon && I.overT[m] < 0) {
+    if (m < M.nmon && I.overT()[m] < 0) {
       const int k0 = __ldg(M.monStart + m), k1 = k0 + __ldg(M.monCount + m);
       double over = 0;
       for (int k = k0; k < k1; ++k) {
@@ -764,7 +792,7 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
         if (qc > 0) over += qc;
       }
       fire = over > M.monThreshold;
-      if (fire) I.overT[m] = R.t;
+      if (fire) I.overT()[m] = R.t;
     }
     unsigned mask = __ballot_sync(kFull, fire);
     while (mask) {
@@ -776,11 +804,11 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
   for (int i0 = 0; i0 < M.nmark; i0 += kLanes) {
     const int i = i0 + lane;
     bool fire = false;
-    if (i < M.nmark && I.markT[i] < 0) {
+    if (i < M.nmark && I.markT()[i] < 0) {
       const double wz = world_z(F, __ldg(M.mkx + i), __ldg(M.mky + i), __ldg(M.mkz + i));
       const bool under = __ldg(M.mkWhen + i) == 0;
       fire = (under && wz < 0) || (!under && wz > 0);
-      if (fire) I.markT[i] = R.t;
+      if (fire) I.markT()[i] = R.t;
     }
     unsigned mask = __ballot_sync(kFull, fire);
     while (mask) {
