@@ -116,7 +116,7 @@ struct Batch::Impl {
     L.dV = take(off, sizeof(double) * static_cast<std::size_t>(std::max(NC, 1)));
     L.q = take(off, sizeof(double) * static_cast<std::size_t>(std::max(NC, 1)));
     L.tmp = NC >= NN ? kSlotAliasDV : take(off, nb);
-    L.passes = take(off, 7 * sizeof(double) * static_cast<std::size_t>(maxGroup) * static_cast<std::size_t>(W * kLevelGroupsPerWarp));
+    L.passes = take(off, 7 * sizeof(double) * static_cast<std::size_t>(maxGroup) * static_cast<std::size_t>(W * kMaxLevelGroupsPerWarp));
     L.hydro = take(off, 8 * 5 * sizeof(double));
     L.misc = take(off, 2 * sizeof(std::int32_t));
     L.merged = take(off, static_cast<std::size_t>(std::max(NG, 1)));

@@ -159,18 +159,26 @@ struct Parked {
   int foundered;
 };
 
-// Lanes that solve one group of nodes' free-surface levels together (8, 16 or 32): a warp works on 32 / kLevelLanes
-// groups at once. Each lane forms the partials of 32 / kLevelLanes lanes of the 32-lane node-pass tree and combines
-// them in the tree's order, so the results do not depend on this choice.
-#ifndef SSB_LEVEL_LANES
-#define SSB_LEVEL_LANES 16
+// Lanes that solve one group of nodes' free-surface levels together (8, 16 or 32), per numerics: a warp works on
+// 32 / kLevelLanes groups at once. Each lane forms the partials of 32 / kLevelLanes lanes of the 32-lane node-pass tree
+// and combines them in the tree's order, so the results do not depend on this choice. Fewer lanes per group give more
+// groups in flight but more partials per lane (registers); on B200 (titanic64 batches) 16 was the fastest for double
+// precision partials and 8 for single precision ones.
+#ifndef SSB_LEVEL_LANES_F64
+#define SSB_LEVEL_LANES_F64 16
 #endif
-constexpr int kLevelLanes = SSB_LEVEL_LANES;
-static_assert(kLevelLanes == 8 || kLevelLanes == 16 || kLevelLanes == 32, "kLevelLanes must be 8, 16 or 32");
-constexpr int kLevelGroupsPerWarp = 32 / kLevelLanes;
+#ifndef SSB_LEVEL_LANES_F32
+#define SSB_LEVEL_LANES_F32 8
+#endif
+template <bool MIXED>
+constexpr int kLevelLanes = MIXED ? SSB_LEVEL_LANES_F32 : SSB_LEVEL_LANES_F64;
+static_assert(kLevelLanes<false> == 8 || kLevelLanes<false> == 16 || kLevelLanes<false> == 32, "level lanes must be 8, 16 or 32");
+static_assert(kLevelLanes<true> == 8 || kLevelLanes<true> == 16 || kLevelLanes<true> == 32, "level lanes must be 8, 16 or 32");
+// the slot's node-pass buffers are sized for the numerics with the most groups per warp
+constexpr int kMaxLevelGroupsPerWarp = 32 / (kLevelLanes<false> < kLevelLanes<true> ? kLevelLanes<false> : kLevelLanes<true>);
 
 // Byte offsets of one simulation slot (one team of warps) in dynamic shared memory; `bytes` is the slot stride.
-// passes holds maxGroup node-pass results per level lane group of the team (kLevelGroupsPerWarp per warp); hydro the
+// passes holds maxGroup node-pass results per level lane group of the team (up to kMaxLevelGroupsPerWarp per warp); hydro the
 // eight buoyancy tree results; misc two ints the team broadcasts (the claimed instance, the yield decision); pose and
 // buoy the step's pose and buoyancy result, which every phase reads (kept here rather than in each thread's registers);
 // parked the run's values during the hydrostatic phases.

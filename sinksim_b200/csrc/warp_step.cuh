@@ -228,7 +228,7 @@ struct PassR {
   double vol, dv, mx, my, mz, zmin, zmax;
 };
 
-// The kLevelLanes consecutive lanes of a warp that solve one group of nodes: `lane` is the lane in the warp, `sub` the
+// The kLevelLanes<MIXED> consecutive lanes of a warp that solve one group of nodes: `lane` is the lane in the warp, `sub` the
 // lane in the group, `mask` the group's lanes.
 struct LevelLanes {
   int lane, sub;
@@ -265,10 +265,10 @@ __device__ __forceinline__ void tree_pair(SegPartial<T>& lo, const SegPartial<T>
 }
 
 // The node pass of node n at world level h: the 32 lane partials, the halving tree and the permeability scaling
-// (hydro.hpp:295-316 / 338-349). Lane `sub` of a level lane group forms the partials of tree lanes sub + kLevelLanes j
-// and combines them over the tree's upper levels (offsets 16 down to kLevelLanes) in registers; the lower levels are
+// (hydro.hpp:295-316 / 338-349). Lane `sub` of a group of LANES lanes forms the partials of tree lanes sub + LANES j
+// and combines them over the tree's upper levels (offsets 16 down to LANES) in registers; the lower levels are
 // shuffles inside the group. Every lane of the group ends with the bits of tree lane 0.
-template <class T>
+template <class T, int LANES>
 __device__ __forceinline__ PassR node_pass_body(const int* segStart, const int* segCount, const double* muArr, const typename Vec2<T>::type* xy,
                                                 const typename Vec2<T>::type* ab, const T* area, T R20, T R21, T R22, T tz, T iR, double iRd,
                                                 int n, double h, const LevelLanes& L) {
@@ -276,16 +276,16 @@ __device__ __forceinline__ PassR node_pass_body(const int* segStart, const int* 
   const T hT = static_cast<T>(h);
   const int f = s0 + L.sub;
   SegPartial<T> p = segment_partial<T>(xy, ab, area, f, s1, R20, R21, R22, tz, iR, hT);
-  if constexpr (kLevelLanes == 16) {
+  if constexpr (LANES == 16) {
     tree_pair(p, segment_partial<T>(xy, ab, area, f + 16, s1, R20, R21, R22, tz, iR, hT));
-  } else if constexpr (kLevelLanes == 8) {
+  } else if constexpr (LANES == 8) {
     tree_pair(p, segment_partial<T>(xy, ab, area, f + 16, s1, R20, R21, R22, tz, iR, hT));
     SegPartial<T> q = segment_partial<T>(xy, ab, area, f + 8, s1, R20, R21, R22, tz, iR, hT);
     tree_pair(q, segment_partial<T>(xy, ab, area, f + 24, s1, R20, R21, R22, tz, iR, hT));
     tree_pair(p, q);
   }
 #pragma unroll
-  for (int off = kLevelLanes / 2; off > 0; off >>= 1) {
+  for (int off = LANES / 2; off > 0; off >>= 1) {
     p.vol = bsum(p.vol, off, L.mask); p.dv = bsum(p.dv, off, L.mask); p.mx = bsum(p.mx, off, L.mask);
     p.my = bsum(p.my, off, L.mask); p.mz = bsum(p.mz, off, L.mask);
     p.zmin = bmin(p.zmin, off, L.lane, L.mask); p.zmax = bmax(p.zmax, off, L.lane, L.mask);
@@ -302,9 +302,9 @@ __device__ __forceinline__ PassR node_pass_body(const int* segStart, const int* 
 template <bool MIXED>
 __device__ __forceinline__ PassR node_pass(const DevModel& M, const Pose& F, int n, double h, const LevelLanes& L) {
   if constexpr (!MIXED)
-    return node_pass_body<double>(M.segStart, M.segCount, M.mu, M.segXY, M.segLH, M.segAr, F.R20, F.R21, F.R22, F.tz, F.iR, F.iR, n, h, L);
+    return node_pass_body<double, kLevelLanes<false>>(M.segStart, M.segCount, M.mu, M.segXY, M.segLH, M.segAr, F.R20, F.R21, F.R22, F.tz, F.iR, F.iR, n, h, L);
   else
-    return node_pass_body<float>(M.segStart, M.segCount, M.mu, M.segXYf, M.segLHf, M.segArf, F.fR20, F.fR21, F.fR22, F.ftz, F.fiR, F.iR, n, h,
+    return node_pass_body<float, kLevelLanes<true>>(M.segStart, M.segCount, M.mu, M.segXYf, M.segLHf, M.segArf, F.fR20, F.fR21, F.fR22, F.ftz, F.fiR, F.iR, n, h,
                                  L);
 }
 
@@ -516,19 +516,20 @@ __device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Sl
 }
 
 // Groups are independent (a group's solve reads and writes only its members), so the team's level lane groups take
-// them in turn: lane group u of the team (kLevelGroupsPerWarp per warp) solves groups u, u + W kLevelGroupsPerWarp, ...
+// them in turn: lane group u of the team (32 / kLevelLanes<MIXED> per warp) solves groups u, u + 32 W / kLevelLanes, ...
 // (the reference's block gave them to its eight warps, device_step.cuh:270-281).
 template <bool MIXED, int W>
 __device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, Slot& S, const Team<W>& T) {
+  constexpr int LANES = kLevelLanes<MIXED>, PER_WARP = 32 / LANES;
   LevelLanes L;
   L.lane = T.lane;
-  L.sub = T.lane % kLevelLanes;
-  const int grp = T.lane / kLevelLanes;
-  if constexpr (kLevelLanes == 32) L.mask = kFull;
-  else L.mask = ((1u << kLevelLanes) - 1u) << (grp * kLevelLanes);
-  const int unit = T.warp * kLevelGroupsPerWarp + grp;
+  L.sub = T.lane % LANES;
+  const int grp = T.lane / LANES;
+  if constexpr (LANES == 32) L.mask = kFull;
+  else L.mask = ((1u << LANES) - 1u) << (grp * LANES);
+  const int unit = T.warp * PER_WARP + grp;
   PassR* P = S.passes + static_cast<std::size_t>(unit) * M.maxGroup;
-  for (int g = unit; g < M.ng; g += W * kLevelGroupsPerWarp) {
+  for (int g = unit; g < M.ng; g += W * PER_WARP) {
     const int N = __ldg(M.gCount + g);
     const int* m = M.gNodes + __ldg(M.gStart + g);
     const int mode = __ldg(M.gMode + g);
