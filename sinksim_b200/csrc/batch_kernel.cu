@@ -178,7 +178,7 @@ __device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
 }
 
 template <bool MIXED, int W>
-__global__ void __launch_bounds__(kMaxWarpsPerBlock * 32, 1) run_batch(DevModel M, DevBatch B, SlotLayout L) {
+__global__ void __launch_bounds__(kMaxWarpsPerBlock * 32, kMinBlocksPerSM) run_batch(DevModel M, DevBatch B, SlotLayout L) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int warpInBlock = threadIdx.x >> 5;
   const int team = warpInBlock / W;

@@ -9,8 +9,18 @@
 
 namespace ssb {
 
-// Warps per block at most (teams of 1, 2, 4 or 8 warps; teams per block x warps per team <= 16).
-constexpr int kMaxWarpsPerBlock = 16;
+// Warps per block at most (teams of 1, 2, 4 or 8 warps; teams per block x warps per team <= kMaxWarpsPerBlock) and the
+// blocks of that size the kernel is compiled to fit on one SM (which sets its register budget: 65,536 registers
+// over kMaxWarpsPerBlock x 32 x kMinBlocksPerSM threads).
+#ifndef SSB_BLOCK_WARPS
+#define SSB_BLOCK_WARPS 16
+#endif
+#ifndef SSB_MIN_BLOCKS
+#define SSB_MIN_BLOCKS 1
+#endif
+constexpr int kMaxWarpsPerBlock = SSB_BLOCK_WARPS;
+constexpr int kMinBlocksPerSM = SSB_MIN_BLOCKS;
+static_assert(kMaxWarpsPerBlock >= 8, "a block must hold an eight-warp team");
 
 bool valid_team_size(int teamWarps);
 cudaError_t configure_batch_kernel(bool mixed, int teamWarps, std::size_t smemBytes);
