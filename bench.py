@@ -36,6 +36,12 @@ sys.path.insert(0, ROOT)
 # (75), 290 connection flows (30), 64 node updates and loads (40).
 FP64_OPS_PER_STEP = 7 * 4408 + 11 * 4058 + 10 * 9422 + 11.5 * 4174 + 71 * 31 + 191 + 75 * 27 + 30 * 290 + 40 * 64
 
+# DRAM bytes (read + write) of one main-phase launch over the 4,096 instances, from ncu (dram__bytes per second x
+# duration of run_batch<portable, 2-warp teams> on the same batch run to 600 s: python bench.py --count 4096 --tmax 600).
+# The traffic is the instances' state going in and out: the geometry and the running state stay on chip, so the figure
+# does not grow with the steps a launch takes.
+KERNEL_DRAM_BYTES_PER_LAUNCH = 25.3e6
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -236,6 +242,7 @@ def main():
     # its wall time is the end-to-end figure, the CUDA-event time of its kernel launch the device figure
     dev_ms, steps_total, e2e_s = 0.0, 0, 0.0
     per_launch_ms = []
+    phase_ms, phase_steps = None, None
     with Clocks(local) as clocks:
         for _ in range(args.steps):
             batch.reset()
@@ -247,6 +254,9 @@ def main():
             dev_ms += ms
             per_launch_ms.append(ms)
             steps_total += batch.total_steps()
+            ps = batch.phase_stats()
+            phase_ms = [p["device_ms"] for p in ps] if phase_ms is None else [a + p["device_ms"] for a, p in zip(phase_ms, ps)]
+            phase_steps = [p["steps"] for p in ps] if phase_steps is None else [a + p["steps"] for a, p in zip(phase_steps, ps)]
     barrier()
     h2d, d2h = batch.transfer_bytes()
     info = batch.launch_info()
@@ -260,14 +270,21 @@ def main():
         fp64_peak = ssb.add_mul_peak(True, local)
         fp32_peak = ssb.add_mul_peak(False, local)
         steps_per_launch = steps_total / args.steps
-        achieved = FP64_OPS_PER_STEP * steps_per_launch / (statistics.mean(per_launch_ms) / 1e3)
+        # the dominant kernel: the launch phase with the most device time; its work over its own CUDA-event time
+        top = max(range(len(phase_ms)), key=lambda k: phase_ms[k])
+        top_warps = batch.phase_stats()[top]["team_warps"]
+        achieved = FP64_OPS_PER_STEP * phase_steps[top] / (phase_ms[top] / 1e3)
+        phases = [{"team_warps": p["team_warps"], "device_ms_per_run": m / args.steps, "share": m / sum(phase_ms),
+                   "sim_steps_per_run": s / args.steps} for p, m, s in zip(batch.phase_stats(), phase_ms, phase_steps)]
         out = {"metric": "sim-steps/s", "value": value, "unit": "sim-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": dev_s_max * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                "dtype": "f64" if args.numerics == "portable" else "f32+f64", "data": "synthetic", "config": workload_config(args),
                "e2e": {"value": e2e, "unit": "sim-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-               "gpu_launches": args.steps, "launch": info, "sim_steps_per_launch": steps_per_launch,
+               "gpu_launches": args.steps * info["phases"], "launch": info, "sim_steps_per_launch": steps_per_launch,
                "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
-                            "frac": achieved / fp64_peak, "traffic": None,
+                            "frac": achieved / fp64_peak, "traffic": KERNEL_DRAM_BYTES_PER_LAUNCH,
+                            "kernel": f"run_batch<{args.numerics}, {top_warps}-warp teams> (launch phase {top})",
+                            "phases": phases,
                             "peak_source": "measured on this GPU: separately rounded FP64 add+mul microbenchmark (no FMA, as the bits require)",
                             "fp32_peak": fp32_peak / 1e12, "ops_per_sim_step": FP64_OPS_PER_STEP,
                             "note": "the step is issue/latency bound; HBM traffic is negligible (L2-resident working set)"},

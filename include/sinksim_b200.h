@@ -89,6 +89,7 @@ typedef struct ssb_launch_info {
   int32_t team_warps, teams_per_block, blocks, blocks_per_sm, yield_below;
   int32_t tail_team_warps, tail_teams_per_block, tail_blocks, tail_blocks_per_sm;
   uint64_t slot_bytes;  /* shared memory of one simulation */
+  int32_t phases;       /* kernel launches of one run: the phases from the main team size up to the tail's */
 } ssb_launch_info;
 
 /* The message of the last failure on this thread. */
@@ -137,6 +138,10 @@ int ssb_batch_launch(ssb_batch* b, float* device_ms);
 int ssb_batch_download(ssb_batch* b);
 /* Bytes one run copies host to device and device to host (inputs and results). */
 int ssb_batch_transfer_bytes(const ssb_batch* b, uint64_t* h2d, uint64_t* d2h);
+/* The last launch by phase (0 .. ssb_launch_info.phases - 1): the phase's team size, its device time in milliseconds
+ * (CUDA events around its kernel launches) and the steps its kernels took. No counterpart in the reference, whose run
+ * is one phase; it serves the per-kernel roofline of the benchmark. */
+int ssb_batch_phase_stats(const ssb_batch* b, int32_t phase, int32_t* team_warps, float* device_ms, int64_t* steps);
 
 /* Results after the run: cuda::Batch::total_steps / result / curve / final_readouts / trace
  * (engine/cuda/batch.cu:302-400). */

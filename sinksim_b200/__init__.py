@@ -51,7 +51,7 @@ class _Summary(C.Structure):
 
 class _LaunchInfo(C.Structure):
     _fields_ = [(k, C.c_int32) for k in ("team_warps", "teams_per_block", "blocks", "blocks_per_sm", "yield_below", "tail_team_warps",
-                                         "tail_teams_per_block", "tail_blocks", "tail_blocks_per_sm")] + [("slot_bytes", C.c_uint64)]
+                                         "tail_teams_per_block", "tail_blocks", "tail_blocks_per_sm")] + [("slot_bytes", C.c_uint64), ("phases", C.c_int32)]
 
 
 _lib = None
@@ -78,6 +78,7 @@ _SIGNATURES = {
     "ssb_batch_download": (C.c_int, [C.c_void_p]),
     "ssb_batch_transfer_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "ssb_batch_total_steps": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "ssb_batch_phase_stats": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_float), C.POINTER(C.c_int64)]),
     "ssb_batch_summary": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_Summary)]),
     "ssb_batch_state": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "ssb_batch_events": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32,
@@ -252,6 +253,15 @@ class Batch:
         s = C.c_int64()
         _check(lib().ssb_batch_total_steps(self._h, C.byref(s)))
         return s.value
+
+    def phase_stats(self):
+        """The last launch by phase: [{team_warps, device_ms, steps}, ...] (CUDA-event time of each phase's kernel)."""
+        out = []
+        for k in range(self.launch_info()["phases"]):
+            w, ms, st = C.c_int32(), C.c_float(), C.c_int64()
+            _check(lib().ssb_batch_phase_stats(self._h, k, C.byref(w), C.byref(ms), C.byref(st)))
+            out.append({"team_warps": w.value, "device_ms": ms.value, "steps": st.value})
+        return out
 
     def summary(self, instance):
         s = _Summary()

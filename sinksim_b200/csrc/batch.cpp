@@ -128,6 +128,10 @@ struct Batch::Impl {
   }
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> phaseEv;           // launch phase k ends at phaseEv[k + 1]; phaseEv[0] starts a round
+  DevBuf<unsigned long long> phaseSteps;      // steps per launch phase in the last launch()
+  std::vector<float> lastPhaseMs;
+  std::vector<unsigned long long> lastPhaseSteps;
 
   // model
   DevBuf<double2> colXY, colLH, segXY, segLH;
@@ -264,6 +268,8 @@ Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, c
   check(cudaStreamCreateWithFlags(&I.stream, cudaStreamNonBlocking), "cudaStreamCreate");
   check(cudaEventCreate(&I.ev0), "cudaEventCreate");
   check(cudaEventCreate(&I.ev1), "cudaEventCreate");
+  I.phaseEv.assign(cfg_.phases.size() + 1, nullptr);
+  for (cudaEvent_t& e : I.phaseEv) check(cudaEventCreate(&e), "cudaEventCreate");
   const CompiledShip& S = *I.ship;
   const CompiledSim& M = I.sim;
   cudaStream_t s = I.stream;
@@ -359,6 +365,7 @@ Batch::~Batch() {
     if (I_->stream) cudaStreamSynchronize(I_->stream);
     if (I_->ev0) cudaEventDestroy(I_->ev0);
     if (I_->ev1) cudaEventDestroy(I_->ev1);
+    for (cudaEvent_t e : I_->phaseEv) if (e) cudaEventDestroy(e);
     if (I_->stream) cudaStreamDestroy(I_->stream);
   }
 }
@@ -453,6 +460,7 @@ void Batch::upload() {
   I.nextCurve.alloc(count); check(cudaMemsetAsync(I.nextCurve.get(), 0, I.nextCurve.bytes(), s), "memset");
   I.queue.alloc(1);
   I.remaining.alloc(1);
+  I.phaseSteps.alloc(cfg_.phases.size());
   I.error.alloc(1); check(cudaMemsetAsync(I.error.get(), 0, I.error.bytes(), s), "memset");
 }
 
@@ -464,17 +472,30 @@ float Batch::launch() {
   check(cudaSetDevice(opt_.device), "cudaSetDevice");
   cudaStream_t s = I.stream;
   const long long maxSteps = opt_.stepsPerLaunch > 0 ? opt_.stepsPerLaunch : LLONG_MAX;
+  const std::size_t nph = cfg_.phases.size();
   check(cudaMemcpyAsync(I.remaining.get(), &opt_.count, sizeof(std::int32_t), cudaMemcpyHostToDevice, s), "copy to device");
+  check(cudaMemsetAsync(I.phaseSteps.get(), 0, I.phaseSteps.bytes(), s), "memset");
+  I.lastPhaseMs.assign(nph, 0.0f);
   check(cudaEventRecord(I.ev0, s), "cudaEventRecord");
   int first = 1;
   for (;;) {
     // phase by phase: the instances a phase paused (and any it did not reach) resume in the next phase's larger teams
-    for (const PhaseConfig& p : cfg_.phases) {
+    check(cudaEventRecord(I.phaseEv[0], s), "cudaEventRecord");
+    for (std::size_t k = 0; k < nph; ++k) {
+      const PhaseConfig& p = cfg_.phases[k];
       check(cudaMemsetAsync(I.queue.get(), 0, sizeof(std::int32_t), s), "memset");
       DevBatch db = I.devBatch(opt_, maxSteps, first);
       db.yieldBelow = p.yieldBelow;
+      db.phaseSteps = I.phaseSteps.get() + k;
       check(launch_batch_kernel(opt_.mixedPrecision, p.teamWarps, I.dm, db, p.layout, p.blocks, p.teamsPerBlock, s), "kernel launch");
+      check(cudaEventRecord(I.phaseEv[k + 1], s), "cudaEventRecord");
       first = 0;
+    }
+    check(cudaEventSynchronize(I.phaseEv[nph]), "kernel execution");
+    for (std::size_t k = 0; k < nph; ++k) {
+      float pm = 0;
+      check(cudaEventElapsedTime(&pm, I.phaseEv[k], I.phaseEv[k + 1]), "cudaEventElapsedTime");
+      I.lastPhaseMs[k] += pm;
     }
     if (opt_.stepsPerLaunch <= 0) break;
     std::vector<std::int32_t> stops;
@@ -488,6 +509,8 @@ float Batch::launch() {
   check(cudaEventSynchronize(I.ev1), "kernel execution");
   float ms = 0;
   check(cudaEventElapsedTime(&ms, I.ev0, I.ev1), "cudaEventElapsedTime");
+  I.phaseSteps.download(I.lastPhaseSteps, s);
+  check(cudaStreamSynchronize(s), "copy to host");
   return ms;
 }
 
@@ -540,6 +563,14 @@ std::size_t Batch::download_bytes() const {
   if (opt_.curveEvery > 0) b += I.curveRec.bytes() + I.curveCount.bytes();
   if (opt_.tracedInstances > 0) b += I.denseRec.bytes() + I.sampleRec.bytes() + I.denseCount.bytes() + I.sampleCount.bytes();
   return b;
+}
+
+std::vector<Batch::PhaseStats> Batch::phase_stats() const {
+  const Impl& I = *I_;
+  std::vector<PhaseStats> v;
+  for (std::size_t k = 0; k < I.lastPhaseMs.size() && k < I.lastPhaseSteps.size(); ++k)
+    v.push_back({cfg_.phases[k].teamWarps, I.lastPhaseMs[k], static_cast<std::int64_t>(I.lastPhaseSteps[k])});
+  return v;
 }
 
 std::int64_t Batch::total_steps() const {

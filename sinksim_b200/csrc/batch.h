@@ -92,6 +92,14 @@ class Batch {
   const BatchOptions& options() const { return opt_; }
   const LaunchConfig& launch_config() const { return cfg_; }
   std::int64_t total_steps() const;
+  // The last launch() by phase: its team size, device time (CUDA events around its kernel launches) and the steps its
+  // kernels took.
+  struct PhaseStats {
+    int teamWarps;
+    float deviceMs;
+    std::int64_t steps;
+  };
+  std::vector<PhaseStats> phase_stats() const;
   std::size_t slot_bytes() const;
   std::int32_t nodes() const;
   std::int32_t connections() const;

@@ -71,6 +71,7 @@ __device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
   T.sync();
 
   long long done = B.steps[inst];
+  const long long done0 = done;
   const bool traced = inst < B.traced;
   int denseCount = 0, sampleCount = 0, curveCount = 0;
   double nextSample = 0, nextCurve = 0;
@@ -166,6 +167,7 @@ __device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
     if (traced) { B.denseCount[inst] = denseCount; B.sampleCount[inst] = sampleCount; B.nextSample[inst] = nextSample; }
     if (B.curveEvery > 0) { B.curveCount[inst] = curveCount; B.nextCurve[inst] = nextCurve; }
     if (stop != kRunning) atomicSub(B.remaining, 1);
+    if (B.phaseSteps) atomicAdd(B.phaseSteps, static_cast<unsigned long long>(done - done0));
   }
   if (stop != kRunning && T.warp == 0) {
     double r7[7];

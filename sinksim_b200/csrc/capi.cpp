@@ -178,6 +178,7 @@ int ssb_batch_launch_info(const ssb_batch* b, ssb_launch_info* out) {
     out->tail_team_warps = t.teamWarps; out->tail_teams_per_block = t.teamsPerBlock; out->tail_blocks = t.blocks;
     out->tail_blocks_per_sm = t.blocksPerSM;
     out->slot_bytes = c.slotBytes;
+    out->phases = static_cast<int32_t>(c.phases.size());
   });
 }
 
@@ -239,6 +240,18 @@ int ssb_batch_transfer_bytes(const ssb_batch* b, uint64_t* h2d, uint64_t* d2h) {
     need(b, "batch");
     if (h2d) *h2d = b->batch->upload_bytes();
     if (d2h) *d2h = b->batch->download_bytes();
+  });
+}
+
+int ssb_batch_phase_stats(const ssb_batch* b, int32_t phase, int32_t* team_warps, float* device_ms, int64_t* steps) {
+  return guard([&] {
+    need(b, "batch");
+    const auto v = b->batch->phase_stats();
+    if (v.empty()) throw std::logic_error("phase statistics before the first launch");
+    if (phase < 0 || static_cast<std::size_t>(phase) >= v.size()) throw std::out_of_range("phase " + std::to_string(phase) + " out of range");
+    if (team_warps) *team_warps = v[phase].teamWarps;
+    if (device_ms) *device_ms = v[phase].deviceMs;
+    if (steps) *steps = v[phase].steps;
   });
 }
 

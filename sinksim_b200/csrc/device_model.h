@@ -138,6 +138,8 @@ struct DevBatch {
   // next launch resumes them with larger teams (shorter steps)
   std::int32_t* remaining;
   std::int32_t yieldBelow;
+  // when not null: the steps this launch took, summed over its instances (the per-phase work figure of the timing)
+  unsigned long long* phaseSteps;
 };
 
 // Pose R = Ry(pitch) Rx(roll) and translation (kernel/frame.hpp:9-21), with the single-precision copies the
