@@ -192,45 +192,17 @@ def main():
     from sinksim_b200.files import load_model
     from sinksim_b200.workloads import deck_edge_rule
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
+    from sinksim_b200.shard import Ranks, shard_bounds
 
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    # one process per GPU; each rank steps its own contiguous block of the instances (weak scaling: count per GPU)
+    ranks = Ranks(backend="nccl", timeout_s=600)
+    world, rank, local = ranks.world, ranks.rank, ranks.local
     ship_p, sim_p = model_paths()
     ship, sim = load_model(ship_p, sim_p)
     rule = deck_edge_rule(ship)
+    barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum
 
-    def barrier():
-        if dist:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        import torch
-
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x):
-        if not dist:
-            return x
-        import torch
-
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
-
-    first = rank * args.count
+    first, _ = shard_bounds(args.count * world, world, rank)
     batch = make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local)
     # warm-up: full batches, untimed
     for _ in range(args.warmup):
@@ -298,8 +270,7 @@ def main():
                                              f"reference sinksim_sweep --numerics {args.numerics} --threads {threads}"}
         print(json.dumps(out))
     batch.close()
-    if dist:
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 

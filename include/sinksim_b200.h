@@ -123,6 +123,10 @@ int ssb_batch_set_connection_activation(ssb_batch* b, int32_t instance, int32_t 
  * setters above, as sinksim_cuda_run --sweep does (apps/sinksim_cuda_run.cpp:37-41). The sweep must have exactly
  * opt->count instances. */
 int ssb_batch_apply_sweep(ssb_batch* b, const char* sweep_path);
+/* Instance i takes instance first + i of a sweep file: one GPU's contiguous shard of a sweep run on several GPUs.
+ * Saved results name the instances by those sweep instances' ids. No counterpart in the reference, which runs a
+ * sweep on one GPU; the per-instance setup is sweep::apply as above. */
+int ssb_batch_apply_sweep_range(ssb_batch* b, const char* sweep_path, int32_t first);
 
 /* cuda::Batch::run (engine/cuda/batch.cu:245-308): uploads the instances, runs every one to its end, downloads the
  * results. *seconds (may be NULL) receives the wall time. */
@@ -164,6 +168,11 @@ int ssb_batch_save_results(const ssb_batch* b, const char* sweep_path, const cha
  * *steps and *seconds (may be NULL) receive the aggregate steps and the wall time. */
 int ssb_run_sweep(const char* ship_path, const char* sim_path, const char* sweep_path, const char* numerics, const char* results_path,
                   int64_t* steps, double* seconds);
+/* ssb_run_sweep on instances [first, first + count) of the sweep (count < 0: to its end) on CUDA device `device`:
+ * one GPU's shard of a sweep run on several GPUs (one process per GPU). The results name the instances by their
+ * sweep ids. No counterpart in the reference, whose GPU runner takes a whole sweep on one GPU. */
+int ssb_run_sweep_range(const char* ship_path, const char* sim_path, const char* sweep_path, const char* numerics, int32_t first,
+                        int32_t count, int32_t device, const char* results_path, int64_t* steps, double* seconds);
 /* sinksim_sweep --compare (apps/sinksim_sweep.cpp:19-31, engine/src/sweep.cpp:234-281): exact comparison.
  * *differing receives the count of differing values; first (may be NULL) the first difference. */
 int ssb_compare_results(const char* a_path, const char* b_path, uint64_t* compared, uint64_t* differing, char* first, size_t first_cap);

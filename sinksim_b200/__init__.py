@@ -71,6 +71,7 @@ _SIGNATURES = {
     "ssb_batch_set_connection_area": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double]),
     "ssb_batch_set_connection_activation": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double]),
     "ssb_batch_apply_sweep": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "ssb_batch_apply_sweep_range": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
     "ssb_batch_run": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "ssb_batch_upload": (C.c_int, [C.c_void_p]),
     "ssb_batch_reset": (C.c_int, [C.c_void_p]),
@@ -88,6 +89,8 @@ _SIGNATURES = {
     "ssb_batch_save_trace": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p]),
     "ssb_batch_save_results": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p]),
     "ssb_run_sweep": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
+    "ssb_run_sweep_range": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_char_p,
+                                      C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
     "ssb_compare_results": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]),
     "ssb_portable_math_host": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64]),
     "ssb_portable_math_device": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64]),
@@ -219,8 +222,12 @@ class Batch:
     def set_connection_activation(self, instance, connection, t_on):
         _check(lib().ssb_batch_set_connection_activation(self._h, instance, connection, float(t_on)))
 
-    def apply_sweep(self, sweep_path):
-        _check(lib().ssb_batch_apply_sweep(self._h, _b(sweep_path)))
+    def apply_sweep(self, sweep_path, first=None):
+        """Instance i takes sweep instance i; with `first`, sweep instance first + i (a shard of a longer sweep)."""
+        if first is None:
+            _check(lib().ssb_batch_apply_sweep(self._h, _b(sweep_path)))
+        else:
+            _check(lib().ssb_batch_apply_sweep_range(self._h, _b(sweep_path), int(first)))
 
     # running
     def run(self):
@@ -314,6 +321,14 @@ def run_sweep(ship_path, sim_path, sweep_path, numerics="portable32", results_pa
     """sinksim_cuda_run --sweep in one call; returns (aggregate steps, wall seconds)."""
     steps, secs = C.c_int64(), C.c_double()
     _check(lib().ssb_run_sweep(_b(ship_path), _b(sim_path), _b(sweep_path), numerics.encode(), _b(results_path), C.byref(steps), C.byref(secs)))
+    return steps.value, secs.value
+
+
+def run_sweep_range(ship_path, sim_path, sweep_path, first, count=-1, numerics="portable32", results_path=None, device=0):
+    """run_sweep on sweep instances [first, first + count) on one device (a shard); returns (steps, wall seconds)."""
+    steps, secs = C.c_int64(), C.c_double()
+    _check(lib().ssb_run_sweep_range(_b(ship_path), _b(sim_path), _b(sweep_path), numerics.encode(), int(first), int(count), int(device),
+                                     _b(results_path), C.byref(steps), C.byref(secs)))
     return steps.value, secs.value
 
 

@@ -416,14 +416,17 @@ void Batch::set_connection_activation(std::int32_t inst, std::int32_t c, double 
   I_->hTOn[static_cast<std::size_t>(inst) * I_->NC + static_cast<std::size_t>(c)] = tOn;
 }
 
-void Batch::apply_sweep(const Sweep& sw) {
+void Batch::apply_sweep(const Sweep& sw, std::int32_t first) {
   Impl& I = *I_;
   if (I.uploaded) throw std::logic_error("Batch: set after run");
-  if (static_cast<std::int32_t>(sw.instances.size()) != opt_.count) throw std::invalid_argument("Batch: sweep instance count differs from the batch count");
+  if (first < 0 || static_cast<std::size_t>(first) + static_cast<std::size_t>(opt_.count) > sw.instances.size())
+    throw std::invalid_argument("Batch: sweep instances " + std::to_string(first) + " .. " + std::to_string(first + opt_.count - 1) +
+                                " do not exist (the sweep has " + std::to_string(sw.instances.size()) + ")");
   for (std::int32_t i = 0; i < opt_.count; ++i) {
     const std::size_t o = static_cast<std::size_t>(i) * I.NC;
-    apply_instance(sw.instances[static_cast<std::size_t>(i)], I.sim, I.hEn.data() + o, I.hArea.data() + o, I.hTOn.data() + o);
+    apply_instance(sw.instances[static_cast<std::size_t>(first + i)], I.sim, I.hEn.data() + o, I.hArea.data() + o, I.hTOn.data() + o);
   }
+  sweepFirst_ = first;
 }
 
 void Batch::upload() {
@@ -735,7 +738,7 @@ Results Batch::results(const Sweep* sw) const {
   r.every = opt_.curveEvery;
   for (std::int32_t i = 0; i < opt_.count; ++i) {
     InstanceResult in;
-    in.id = sw ? sw->instances[static_cast<std::size_t>(i)].id : "instance" + std::to_string(i);
+    in.id = sw ? sw->instances[static_cast<std::size_t>(sweepFirst_ + i)].id : "instance" + std::to_string(i);
     const Summary s = summary(i);
     in.foundered = s.foundered; in.founderT = s.founderT; in.tEnd = s.tEnd; in.steps = s.steps;
     const CurveRecord f = final_readouts(i);

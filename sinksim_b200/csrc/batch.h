@@ -76,7 +76,10 @@ class Batch {
   void set_connection_enabled(std::int32_t inst, std::int32_t c, bool en);
   void set_connection_area(std::int32_t inst, std::int32_t c, double area);
   void set_connection_activation(std::int32_t inst, std::int32_t c, double tOn);
-  void apply_sweep(const Sweep& sw);  // instance i takes sweep instance i
+  // Instance i takes sweep instance first + i (a shard of a larger sweep when first > 0 or the sweep is longer);
+  // results() then names the instances by those sweep instances' ids.
+  void apply_sweep(const Sweep& sw, std::int32_t first = 0);
+  std::int32_t sweep_first() const { return sweepFirst_; }
 
   // run() = upload() + launch() + download(); returns the wall seconds of all three.
   double run();
@@ -136,6 +139,7 @@ class Batch {
   std::unique_ptr<Impl> I_;
   BatchOptions opt_;
   LaunchConfig cfg_;
+  std::int32_t sweepFirst_ = 0;
 };
 
 }  // namespace ssb

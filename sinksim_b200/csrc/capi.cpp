@@ -202,7 +202,19 @@ int ssb_batch_apply_sweep(ssb_batch* b, const char* sweep_path) {
   return guard([&] {
     need(b, "batch"); need(sweep_path, "sweep_path");
     auto sw = std::make_unique<ssb::Sweep>(ssb::load_sweep(sweep_path, b->batch->sim()));
+    if (static_cast<std::int32_t>(sw->instances.size()) != b->batch->options().count)
+      throw std::invalid_argument("the sweep has " + std::to_string(sw->instances.size()) + " instances, the batch " +
+                                  std::to_string(b->batch->options().count));
     b->batch->apply_sweep(*sw);
+    b->sweep = std::move(sw);
+  });
+}
+
+int ssb_batch_apply_sweep_range(ssb_batch* b, const char* sweep_path, int32_t first) {
+  return guard([&] {
+    need(b, "batch"); need(sweep_path, "sweep_path");
+    auto sw = std::make_unique<ssb::Sweep>(ssb::load_sweep(sweep_path, b->batch->sim()));
+    b->batch->apply_sweep(*sw, first);
     b->sweep = std::move(sw);
   });
 }
@@ -328,46 +340,64 @@ int ssb_batch_save_results(const ssb_batch* b, const char* sweep_path, const cha
       own = std::make_unique<ssb::Sweep>(ssb::load_sweep(sweep_path, b->batch->sim()));
       sw = own.get();
     }
-    if (sw && static_cast<std::int32_t>(sw->instances.size()) != b->batch->options().count)
-      throw std::invalid_argument("the sweep's instance count differs from the batch's");
+    if (sw && static_cast<std::size_t>(b->batch->sweep_first()) + static_cast<std::size_t>(b->batch->options().count) > sw->instances.size())
+      throw std::invalid_argument("the sweep has fewer instances than the batch's range of it");
     ssb::Results r = b->batch->results(sw);
     if (sw) { r.tMax = sw->tMax; r.every = sw->every; }
     ssb::save_results(r, results_path);
   });
 }
 
+namespace {
+
+// sinksim_cuda_run --sweep on instances [first, first + count) of the sweep (count < 0: to its end).
+void run_sweep_range(const char* ship_path, const char* sim_path, const char* sweep_path, const char* numerics, std::int32_t first,
+                     std::int32_t count, int device, const char* results_path, int64_t* steps, double* seconds) {
+  need(ship_path, "ship_path"); need(sim_path, "sim_path"); need(sweep_path, "sweep_path"); need(numerics, "numerics");
+  const std::string nm = numerics;
+  if (nm != "portable" && nm != "portable32")
+    throw Unsupported("numerics " + nm + " is not available on the GPU engine (use portable or portable32)");
+  need_device();
+  auto ship = ssb::load_ship(ship_path);
+  const ssb::CompiledSim sim = ssb::load_sim(sim_path);
+  ssb::check_pairing(*ship, sim);
+  const ssb::Sweep sw = ssb::load_sweep(sweep_path, sim);
+  const auto total = static_cast<std::int32_t>(sw.instances.size());
+  if (count < 0) count = total - first;
+  if (first < 0 || count < 1 || first + count > total)
+    throw std::invalid_argument("sweep instances " + std::to_string(first) + " .. " + std::to_string(first + count - 1) + " do not exist (the sweep has " +
+                                std::to_string(total) + ")");
+  ssb::BatchOptions opt;
+  opt.stopWhenStable = sw.stopWhenStable;
+  opt.count = count;
+  opt.mixedPrecision = nm == "portable32";
+  opt.tracedInstances = 0;
+  opt.tMax = sw.tMax;
+  opt.curveEvery = sw.every;
+  opt.device = device;
+  ssb::Batch batch(ship, sim, opt);
+  batch.apply_sweep(sw, first);
+  const double s = batch.run();
+  if (steps) *steps = batch.total_steps();
+  if (seconds) *seconds = s;
+  if (results_path) {
+    ssb::Results r = batch.results(&sw);
+    r.tMax = sw.tMax;
+    r.every = sw.every;
+    ssb::save_results(r, results_path);
+  }
+}
+
+}  // namespace
+
 int ssb_run_sweep(const char* ship_path, const char* sim_path, const char* sweep_path, const char* numerics, const char* results_path,
                   int64_t* steps, double* seconds) {
-  return guard([&] {
-    need(ship_path, "ship_path"); need(sim_path, "sim_path"); need(sweep_path, "sweep_path"); need(numerics, "numerics");
-    const std::string nm = numerics;
-    if (nm != "portable" && nm != "portable32")
-      throw Unsupported("numerics " + nm + " is not available on the GPU engine (use portable or portable32)");
-    need_device();
-    auto ship = ssb::load_ship(ship_path);
-    const ssb::CompiledSim sim = ssb::load_sim(sim_path);
-    ssb::check_pairing(*ship, sim);
-    const ssb::Sweep sw = ssb::load_sweep(sweep_path, sim);
-    if (sw.instances.empty()) throw std::invalid_argument("the sweep has no instances");
-    ssb::BatchOptions opt;
-    opt.stopWhenStable = sw.stopWhenStable;
-    opt.count = static_cast<std::int32_t>(sw.instances.size());
-    opt.mixedPrecision = nm == "portable32";
-    opt.tracedInstances = 0;
-    opt.tMax = sw.tMax;
-    opt.curveEvery = sw.every;
-    ssb::Batch batch(ship, sim, opt);
-    batch.apply_sweep(sw);
-    const double s = batch.run();
-    if (steps) *steps = batch.total_steps();
-    if (seconds) *seconds = s;
-    if (results_path) {
-      ssb::Results r = batch.results(&sw);
-      r.tMax = sw.tMax;
-      r.every = sw.every;
-      ssb::save_results(r, results_path);
-    }
-  });
+  return guard([&] { run_sweep_range(ship_path, sim_path, sweep_path, numerics, 0, -1, 0, results_path, steps, seconds); });
+}
+
+int ssb_run_sweep_range(const char* ship_path, const char* sim_path, const char* sweep_path, const char* numerics, int32_t first,
+                        int32_t count, int32_t device, const char* results_path, int64_t* steps, double* seconds) {
+  return guard([&] { run_sweep_range(ship_path, sim_path, sweep_path, numerics, first, count, device, results_path, steps, seconds); });
 }
 
 int ssb_compare_results(const char* a_path, const char* b_path, uint64_t* compared, uint64_t* differing, char* first, size_t first_cap) {
