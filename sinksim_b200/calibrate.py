@@ -1,0 +1,464 @@
+"""Calibration on the batch engine: objectives over instance results, many parameter points per GPU launch.
+
+* The reference's calibration driver (tools/py/calibrate_gpu.py): the oracle's objective against the 1912
+  observations (trim, list, founder time, event times) and its batched random search over connection-kind scales,
+  one GPU batch per round.
+* Gradient calibration on the plain batched engine: a trajectory objective (squared trim and heave residuals at fixed
+  times against a target trajectory), gradients by central finite differences with every point's 2 P + 1 runs in
+  one batch, batched L-BFGS over many restarts, and a torch.autograd.Function whose backward returns those gradients.
+
+Parameters are a vector theta: log scale factors on connection kinds (area = compiled area x exp(theta_k) for every
+connection of kind k: the single product of sweep::apply's kind scale, engine/include/sinksim/sweep.hpp:49-65, so a
+point here and the same scales in a sweep file give the same bits) followed by absolute areas (m2) of chosen
+connections, set after the kind scales as a sweep's connection overrides are.
+
+    python -m sinksim_b200.calibrate search  --observations obs.json [--rounds 5 --batch 264 --span 0.3]
+    python -m sinksim_b200.calibrate lbfgs   [--restarts 64 --iters 30 --seed 1]
+"""
+import argparse
+import json
+import math
+import os
+import random
+import sys
+import time
+
+import numpy as np
+
+KIND_PARAMS = ("breach", "over", "down", "top")
+CURVE_COLUMNS = ("t", "trim", "list", "water", "inflow", "draftF", "draftA")
+
+
+class ParamSpace:
+    """theta -> per-connection areas for one compiled sim."""
+
+    def __init__(self, sim, kinds=KIND_PARAMS, conns=()):
+        names = list(sim["kindNames"])
+        missing = [k for k in kinds if k not in names]
+        if missing:
+            raise ValueError(f"connection kinds {missing} are not in this sim ({names})")
+        kind = np.asarray(sim["kind"])
+        self.kinds = tuple(kinds)
+        self.conns = tuple(int(c) for c in conns)
+        self.area0 = [float(a) for a in sim["area"]]
+        self.members = [[int(c) for c in np.nonzero(kind == names.index(k))[0]] for k in self.kinds]
+        n = len(self.area0)
+        if any(not 0 <= c < n for c in self.conns):
+            raise ValueError("connection index out of range")
+
+    @property
+    def dim(self):
+        return len(self.kinds) + len(self.conns)
+
+    def areas(self, theta):
+        """{connection: area} of one point (only the connections theta touches)."""
+        theta = [float(v) for v in theta]
+        if len(theta) != self.dim:
+            raise ValueError(f"theta has {len(theta)} values, the space {self.dim}")
+        out = {}
+        for k, members in enumerate(self.members):
+            factor = math.exp(theta[k])
+            for c in members:
+                out[c] = self.area0[c] * factor
+        for j, c in enumerate(self.conns):
+            out[c] = theta[len(self.kinds) + j]
+        return out
+
+    def scales(self, theta):
+        """The kind-scale factors of one point, as a sweep instance's "scale" would hold them."""
+        return {k: math.exp(float(theta[i])) for i, k in enumerate(self.kinds)}
+
+
+class InstanceResult(dict):
+    """One instance's results in the batch-results layout: curve (columns of the readout curve), foundered,
+    founderT, events ([{t, id}]) and steps."""
+
+
+def _results_from_batch(batch, sim_doc, count):
+    mon_ids = list(sim_doc["monitors"]["id"])
+    mark_ids = list(sim_doc["marks"]["id"])
+    out = []
+    for i in range(count):
+        s = batch.summary(i)
+        rec = batch.curve(i)
+        curve = {name: [float(v) for v in rec[:, j]] for j, name in enumerate(CURVE_COLUMNS)}
+        events = []
+        for t, ident, kind in batch.events(i):
+            events.append({"t": t, "id": mon_ids[ident] if kind == 0 else mark_ids[ident] if kind == 1 else "founder"})
+        out.append(InstanceResult(curve=curve, foundered=s["foundered"], founderT=s["founder_t"], events=events,
+                                  steps=s["steps"]))
+    return out
+
+
+class BatchEvaluator:
+    """Runs parameter points of one model as the instances of one GPU batch."""
+
+    def __init__(self, ship_path, sim_path, space=None, numerics="portable", t_max=5 * 3600.0, curve_every=30.0, device=0,
+                 rule=None, stop_when_stable=False):
+        from .files import load_model, read_json
+
+        self.ship_path, self.sim_path = ship_path, sim_path
+        _, self.sim = load_model(ship_path, sim_path)
+        self.sim_doc = read_json(sim_path)
+        self.space = space or ParamSpace(self.sim)
+        self.numerics, self.t_max, self.curve_every, self.device = numerics, float(t_max), float(curve_every), device
+        self.rule, self.stop_when_stable = rule, stop_when_stable
+        self.runs = 0
+        self.instances = 0
+        self.device_ms = 0.0
+
+    def run(self, thetas):
+        """Results of every row of thetas ([M, dim]), in order."""
+        from . import Batch
+
+        thetas = np.atleast_2d(np.asarray(thetas, dtype=np.float64))
+        m = thetas.shape[0]
+        b = Batch(self.ship_path, self.sim_path, count=m, numerics=self.numerics, traced_instances=0, t_max=self.t_max,
+                  curve_every=self.curve_every, device=self.device, rule=self.rule, stop_when_stable=self.stop_when_stable)
+        try:
+            for i in range(m):
+                for c, a in self.space.areas(thetas[i]).items():
+                    b.set_connection_area(i, c, a)
+            b.upload()
+            self.device_ms += b.launch()
+            b.download()
+            res = _results_from_batch(b, self.sim_doc, m)
+        finally:
+            b.close()
+        self.runs += 1
+        self.instances += m
+        return res
+
+
+# ------------------------------------------------------------------------------------------ objectives
+
+def interpolate(ts, ys, t, after=None):
+    """Linear interpolation of a curve column at time t (s); past the last record its value (or `after`). The
+    oracle's calibration reads its curves this way (tools/py/sweep.py:93-103)."""
+    if t >= ts[-1]:
+        return ys[-1] if after is None else after
+    for i in range(1, len(ts)):
+        if ts[i] >= t:
+            frac = (t - ts[i - 1]) / (ts[i] - ts[i - 1])
+            return ys[i - 1] + frac * (ys[i] - ys[i - 1])
+    return ys[0]
+
+
+def oracle_terms(inst, obs):
+    """The residual terms of the oracle's calibration objective (tools/py/calibrate_gpu.py:35-64) in its order:
+    (weight, residual / sigma) for each trim point after minute 0, the founder time, each list point and each event
+    (an event that did not happen counts at the founder time; an instance still afloat founders at afloatFounderMin)."""
+    ob = obs["objective"]
+    curve = inst["curve"]
+    sank = bool(inst["foundered"])
+    founder_min = inst["founderT"] / 60 if sank else ob["afloatFounderMin"]
+    founder_s = inst["founderT"] if sank else 1e9
+    terms = []
+    for p in obs["trim"]:
+        minute = p["min"]
+        if minute == 0:
+            continue
+        sigma = next(band["sigma"] for band in ob["trimSigmaByMinute"] if minute <= band["upTo"])
+        model = ob["trimAfterFounder"] if minute * 60 > founder_s else interpolate(curve["t"], curve["trim"], minute * 60)
+        terms.append((1.0, (model - p["deg"]) / sigma))
+    terms.append((1.0, (founder_min - obs["founderMin"]) / ob["founderSigmaMin"]))
+    for p in obs["list"]:
+        minute = p["min"]
+        model = ob["listAfterFounder"] if minute * 60 > founder_s else interpolate(curve["t"], curve["list"], minute * 60)
+        terms.append((ob["listWeight"], (model - p["deg"]) / ob["listSigmaDeg"]))
+    seen = {}
+    for e in inst["events"]:
+        seen[e["id"]] = e["t"] / 60
+    for e in ob["events"]:
+        terms.append((1.0, (seen.get(e["id"], founder_min) - e["obsMin"]) / e["sigmaMin"]))
+    return terms
+
+
+def oracle_objective(inst, obs):
+    """J = sum of weight x (residual / sigma)^2 over oracle_terms, accumulated in order from 0."""
+    total = 0.0
+    for w, r in oracle_terms(inst, obs):
+        total += r ** 2 if w == 1.0 else w * r ** 2
+    return total
+
+
+class TrajectoryObjective:
+    """Sum of squared trim (deg) and heave (m) residuals at fixed times against a target trajectory.
+
+    Heave is the mean of the forward and aft drafts of the readouts. The curve is recorded every `every` seconds and
+    the times are multiples of it, so each value is a record's; an instance that stopped earlier holds its last
+    record."""
+
+    def __init__(self, times, trim, heave):
+        self.times = [float(t) for t in times]
+        self.trim = [float(v) for v in trim]
+        self.heave = [float(v) for v in heave]
+
+    @staticmethod
+    def sample(inst, times):
+        c = inst["curve"]
+        heave_curve = [0.5 * (f + a) for f, a in zip(c["draftF"], c["draftA"])]
+        return ([interpolate(c["t"], c["trim"], t) for t in times], [interpolate(c["t"], heave_curve, t) for t in times])
+
+    @classmethod
+    def from_target(cls, inst, times):
+        trim, heave = cls.sample(inst, times)
+        return cls(times, trim, heave)
+
+    def __call__(self, inst):
+        trim, heave = self.sample(inst, self.times)
+        total = 0.0
+        for k in range(len(self.times)):
+            total += (trim[k] - self.trim[k]) ** 2 + (heave[k] - self.heave[k]) ** 2
+        return total
+
+
+def default_times(t_end=7920.0, n=8):
+    """n equally spaced times ending at t_end (s): 990 s apart for 8 times in 2.2 h (7,920 s)."""
+    return [t_end * (k + 1) / n for k in range(n)]
+
+
+# ------------------------------------------------------------------------------------------ gradients
+
+def fd_steps(theta, h_rel):
+    """Central-difference step per parameter: h_rel x max(|theta_i|, 1)."""
+    return h_rel * np.maximum(np.abs(theta), 1.0)
+
+
+def fd_stencil(thetas, h_rel):
+    """The points of central differences around each row of thetas ([R, P]): rows [R x (2 P + 1), P], per point its
+    centre, then +h and -h along each parameter in turn."""
+    thetas = np.atleast_2d(np.asarray(thetas, dtype=np.float64))
+    r, p = thetas.shape
+    out = np.empty((r, 2 * p + 1, p))
+    for i in range(r):
+        h = fd_steps(thetas[i], h_rel)
+        out[i, 0] = thetas[i]
+        for j in range(p):
+            out[i, 1 + 2 * j] = thetas[i]
+            out[i, 1 + 2 * j, j] += h[j]
+            out[i, 2 + 2 * j] = thetas[i]
+            out[i, 2 + 2 * j, j] -= h[j]
+    return out.reshape(r * (2 * p + 1), p)
+
+
+def fd_reduce(thetas, values, h_rel):
+    """Objective and central-difference gradient per point from the stencil's objective values."""
+    thetas = np.atleast_2d(np.asarray(thetas, dtype=np.float64))
+    r, p = thetas.shape
+    v = np.asarray(values, dtype=np.float64).reshape(r, 2 * p + 1)
+    f = v[:, 0].copy()
+    g = np.empty((r, p))
+    for i in range(r):
+        h = fd_steps(thetas[i], h_rel)
+        # (theta + h) - (theta - h) as the stencil rounded it
+        for j in range(p):
+            span = (thetas[i, j] + h[j]) - (thetas[i, j] - h[j])
+            g[i, j] = (v[i, 1 + 2 * j] - v[i, 2 + 2 * j]) / span
+    return f, g
+
+
+def value_and_grad(evaluator, objective, thetas, h_rel=1e-6):
+    """Objective and its central-difference gradient at every row of thetas, all from one batch."""
+    pts = fd_stencil(thetas, h_rel)
+    vals = [objective(inst) for inst in evaluator.run(pts)]
+    return fd_reduce(thetas, vals, h_rel)
+
+
+# ------------------------------------------------------------------------------------------ optimisers
+
+def lbfgs_batched(fg, x0, max_iter=50, memory=8, f_target=None, rel_tol=1e-12, c1=1e-4, max_backtracks=12, callback=None):
+    """L-BFGS on many independent starting points at once; fg(X [K, P]) -> (f [K], g [K, P]) evaluates all of its rows
+    in one call (one GPU batch).
+
+    Each iteration evaluates every active point's trial step together; a point whose trial fails the Armijo test
+    halves its step and retries in the next call. A point stops when f <= f_target, when its relative decrease falls
+    below rel_tol, or after max_iter iterations. Returns (x, f, info) with info = {iterations, evaluations,
+    history: [best f after each call]}."""
+    x = np.array(x0, dtype=np.float64, copy=True)
+    r, p = x.shape
+    f, g = fg(x)
+    f = np.asarray(f, dtype=np.float64)
+    g = np.asarray(g, dtype=np.float64)
+    S = [[] for _ in range(r)]
+    Y = [[] for _ in range(r)]
+    active = np.ones(r, dtype=bool)
+    if f_target is not None:
+        active &= f > f_target
+    iters = np.zeros(r, dtype=int)
+    calls = 1
+    history = [float(np.min(f))]
+
+    def direction(i):
+        q = g[i].copy()
+        alphas = []
+        for s, y in zip(reversed(S[i]), reversed(Y[i])):
+            rho = 1.0 / float(y @ s)
+            a = rho * float(s @ q)
+            alphas.append((a, rho, s, y))
+            q -= a * y
+        if S[i]:
+            s, y = S[i][-1], Y[i][-1]
+            q *= float(s @ y) / float(y @ y)
+        for a, rho, s, y in reversed(alphas):
+            b = rho * float(y @ q)
+            q += (a - b) * s
+        d = -q
+        if float(d @ g[i]) >= 0:  # not a descent direction: restart from steepest descent
+            S[i].clear()
+            Y[i].clear()
+            d = -g[i]
+        return d
+
+    dirs = np.zeros_like(x)
+    steps = np.ones(r)
+    backtracks = np.zeros(r, dtype=int)
+    fresh = np.ones(r, dtype=bool)  # needs a new direction
+    while active.any():
+        idx = np.nonzero(active)[0]
+        for i in idx:
+            if fresh[i]:
+                dirs[i] = direction(i)
+                gnorm = float(np.linalg.norm(g[i]))
+                steps[i] = 1.0 if S[i] else min(1.0, 0.1 / max(gnorm, 1e-300))
+                backtracks[i] = 0
+                fresh[i] = False
+        trial = x[idx] + steps[idx, None] * dirs[idx]
+        ft, gt = fg(trial)
+        calls += 1
+        for k, i in enumerate(idx):
+            slope = float(dirs[i] @ g[i])
+            if ft[k] <= f[i] + c1 * steps[i] * slope:
+                s = trial[k] - x[i]
+                y = gt[k] - g[i]
+                if float(y @ s) > 1e-300:
+                    S[i].append(s)
+                    Y[i].append(y)
+                    if len(S[i]) > memory:
+                        S[i].pop(0)
+                        Y[i].pop(0)
+                decrease = f[i] - ft[k]
+                x[i], f[i], g[i] = trial[k], ft[k], gt[k]
+                iters[i] += 1
+                fresh[i] = True
+                if (f_target is not None and f[i] <= f_target) or iters[i] >= max_iter or decrease <= rel_tol * max(abs(f[i]), 1e-300):
+                    active[i] = False
+            else:
+                steps[i] *= 0.5
+                backtracks[i] += 1
+                if backtracks[i] > max_backtracks:
+                    active[i] = False
+        history.append(float(np.min(f)))
+        if callback:
+            callback(calls, x, f)
+    return x, f, {"iterations": iters, "evaluations": calls, "history": history}
+
+
+def random_search(evaluator, objective, kinds=KIND_PARAMS, rounds=5, batch=264, span=0.3, shrink=0.5, seed=20261008, log=None):
+    """The reference's batched search (tools/py/calibrate_gpu.py:96-125): each round one batch of log-uniform points
+    around the current best (the origin, the compiled model's own values, first), keep the best, shrink the box.
+    Points are drawn from random.Random(seed) in the reference's order. Returns (best J, best log scales, history)."""
+    rng = random.Random(seed)
+    centre = {k: 0.0 for k in kinds}
+    best = (math.inf, None)
+    history = []
+    for rnd in range(rounds):
+        points = [{k: 0.0 for k in kinds}] if rnd == 0 else []
+        while len(points) < batch:
+            points.append({k: centre[k] + rng.uniform(-span, span) for k in kinds})
+        thetas = np.array([[p[k] for k in kinds] for p in points])
+        t0 = time.time()
+        scores = [objective(inst) for inst in evaluator.run(thetas)]
+        order = sorted(range(len(points)), key=lambda i: scores[i])
+        top = order[0]
+        history.append({"round": rnd, "points": len(points), "seconds": time.time() - t0, "best": scores[top],
+                        "scales": {k: math.exp(v) for k, v in points[top].items()}})
+        if log:
+            log(history[-1])
+        if scores[top] < best[0]:
+            best = (scores[top], dict(points[top]))
+        centre = dict(points[top])
+        span *= shrink
+    return best[0], best[1], history
+
+
+# ------------------------------------------------------------------------------------------ torch
+
+def batch_loss(theta, evaluator, objective, h_rel=1e-6):
+    """Objective of every row of theta (a float64 torch tensor [R, P]) as a differentiable torch value: the forward
+    runs the points and their central-difference stencils in one batch; the backward returns those gradients."""
+    import torch
+
+    class _BatchObjective(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, th):
+            f, g = value_and_grad(evaluator, objective, th.detach().cpu().numpy(), h_rel)
+            ctx.save_for_backward(torch.as_tensor(g, dtype=th.dtype, device=th.device))
+            return torch.as_tensor(f, dtype=th.dtype, device=th.device)
+
+        @staticmethod
+        def backward(ctx, grad_out):
+            (g,) = ctx.saved_tensors
+            return grad_out[:, None] * g
+
+    return _BatchObjective.apply(theta)
+
+
+# ------------------------------------------------------------------------------------------ command line
+
+def _model_paths(args):
+    from .files import decompressed
+
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    ship = args.ship or decompressed(os.path.join(here, "tests", "golden", "titanic64.ship.json.gz"))
+    sim = args.sim or decompressed(os.path.join(here, "tests", "golden", "titanic.sim.json.gz"))
+    return ship, sim
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(prog="python -m sinksim_b200.calibrate")
+    ap.add_argument("mode", choices=("search", "lbfgs"))
+    ap.add_argument("--ship")
+    ap.add_argument("--sim")
+    ap.add_argument("--numerics", default="portable")
+    ap.add_argument("--observations", help="observations file (search mode)")
+    ap.add_argument("--rounds", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=264)
+    ap.add_argument("--span", type=float, default=0.3)
+    ap.add_argument("--shrink", type=float, default=0.5)
+    ap.add_argument("--seed", type=int, default=20261008)
+    ap.add_argument("--restarts", type=int, default=64)
+    ap.add_argument("--iters", type=int, default=30)
+    ap.add_argument("--h", type=float, default=1e-6, help="relative central-difference step")
+    args = ap.parse_args(argv)
+    ship, sim = _model_paths(args)
+    if args.mode == "search":
+        if not args.observations:
+            ap.error("search needs --observations")
+        with open(args.observations) as f:
+            obs = json.load(f)
+        ob = obs["objective"]
+        ev = BatchEvaluator(ship, sim, numerics=args.numerics, t_max=ob["tMaxMin"] * 60, curve_every=ob["historyEverySec"])
+        J, p, _ = random_search(ev, lambda inst: oracle_objective(inst, obs), rounds=args.rounds, batch=args.batch, span=args.span,
+                                shrink=args.shrink, seed=args.seed, log=lambda h: print(json.dumps(h)))
+        print(json.dumps({"best": J, "scales": {k: math.exp(v) for k, v in p.items()}, "instances": ev.instances,
+                          "device_s": ev.device_ms / 1e3}))
+        return 0
+    # lbfgs: hidden kind scales drawn from the seed, the target trajectory from them, restarts from lognormal draws
+    times = default_times()
+    rng = np.random.default_rng(args.seed)
+    ev = BatchEvaluator(ship, sim, numerics=args.numerics, t_max=times[-1], curve_every=times[1] - times[0])
+    hidden = rng.normal(0.0, 0.3, size=ev.space.dim)
+    target = TrajectoryObjective.from_target(ev.run(hidden[None, :])[0], times)
+    x0 = rng.normal(0.0, 0.3, size=(args.restarts, ev.space.dim))
+    t0 = time.time()
+    x, fx, info = lbfgs_batched(lambda X: value_and_grad(ev, target, X, args.h), x0, max_iter=args.iters)
+    best = int(np.argmin(fx))
+    print(json.dumps({"restarts": args.restarts, "best_objective": float(fx[best]), "recovery_error": float(np.max(np.abs(x[best] - hidden))),
+                      "evaluations": info["evaluations"], "instances": ev.instances, "wall_s": time.time() - t0,
+                      "device_s": ev.device_ms / 1e3}))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,93 @@
+"""Calibration host logic: the oracle's objective restated (checked against the reference's own scores of the
+reference CPU engine's results), the parameter mapping, the central-difference stencil and the batched L-BFGS."""
+import gzip
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from _support import GOLDEN, load_model, titanic
+from sinksim_b200.calibrate import (ParamSpace, TrajectoryObjective, default_times, fd_reduce, fd_stencil, interpolate, lbfgs_batched,
+                                    oracle_objective)
+
+
+def _obs():
+    with open(os.path.join(GOLDEN, "titanic-1912.observations.json")) as f:
+        return json.load(f)
+
+
+def test_oracle_objective_equals_the_reference_scores():
+    with open(os.path.join(GOLDEN, "calibration.points.json")) as f:
+        pts = json.load(f)
+    with gzip.open(os.path.join(GOLDEN, "calibration.results.json.gz"), "rt") as f:
+        res = json.load(f)
+    obs = _obs()
+    for inst, J in zip(res["instances"], pts["J"]):
+        assert oracle_objective(inst, obs) == J
+    assert abs(pts["J"][0] - 10.4395) < 1e-3  # the compiled model's own values (kind scales 1)
+
+
+def test_interpolate():
+    ts, ys = [0.0, 10.0, 20.0], [1.0, 3.0, 2.0]
+    assert interpolate(ts, ys, 5.0) == 2.0
+    assert interpolate(ts, ys, 20.0) == 2.0 and interpolate(ts, ys, 25.0, after=7.0) == 7.0
+    assert interpolate(ts, ys, 0.0) == 1.0
+
+
+def test_param_space_is_the_sweep_product():
+    _, sim = load_model(*titanic())
+    sp = ParamSpace(sim, conns=(3,))
+    theta = [0.1, -0.2, 0.05, 0.3, 0.123]
+    a = sp.areas(theta)
+    kinds = list(sim["kindNames"])
+    for c, area in a.items():
+        if c == 3:
+            assert area == 0.123
+            continue
+        k = sp.kinds.index(kinds[int(sim["kind"][c])])
+        assert area == float(sim["area"][c]) * math.exp(theta[k])
+    assert sp.scales(theta) == {k: math.exp(theta[i]) for i, k in enumerate(sp.kinds)}
+    with pytest.raises(ValueError):
+        sp.areas([0.0])
+
+
+def test_central_differences_of_a_quadratic():
+    A = np.array([[3.0, 0.5, 0.0], [0.5, 2.0, 0.1], [0.0, 0.1, 1.0]])
+    thetas = np.array([[0.3, -0.2, 1.5], [2.0, 0.1, -3.0]])
+    pts = fd_stencil(thetas, 1e-6)
+    assert pts.shape == (2 * 7, 3)
+    vals = [0.5 * p @ A @ p for p in pts]
+    f, g = fd_reduce(thetas, vals, 1e-6)
+    assert np.allclose(f, [0.5 * t @ A @ t for t in thetas])
+    assert np.allclose(g, thetas @ A, rtol=1e-6, atol=1e-7)
+
+
+def test_batched_lbfgs_finds_every_rosenbrock_minimum():
+    calls = []
+
+    def fg(X):
+        calls.append(len(X))
+        x, y = X[:, 0], X[:, 1]
+        f = (1 - x) ** 2 + 100 * (y - x * x) ** 2
+        g = np.stack([-2 * (1 - x) - 400 * x * (y - x * x), 200 * (y - x * x)], axis=1)
+        return f, g
+
+    x0 = np.random.default_rng(7).uniform(-2, 2, size=(16, 2))
+    x, f, info = lbfgs_batched(fg, x0, max_iter=500, f_target=1e-14)
+    assert np.all(f < 1e-12), f
+    assert np.allclose(x, 1.0, atol=1e-6)
+    assert info["evaluations"] == len(calls) and max(calls) == 16
+
+
+def test_trajectory_objective():
+    times = default_times()
+    assert len(times) == 8 and times[0] == 990.0 and times[-1] == 7920.0
+    t = [990.0 * k for k in range(9)]
+    inst = {"curve": {"t": t, "trim": [0.01 * k for k in range(9)], "draftF": [10 + 0.1 * k for k in range(9)],
+                      "draftA": [10.0] * 9}}
+    obj = TrajectoryObjective.from_target(inst, times)
+    assert obj(inst) == 0.0
+    other = {"curve": dict(inst["curve"], trim=[0.02 * k for k in range(9)])}
+    assert obj(other) == pytest.approx(sum((0.01 * k) ** 2 for k in range(1, 9)))
