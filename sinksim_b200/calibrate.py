@@ -220,6 +220,13 @@ def default_times(t_end=7920.0, n=8):
 
 # ------------------------------------------------------------------------------------------ gradients
 
+# The simulated objectives are smooth only at coarse scales: connection limiters switch, Newton iteration counts and
+# threshold crossings change from one parameter value to the next, so central differences with relative steps of 1e-4
+# and below are noise (on titanic64, 1.1 h trajectory: a derivative of about -7 at steps of 1e-2 and 1e-3 reads -15 at
+# 1e-4, -76 at 1e-6 and 2e4 at 1e-8). The default step is 1e-2.
+DEFAULT_FD_STEP = 1e-2
+
+
 def fd_steps(theta, h_rel):
     """Central-difference step per parameter: h_rel x max(|theta_i|, 1)."""
     return h_rel * np.maximum(np.abs(theta), 1.0)
@@ -258,7 +265,7 @@ def fd_reduce(thetas, values, h_rel):
     return f, g
 
 
-def value_and_grad(evaluator, objective, thetas, h_rel=1e-6):
+def value_and_grad(evaluator, objective, thetas, h_rel=DEFAULT_FD_STEP):
     """Objective and its central-difference gradient at every row of thetas, all from one batch."""
     pts = fd_stencil(thetas, h_rel)
     vals = [objective(inst) for inst in evaluator.run(pts)]
@@ -384,7 +391,7 @@ def random_search(evaluator, objective, kinds=KIND_PARAMS, rounds=5, batch=264, 
 
 # ------------------------------------------------------------------------------------------ torch
 
-def batch_loss(theta, evaluator, objective, h_rel=1e-6):
+def batch_loss(theta, evaluator, objective, h_rel=DEFAULT_FD_STEP):
     """Objective of every row of theta (a float64 torch tensor [R, P]) as a differentiable torch value: the forward
     runs the points and their central-difference stencils in one batch; the backward returns those gradients."""
     import torch
@@ -429,7 +436,7 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=20261008)
     ap.add_argument("--restarts", type=int, default=64)
     ap.add_argument("--iters", type=int, default=30)
-    ap.add_argument("--h", type=float, default=1e-6, help="relative central-difference step")
+    ap.add_argument("--h", type=float, default=DEFAULT_FD_STEP, help="relative central-difference step")
     args = ap.parse_args(argv)
     ship, sim = _model_paths(args)
     if args.mode == "search":
