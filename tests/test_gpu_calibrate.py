@@ -60,5 +60,5 @@ def test_torch_loss_gradient_is_the_batch_central_difference():
     loss = batch_loss(theta, ev, target).sum()
     loss.backward()
     f, g = value_and_grad(ev, target, x0)
-    assert float(loss) == float(np.sum(f))
+    assert float(loss.detach()) == float(np.sum(f))
     assert np.array_equal(theta.grad.numpy(), g)
