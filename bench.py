@@ -53,12 +53,24 @@ def parse():
     ap.add_argument("--count", type=int, default=4096, help="instances per GPU")
     ap.add_argument("--tmax", type=float, default=5 * 3600.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--model", default="titanic64", choices=("titanic64", "liner"),
+                    help="titanic64: the reference's compiled model; liner: the generated benchmark liner")
     return ap.parse_args()
 
 
-def model_paths():
+MODELS = {
+    "titanic64": "titanic64 (4408 columns, 64 spaces, 290 connections; the reference's compiled model)",
+    "liner": "liner269 (generated 269 x 28 m liner: 4408 columns, 64 spaces, 290 connections)",
+}
+
+
+def model_paths(model="titanic64"):
     from sinksim_b200.files import decompressed
 
+    if model == "liner":
+        from sinksim_b200 import hullgen
+
+        return hullgen.write(os.path.join(tempfile.gettempdir(), "sinksim_b200_bench_liner"))
     golden = os.path.join(ROOT, "tests", "golden")
     return decompressed(os.path.join(golden, "titanic64.ship.json.gz")), decompressed(os.path.join(golden, "titanic.sim.json.gz"))
 
@@ -150,7 +162,7 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    ship_p, sim_p = model_paths()
+    ship_p, sim_p = model_paths(args.model)
     from sinksim_b200.files import load_model
 
     _, sim = load_model(ship_p, sim_p)
@@ -175,7 +187,7 @@ def reference_arm(args):
 
 
 def workload_config(args):
-    return {"workload": f"titanic64 uneven-run-length batch, {args.count} instances per GPU", "model": "titanic64 (4408 columns, 64 spaces, 290 connections)",
+    return {"workload": f"{args.model} uneven-run-length batch, {args.count} instances per GPU", "model": MODELS[args.model],
             "global_batch": args.count * args.gpus, "numerics": args.numerics, "t_max_s": args.tmax, "dt_s": 0.25,
             "retire": "founder | sink (|trim|>15 deg, bow deck edge under) | settle (|pitch rate|<1e-5 rad/s for 600 s) | tMax",
             "parallelism": f"instances sharded over {args.gpus} GPU(s), no collective in the step",
@@ -197,7 +209,7 @@ def main():
     # one process per GPU; each rank steps its own contiguous block of the instances (weak scaling: count per GPU)
     ranks = Ranks(backend="nccl", timeout_s=600)
     world, rank, local = ranks.world, ranks.rank, ranks.local
-    ship_p, sim_p = model_paths()
+    ship_p, sim_p = model_paths(args.model)
     ship, sim = load_model(ship_p, sim_p)
     rule = deck_edge_rule(ship)
     barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum

@@ -13,7 +13,7 @@ and mass recipe in oracle/js/core/core.js:192-330, 716-824). This module builds 
 * connections: bulkhead-top weirs and doors (area U(1, 3) m2, sill U(0, 1) m, closed) between longitudinally adjacent
   spaces (the bulkhead weirs' crest is the bulkhead deck's height where the deck is lower), two deck openings
   (U(0.5, 4) m2) between each space and the one above plus extra hatches amidships, weather-deck openings to the sea,
-  and breaches below the waterline in the forward compartments, on alternating sides;
+  and breaches below the waterline in the forward compartments, on alternating sides (the last ones closed);
 * mass for an even-keel draft T with metacentric height GM; inertia, added mass and damping from critical-damping
   fractions of the intact hydrostatics (the reference's recipe, core.js:800-816); the state at rest at that draft;
 * every hashed array carries the FNV-1a 64-bit hash the loader verifies (hashing order of export_compiled.js:24-33,
@@ -78,11 +78,11 @@ class HullSpec:
     """Dimensions of a parametric liner (metres); the defaults are the 269 x 28 m benchmark liner."""
 
     def __init__(self, L=269.0, B=28.0, depth=18.0, sheer=4.0, nx=152, ny=29, n_comp=16, n_decks=4, draft=10.5, gm=0.8,
-                 end_rise=3.0, breaches=6, breach_area=1.2, top_openings=4, extra_hatches=4, dt=0.25, bulkhead_top=13.5):
+                 end_rise=3.0, breaches=6, reserve_breaches=2, breach_area=1.2, top_openings=4, extra_hatches=2, dt=0.25, bulkhead_top=13.5):
         self.L, self.B, self.depth, self.sheer = float(L), float(B), float(depth), float(sheer)
         self.nx, self.ny, self.n_comp, self.n_decks = int(nx), int(ny), int(n_comp), int(n_decks)
         self.draft, self.gm, self.end_rise = float(draft), float(gm), float(end_rise)
-        self.breaches, self.breach_area, self.dt = int(breaches), float(breach_area), float(dt)
+        self.breaches, self.reserve_breaches, self.breach_area, self.dt = int(breaches), int(reserve_breaches), float(breach_area), float(dt)
         self.top_openings, self.extra_hatches, self.bulkhead_top = int(top_openings), int(extra_hatches), float(bulkhead_top)
 
     def half_breadth(self, x):
@@ -254,17 +254,19 @@ def build_connections(spec, cols, nodes, rng):
         d = j % (nd - 1)
         x = 0.5 * spec.L - (k + 0.5) * comp_len
         add(k * nd + d, k * nd + d + 1, ORIFICE, x, 0.0, floors[d + 1], rng.uniform(0.5, 4.0), K_DOWN, k, True)
-    # breaches: below the waterline in the forward compartments (from the second), shares of the total area
+    # breaches: below the waterline in the forward compartments (from the second), on alternating sides; the first
+    # `breaches` share the total area and are open, the reserve ones aft of them are closed (a sweep may open them)
     w = rng.uniform(0.5, 1.5, size=spec.breaches)
     w = w / w.sum()
-    for j in range(spec.breaches):
+    for j in range(spec.breaches + spec.reserve_breaches):
         k = min(1 + j, ncmp - 1)
         x = 0.5 * spec.L - (k + rng.uniform(0.3, 0.7)) * comp_len
         z = spec.draft - rng.uniform(2.0, 4.0)
         z = max(z, float(spec.bottom(x)) + 0.5)
         d = max(dd for dd in range(nd) if floors[dd] <= z)
-        side = -1.0 if j % 2 == 0 else 1.0  # alternating sides
-        add(-1, k * nd + d, ORIFICE, x, side * float(spec.half_breadth(x)), z, float(spec.breach_area * w[j]), K_BREACH, j + 1, True)
+        side = -1.0 if j % 2 == 0 else 1.0
+        area = float(spec.breach_area * w[j]) if j < spec.breaches else float(spec.breach_area / spec.breaches)
+        add(-1, k * nd + d, ORIFICE, x, side * float(spec.half_breadth(x)), z, area, K_BREACH, j + 1, j < spec.breaches)
     C["n"] = len(C["a"])
     return C
 

@@ -28,8 +28,9 @@ def test_liner_shape(liner):
     assert sim["connections"]["n"] == 290
     kinds = sim["connections"]["kindNames"]
     k = np.array(sim["connections"]["kind"])
-    breach = k == kinds.index("breach")
-    assert breach.sum() == 6
+    breach = (k == kinds.index("breach")) & (np.array(sim["connections"]["en"]) == 1)
+    assert breach.sum() == 6                                   # six open breaches, and two closed ones aft of them
+    assert (k == kinds.index("breach")).sum() == 8
     assert np.isclose(np.array(sim["connections"]["area"])[breach].sum(), 1.2)
     doors = np.array(sim["connections"]["area"])[k == kinds.index("door")]
     assert doors.min() >= 1.0 and doors.max() <= 3.0
