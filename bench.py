@@ -40,7 +40,7 @@ FP64_OPS_PER_STEP = 7 * 4408 + 11 * 4058 + 10 * 9422 + 11.5 * 4174 + 71 * 31 + 1
 # duration of run_batch<portable, 2-warp teams> on the same batch run to 600 s: python bench.py --count 4096 --tmax 600).
 # The traffic is the instances' state going in and out: the geometry and the running state stay on chip, so the figure
 # does not grow with the steps a launch takes.
-KERNEL_DRAM_BYTES_PER_LAUNCH = 25.3e6
+KERNEL_DRAM_BYTES_PER_LAUNCH = 24.6e6
 
 
 def parse():
