@@ -109,6 +109,15 @@ void ssb_batch_options_init(ssb_batch_options* opt);
  * engine/src/compiled.cpp:108-279) and creates a batch of opt->count instances of it
  * (cuda::Batch::Batch, engine/cuda/batch.cu:170-209). */
 int ssb_batch_create(const char* ship_path, const char* sim_path, const ssb_batch_options* opt, ssb_batch** out);
+/* A fleet: instances of several compiled models in one batch, stepped in the same launches (no counterpart in the
+ * reference, which runs one model per batch). instance_model[i] (opt->count entries) picks instance i's model among
+ * the n_models ship/sim pairs. Per-instance setters, runs, summaries, states, events, curves and final readouts work
+ * as for one model, with each instance's own node and connection counts (ssb_batch_instance_shape); sweeps, traces,
+ * batch-results files and the no-allocation run take a batch of one model and return SSB_EINVAL / SSB_ESTATE here. */
+int ssb_fleet_create(int32_t n_models, const char* const* ship_paths, const char* const* sim_paths, const int32_t* instance_model,
+                     const ssb_batch_options* opt, ssb_batch** out);
+/* Instance i's model (index into the fleet's models; 0 for a batch of one model), node count and connection count. */
+int ssb_batch_instance_shape(const ssb_batch* b, int32_t instance, int32_t* model, int32_t* nodes, int32_t* connections);
 void ssb_batch_destroy(ssb_batch* b);
 int ssb_batch_nodes(const ssb_batch* b, int32_t* nodes, int32_t* connections);
 int ssb_batch_launch_info(const ssb_batch* b, ssb_launch_info* out);

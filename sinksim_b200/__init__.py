@@ -71,6 +71,8 @@ _SIGNATURES = {
     "ssb_batch_set_connection_area": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double]),
     "ssb_batch_set_connection_activation": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double]),
     "ssb_batch_apply_sweep": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "ssb_fleet_create": (C.c_int, [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), C.POINTER(C.c_int32), C.c_void_p, C.POINTER(C.c_void_p)]),
+    "ssb_batch_instance_shape": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "ssb_batch_apply_sweep_range": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
     "ssb_batch_run": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "ssb_batch_upload": (C.c_int, [C.c_void_p]),
@@ -163,7 +165,7 @@ class Batch:
 
     def __init__(self, ship_path, sim_path, count=1, numerics="portable32", traced_instances=0, dense_steps=400, sample_every=60.0,
                  curve_every=0.0, t_max=5 * 3600.0, steps_per_launch=0, team_warps=0, tail_team_warps=-1, teams_per_block=0, yield_below=-1,
-                 blocks=0, device=0, rule=None, stop_when_stable=False, handover_factor=0.0):
+                 blocks=0, device=0, rule=None, stop_when_stable=False, handover_factor=0.0, _fleet=None):
         if numerics not in NUMERICS:
             raise SinksimError(-4, f"numerics {numerics!r} is not available on the GPU (portable or portable32)")
         o = _Options()
@@ -179,13 +181,34 @@ class Batch:
             o.rule_pitch, o.rule_x, o.rule_y, o.rule_z = rule["pitch"], rule["x"], rule["y"], rule["z"]
             o.rule_wth, o.rule_settle = rule["wth"], rule["settle"]
         h = C.c_void_p()
-        _check(lib().ssb_batch_create(_b(ship_path), _b(sim_path), C.byref(o), C.byref(h)))
+        if _fleet is None:
+            _check(lib().ssb_batch_create(_b(ship_path), _b(sim_path), C.byref(o), C.byref(h)))
+        else:
+            models, instance_model = _fleet
+            ships = (C.c_char_p * len(models))(*[_b(s) for s, _ in models])
+            sims = (C.c_char_p * len(models))(*[_b(m) for _, m in models])
+            im = (C.c_int32 * count)(*[int(v) for v in instance_model])
+            _check(lib().ssb_fleet_create(len(models), ships, sims, im, C.byref(o), C.byref(h)))
         self._h = h
         self.count = count
         self.numerics = numerics
         n, c = C.c_int32(), C.c_int32()
         _check(lib().ssb_batch_nodes(self._h, C.byref(n), C.byref(c)))
         self.nodes, self.connections = n.value, c.value
+
+    @classmethod
+    def fleet(cls, models, instance_model, **options):
+        """Instances of several models in one batch: models = [(ship_path, sim_path), ...], instance_model[i] = the model
+        of instance i. Options as for Batch (count is len(instance_model)); no traces, sweeps or batch-results files."""
+        instance_model = list(instance_model)
+        options.pop("count", None)
+        return cls(None, None, count=len(instance_model), _fleet=(list(models), instance_model), **options)
+
+    def instance_shape(self, instance):
+        """(model index, nodes, connections) of one instance."""
+        m, n, c = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(lib().ssb_batch_instance_shape(self._h, instance, C.byref(m), C.byref(n), C.byref(c)))
+        return m.value, n.value, c.value
 
     def close(self):
         if getattr(self, "_h", None):
@@ -277,7 +300,7 @@ class Batch:
                     t_end=s.t_end, steps=s.steps, event_count=s.event_count, curve_count=s.curve_count, outputs=list(s.outputs))
 
     def state(self, instance):
-        r = np.empty(10 + 5 * self.nodes)
+        r = np.empty(10 + 5 * self.instance_shape(instance)[1])
         _check(lib().ssb_batch_state(self._h, instance, _dptr(r)))
         return r
 

@@ -54,19 +54,118 @@ class DevBuf {
   }
 };
 
-template <class T>
-std::vector<T> repeat(const std::vector<T>& v, std::size_t times) {
-  std::vector<T> out;
-  out.reserve(v.size() * times);
-  for (std::size_t i = 0; i < times; ++i) out.insert(out.end(), v.begin(), v.end());
-  return out;
-}
 
 std::uint32_t take(std::uint32_t& off, std::size_t bytes) {
   const std::uint32_t at = off;
   off = static_cast<std::uint32_t>((off + bytes + 15) & ~static_cast<std::size_t>(15));
   return at;
 }
+
+// One compiled model on the device: its geometry in the kernel's layout (paired fields, the segment -> column gather
+// resolved, float copies), its node, group, connection, incidence, monitor and mark tables, and the DevModel that
+// points into them.
+struct ModelDev {
+  std::shared_ptr<const CompiledShip> ship;
+  CompiledSim sim;
+  Incidence inc;
+  MonitorLists mons;
+  std::int32_t NN = 0, NC = 0, NG = 0, nmon = 0, nmark = 0, evCap = 0, maxGroup = 0;
+  DevBuf<double2> colXY, colLH, segXY, segLH;
+  DevBuf<float2> colXYf, colLHf, segXYf, segLHf;
+  DevBuf<float> colAf, segArf;
+  DevBuf<double> colA, segAr, mu, vmax, amin, aov;
+  DevBuf<std::int32_t> segStart, segCount, gStart, gCount, gNodes, ca, cb, skip, incStart, incCount, incConn, sea, monStart, monCount, monConn;
+  DevBuf<std::uint8_t> gMode, law, incSide, mkWhen;
+  DevBuf<double> gpx, gpy, gpz, kx, ky, kz, coef, mkx, mky, mkz;
+  DevModel dm{};
+
+  ModelDev(std::shared_ptr<const CompiledShip> s, const CompiledSim& m) : ship(std::move(s)), sim(m) {
+    if (!ship) throw std::invalid_argument("Batch: null ship");
+    check_pairing(*ship, sim);
+    inc = build_incidence(sim);
+    mons = build_monitor_lists(sim);
+    NN = ship->nodes(); NC = sim.connections(); NG = sim.groups();
+    nmon = sim.monitors(); nmark = sim.marks(); evCap = nmon + nmark + 1; maxGroup = sim.maxGroupSize();
+  }
+
+  void upload(cudaStream_t s) {
+    const CompiledShip& S = *ship;
+    const CompiledSim& M = sim;
+    {
+      const std::size_t nc = S.x.size(), ns = S.segCol.size();
+      std::vector<double2> cxy(nc), clh(nc), sxy(ns), slh(ns);
+      std::vector<float2> cxyf(nc), clhf(nc), sxyf(ns), slhf(ns);
+      std::vector<double> sa(ns);
+      std::vector<float> caf(nc), saf(ns);
+      for (std::size_t i = 0; i < nc; ++i) {
+        cxy[i] = double2{S.x[i], S.y[i]};
+        clh[i] = double2{S.zlo[i], S.zhi[i]};
+        cxyf[i] = float2{static_cast<float>(S.x[i]), static_cast<float>(S.y[i])};
+        clhf[i] = float2{static_cast<float>(S.zlo[i]), static_cast<float>(S.zhi[i])};
+        caf[i] = static_cast<float>(S.dxdy[i]);
+      }
+      for (std::size_t j = 0; j < ns; ++j) {
+        const auto c = static_cast<std::size_t>(S.segCol[j]);
+        sxy[j] = double2{S.x[c], S.y[c]};
+        slh[j] = double2{S.segA[j], S.segE[j]};
+        sa[j] = S.dxdy[c];
+        sxyf[j] = float2{static_cast<float>(S.x[c]), static_cast<float>(S.y[c])};
+        slhf[j] = float2{static_cast<float>(S.segA[j]), static_cast<float>(S.segE[j])};
+        saf[j] = static_cast<float>(S.dxdy[c]);
+      }
+      colXY.upload(cxy, s); colLH.upload(clh, s); colA.upload(S.dxdy, s);
+      colXYf.upload(cxyf, s); colLHf.upload(clhf, s); colAf.upload(caf, s);
+      segXY.upload(sxy, s); segLH.upload(slh, s); segAr.upload(sa, s);
+      segXYf.upload(sxyf, s); segLHf.upload(slhf, s); segArf.upload(saf, s);
+      check(cudaStreamSynchronize(s), "stream sync");
+    }
+    mu.upload(S.mu, s); vmax.upload(S.vmax, s); amin.upload(S.amin, s); aov.upload(S.aov, s);
+    segStart.upload(S.segStart, s); segCount.upload(S.segCount, s);
+    gStart.upload(M.gNodeStart, s); gCount.upload(M.gNodeCount, s); gNodes.upload(M.gNodes, s); gMode.upload(M.gMode, s);
+    gpx.upload(M.gpx, s); gpy.upload(M.gpy, s); gpz.upload(M.gpz, s);
+    ca.upload(M.ca, s); cb.upload(M.cb, s); skip.upload(M.cSkipGroup, s); law.upload(M.cLaw, s);
+    kx.upload(M.cx, s); ky.upload(M.cy, s); kz.upload(M.cz, s); coef.upload(M.cCoef, s);
+    incStart.upload(inc.start, s); incCount.upload(inc.count, s); incConn.upload(inc.conn, s); incSide.upload(inc.side, s);
+    sea.upload(inc.sea.empty() ? std::vector<std::int32_t>{0} : inc.sea, s);
+    monStart.upload(mons.start.empty() ? std::vector<std::int32_t>{0} : mons.start, s);
+    monCount.upload(mons.count.empty() ? std::vector<std::int32_t>{0} : mons.count, s);
+    monConn.upload(mons.conn.empty() ? std::vector<std::int32_t>{0} : mons.conn, s);
+    mkx.upload(M.mkx.empty() ? std::vector<double>{0} : M.mkx, s);
+    mky.upload(M.mky.empty() ? std::vector<double>{0} : M.mky, s);
+    mkz.upload(M.mkz.empty() ? std::vector<double>{0} : M.mkz, s);
+    mkWhen.upload(M.mkWhen.empty() ? std::vector<std::uint8_t>{0} : M.mkWhen, s);
+    check(cudaStreamSynchronize(s), "model upload");
+
+    DevModel& d = dm;
+    d.ncol = S.columns();
+    d.colXY = colXY.get(); d.colLH = colLH.get(); d.colA = colA.get();
+    d.colXYf = colXYf.get(); d.colLHf = colLHf.get(); d.colAf = colAf.get();
+    d.nseg = S.segments();
+    d.segXY = segXY.get(); d.segLH = segLH.get(); d.segAr = segAr.get();
+    d.segXYf = segXYf.get(); d.segLHf = segLHf.get(); d.segArf = segArf.get();
+    d.nn = NN;
+    d.mu = mu.get(); d.vmax = vmax.get(); d.amin = amin.get(); d.aov = aov.get();
+    d.segStart = segStart.get(); d.segCount = segCount.get();
+    d.ng = NG;
+    d.gStart = gStart.get(); d.gCount = gCount.get(); d.gNodes = gNodes.get(); d.gMode = gMode.get();
+    d.gpx = gpx.get(); d.gpy = gpy.get(); d.gpz = gpz.get(); d.gMargin = M.gMargin; d.maxGroup = maxGroup;
+    d.nc = NC;
+    d.ca = ca.get(); d.cb = cb.get(); d.skip = skip.get(); d.law = law.get();
+    d.kx = kx.get(); d.ky = ky.get(); d.kz = kz.get(); d.coef = coef.get();
+    d.incStart = incStart.get(); d.incCount = incCount.get(); d.incConn = incConn.get(); d.incSide = incSide.get();
+    d.nsea = static_cast<std::int32_t>(inc.sea.size()); d.sea = sea.get();
+    d.nmon = nmon; d.monThreshold = M.monitorThreshold;
+    d.monStart = monStart.get(); d.monCount = monCount.get(); d.monConn = monConn.get();
+    d.nmark = nmark; d.mkx = mkx.get(); d.mky = mky.get(); d.mkz = mkz.get(); d.mkWhen = mkWhen.get();
+    d.hullTopBelow = M.hullTopBelow; d.pitchAbsAbove = M.pitchAbsAbove; d.buoyancyBelow = M.buoyancyBelow; d.minT = M.minT;
+    d.rho = M.rho; d.g = M.g; d.sq2g = std::sqrt(2 * M.g); d.dt = M.dt;
+    d.ms = M.body[0]; d.g0x = M.body[2]; d.g0y = M.body[3]; d.g0z = M.body[4]; d.XO = M.body[5]; d.YO = M.body[6];
+    d.mh0 = M.body[7]; d.Ith0 = M.body[8]; d.Iph0 = M.body[9]; d.cDz = M.body[10]; d.cDth = M.body[11]; d.cDph = M.body[12];
+    d.qz = M.body[13]; d.qth = M.body[14]; d.qph = M.body[15];
+    d.xFP = M.xFP; d.xAP = M.xAP;
+    d.evCap = evCap;
+  }
+};
 
 }  // namespace
 
@@ -97,15 +196,26 @@ DeviceInfo device_info(int device) {
 }
 
 struct Batch::Impl {
-  std::shared_ptr<const CompiledShip> ship;
-  CompiledSim sim;
-  Incidence inc;
-  MonitorLists mons;
+  // The models of the batch (one, or several for a fleet), the model of every instance and where each instance's
+  // per-node, per-connection, event, monitor and mark values start in the per-instance arrays (count + 1 prefix sums).
+  std::vector<std::unique_ptr<ModelDev>> models;
+  std::vector<std::int32_t> instModel;
+  std::vector<long long> nodeOff, connOff, evOff, monOff, markOff;
+  DevBuf<DevModel> dModels;
+  DevBuf<std::int32_t> dInstModel;
+  DevBuf<long long> dNodeOff, dConnOff, dEvOff, dMonOff, dMarkOff;
   DeviceInfo info;
-  std::int32_t NN = 0, NC = 0, NG = 0, nmon = 0, nmark = 0, evCap = 0, maxGroup = 0, recSize = 0, maxSamples = 0, curveMax = 0;
+  // the largest sizes over the models (the slot is laid out for them) and the trace/curve record counts
+  std::int32_t NN = 0, NC = 0, NG = 0, maxGroup = 0, recSize = 0, maxSamples = 0, curveMax = 0;
+
+  bool fleet() const { return models.size() > 1; }
+  const ModelDev& m0() const { return *models.front(); }
+  const ModelDev& model(std::size_t inst) const { return *models[static_cast<std::size_t>(instModel[inst])]; }
+
   // The shared-memory slot of one simulation stepped by a team of W warps: per-node state and scratch, per-connection
-  // dV and q, one group-pass buffer per warp, the buoyancy tree results. The loads' sixth scratch column reuses dV
-  // when there are at least as many connections as nodes.
+  // dV and q, the group-pass buffers, the buoyancy tree results, the pose, buoyancy result and parked run values, and
+  // in a fleet the team's copy of its instance's model. The loads' sixth scratch column reuses dV when there are at
+  // least as many connections as nodes.
   SlotLayout layout_for(int W) const {
     SlotLayout L{};
     std::uint32_t off = 0;
@@ -123,6 +233,7 @@ struct Batch::Impl {
     L.pose = take(off, sizeof(Pose));
     L.buoy = take(off, sizeof(Buoy));
     L.parked = take(off, sizeof(Parked));
+    L.model = fleet() ? take(off, sizeof(DevModel)) : 0u;
     L.bytes = off;
     return L;
   }
@@ -133,15 +244,6 @@ struct Batch::Impl {
   std::vector<float> lastPhaseMs;
   std::vector<unsigned long long> lastPhaseSteps;
 
-  // model
-  DevBuf<double2> colXY, colLH, segXY, segLH;
-  DevBuf<float2> colXYf, colLHf, segXYf, segLHf;
-  DevBuf<float> colAf, segArf;
-  DevBuf<double> colA, segAr, mu, vmax, amin, aov;
-  DevBuf<std::int32_t> segStart, segCount, gStart, gCount, gNodes, ca, cb, skip, incStart, incCount, incConn, sea, monStart, monCount, monConn;
-  DevBuf<std::uint8_t> gMode, law, incSide, mkWhen;
-  DevBuf<double> gpx, gpy, gpz, kx, ky, kz, coef, mkx, mky, mkz;
-  DevModel dm{};
 
   // per instance (device)
   DevBuf<std::uint8_t> en;
@@ -186,15 +288,34 @@ struct Batch::Impl {
     b.error = error.get();
     b.remaining = remaining.get();
     b.yieldBelow = 0;
+    if (fleet()) {
+      b.models = dModels.get(); b.model = dInstModel.get();
+      b.nodeOff = dNodeOff.get(); b.connOff = dConnOff.get(); b.evOff = dEvOff.get(); b.monOff = dMonOff.get(); b.markOff = dMarkOff.get();
+    }
     return b;
   }
 };
 
 Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, const BatchOptions& opt) : I_(new Impl), opt_(opt) {
+  std::vector<std::pair<std::shared_ptr<const CompiledShip>, CompiledSim>> models;
+  models.emplace_back(std::move(ship), sim);
+  init(std::move(models), std::vector<std::int32_t>(static_cast<std::size_t>(std::max(opt.count, 0)), 0));
+}
+
+Batch::Batch(std::vector<std::pair<std::shared_ptr<const CompiledShip>, CompiledSim>> models, std::vector<std::int32_t> instanceModel,
+             const BatchOptions& opt)
+    : I_(new Impl), opt_(opt) {
+  opt_.count = static_cast<std::int32_t>(instanceModel.size());
+  init(std::move(models), std::move(instanceModel));
+}
+
+void Batch::init(std::vector<std::pair<std::shared_ptr<const CompiledShip>, CompiledSim>> models, std::vector<std::int32_t> instanceModel) {
   Impl& I = *I_;
-  if (!ship) throw std::invalid_argument("Batch: null ship");
+  if (models.empty()) throw std::invalid_argument("Batch: no model");
   if (opt_.count < 1) throw std::invalid_argument("Batch: count must be at least 1");
   if (!(opt_.tMax > 0)) throw std::invalid_argument("Batch: tMax must be positive");
+  if (models.size() > 1 && opt_.tracedInstances > 0) throw std::invalid_argument("Batch: a fleet of several models records no traces");
+  if (models.size() > 1 && opt_.stepsPerLaunch > 0) throw std::invalid_argument("Batch: a fleet of several models runs in one launch per phase");
   if (opt_.tracedInstances > opt_.count) opt_.tracedInstances = opt_.count;
   if (opt_.tracedInstances < 0) opt_.tracedInstances = 0;
   if (opt_.tracedInstances > 0 && !(opt_.sampleEvery > 0)) throw std::invalid_argument("Batch: sampleEvery must be positive");
@@ -202,21 +323,31 @@ Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, c
   std::string why;
   if (!cuda_available(&why)) throw std::runtime_error("Batch: " + why);
   check(cudaSetDevice(opt_.device), "cudaSetDevice");
-  I.ship = std::move(ship);
-  I.sim = sim;
-  check_pairing(*I.ship, I.sim);
-  I.inc = build_incidence(I.sim);
-  I.mons = build_monitor_lists(I.sim);
+  for (auto& m : models) I.models.push_back(std::make_unique<ModelDev>(std::move(m.first), m.second));
+  I.instModel = std::move(instanceModel);
+  const auto count = static_cast<std::size_t>(opt_.count);
+  I.nodeOff.assign(count + 1, 0); I.connOff.assign(count + 1, 0); I.evOff.assign(count + 1, 0);
+  I.monOff.assign(count + 1, 0); I.markOff.assign(count + 1, 0);
+  for (std::size_t i = 0; i < count; ++i) {
+    const std::int32_t m = I.instModel[i];
+    if (m < 0 || static_cast<std::size_t>(m) >= I.models.size())
+      throw std::out_of_range("Batch: instance " + std::to_string(i) + " refers to model " + std::to_string(m) + " of " + std::to_string(I.models.size()));
+    const ModelDev& d = *I.models[static_cast<std::size_t>(m)];
+    I.nodeOff[i + 1] = I.nodeOff[i] + d.NN; I.connOff[i + 1] = I.connOff[i] + d.NC; I.evOff[i + 1] = I.evOff[i] + d.evCap;
+    I.monOff[i + 1] = I.monOff[i] + d.nmon; I.markOff[i + 1] = I.markOff[i] + d.nmark;
+  }
+  for (const auto& d : I.models) {
+    I.NN = std::max(I.NN, d->NN); I.NC = std::max(I.NC, d->NC); I.NG = std::max(I.NG, d->NG); I.maxGroup = std::max(I.maxGroup, d->maxGroup);
+  }
   I.info = device_info(opt_.device);
-  I.NN = I.ship->nodes(); I.NC = I.sim.connections(); I.NG = I.sim.groups();
-  I.nmon = I.sim.monitors(); I.nmark = I.sim.marks(); I.evCap = I.nmon + I.nmark + 1; I.maxGroup = I.sim.maxGroupSize();
-  I.recSize = 10 + 5 * I.NN;
+  I.recSize = 10 + 5 * I.m0().NN;
   I.maxSamples = opt_.tracedInstances > 0 ? static_cast<std::int32_t>(std::floor(opt_.tMax / opt_.sampleEvery)) + 2 : 0;
   I.curveMax = opt_.curveEvery > 0 ? static_cast<std::int32_t>(std::floor(opt_.tMax / opt_.curveEvery)) + 2 : 0;
 
   // launch shape. Teams of W warps; a slot of shared memory per team; persistent grids sized to the device.
   // Main phase: single-warp teams when the batch fills the device (the most simulations per SM), larger teams when it
   // does not. Later phases: when the unfinished instances fit the resident teams of twice the size, they resume there.
+  const bool fleet = I.fleet();
   const std::size_t optin = I.info.sharedPerBlockOptIn;
   const int sms = I.info.multiprocessors;
   cfg_.slotBytes = I.layout_for(1).bytes;
@@ -235,8 +366,8 @@ Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, c
     tpb = std::max(1, std::min(tpb, maxTeams));
     p.teamsPerBlock = tpb;
     const std::size_t smem = static_cast<std::size_t>(tpb) * L.bytes;
-    check(configure_batch_kernel(opt_.mixedPrecision, W, smem), "cudaFuncSetAttribute");
-    check(batch_kernel_occupancy(opt_.mixedPrecision, W, tpb, smem, &p.blocksPerSM), "occupancy");
+    check(configure_batch_kernel(opt_.mixedPrecision, W, smem, fleet), "cudaFuncSetAttribute");
+    check(batch_kernel_occupancy(opt_.mixedPrecision, W, tpb, smem, &p.blocksPerSM, fleet), "occupancy");
     if (p.blocksPerSM < 1) throw std::runtime_error("Batch: the kernel cannot be resident with " + std::to_string(tpb) + " simulations per block");
     p.blocks = std::min((count + tpb - 1) / tpb, p.blocksPerSM * sms);
     return p;
@@ -270,94 +401,36 @@ Batch::Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, c
   check(cudaEventCreate(&I.ev1), "cudaEventCreate");
   I.phaseEv.assign(cfg_.phases.size() + 1, nullptr);
   for (cudaEvent_t& e : I.phaseEv) check(cudaEventCreate(&e), "cudaEventCreate");
-  const CompiledShip& S = *I.ship;
-  const CompiledSim& M = I.sim;
   cudaStream_t s = I.stream;
-  {
-    // geometry in the kernel's layout: paired fields, the segment -> column gather resolved, float copies
-    const std::size_t nc = S.x.size(), ns = S.segCol.size();
-    std::vector<double2> cxy(nc), clh(nc), sxy(ns), slh(ns);
-    std::vector<float2> cxyf(nc), clhf(nc), sxyf(ns), slhf(ns);
-    std::vector<double> sa(ns);
-    std::vector<float> caf(nc), saf(ns);
-    for (std::size_t i = 0; i < nc; ++i) {
-      cxy[i] = double2{S.x[i], S.y[i]};
-      clh[i] = double2{S.zlo[i], S.zhi[i]};
-      cxyf[i] = float2{static_cast<float>(S.x[i]), static_cast<float>(S.y[i])};
-      clhf[i] = float2{static_cast<float>(S.zlo[i]), static_cast<float>(S.zhi[i])};
-      caf[i] = static_cast<float>(S.dxdy[i]);
-    }
-    for (std::size_t j = 0; j < ns; ++j) {
-      const auto c = static_cast<std::size_t>(S.segCol[j]);
-      sxy[j] = double2{S.x[c], S.y[c]};
-      slh[j] = double2{S.segA[j], S.segE[j]};
-      sa[j] = S.dxdy[c];
-      sxyf[j] = float2{static_cast<float>(S.x[c]), static_cast<float>(S.y[c])};
-      slhf[j] = float2{static_cast<float>(S.segA[j]), static_cast<float>(S.segE[j])};
-      saf[j] = static_cast<float>(S.dxdy[c]);
-    }
-    I.colXY.upload(cxy, s); I.colLH.upload(clh, s); I.colA.upload(S.dxdy, s);
-    I.colXYf.upload(cxyf, s); I.colLHf.upload(clhf, s); I.colAf.upload(caf, s);
-    I.segXY.upload(sxy, s); I.segLH.upload(slh, s); I.segAr.upload(sa, s);
-    I.segXYf.upload(sxyf, s); I.segLHf.upload(slhf, s); I.segArf.upload(saf, s);
-    check(cudaStreamSynchronize(s), "stream sync");
+  for (auto& d : I.models) d->upload(s);
+  if (fleet) {
+    std::vector<DevModel> dms;
+    for (const auto& d : I.models) dms.push_back(d->dm);
+    I.dModels.upload(dms, s);
+    I.dInstModel.upload(I.instModel, s);
+    I.dNodeOff.upload(I.nodeOff, s); I.dConnOff.upload(I.connOff, s); I.dEvOff.upload(I.evOff, s);
+    I.dMonOff.upload(I.monOff, s); I.dMarkOff.upload(I.markOff, s);
+    check(cudaStreamSynchronize(s), "fleet tables upload");
   }
-  I.mu.upload(S.mu, s); I.vmax.upload(S.vmax, s); I.amin.upload(S.amin, s); I.aov.upload(S.aov, s);
-  I.segStart.upload(S.segStart, s); I.segCount.upload(S.segCount, s);
-  I.gStart.upload(M.gNodeStart, s); I.gCount.upload(M.gNodeCount, s); I.gNodes.upload(M.gNodes, s); I.gMode.upload(M.gMode, s);
-  I.gpx.upload(M.gpx, s); I.gpy.upload(M.gpy, s); I.gpz.upload(M.gpz, s);
-  I.ca.upload(M.ca, s); I.cb.upload(M.cb, s); I.skip.upload(M.cSkipGroup, s); I.law.upload(M.cLaw, s);
-  I.kx.upload(M.cx, s); I.ky.upload(M.cy, s); I.kz.upload(M.cz, s); I.coef.upload(M.cCoef, s);
-  I.incStart.upload(I.inc.start, s); I.incCount.upload(I.inc.count, s); I.incConn.upload(I.inc.conn, s); I.incSide.upload(I.inc.side, s);
-  I.sea.upload(I.inc.sea.empty() ? std::vector<std::int32_t>{0} : I.inc.sea, s);
-  I.monStart.upload(I.mons.start.empty() ? std::vector<std::int32_t>{0} : I.mons.start, s);
-  I.monCount.upload(I.mons.count.empty() ? std::vector<std::int32_t>{0} : I.mons.count, s);
-  I.monConn.upload(I.mons.conn.empty() ? std::vector<std::int32_t>{0} : I.mons.conn, s);
-  I.mkx.upload(M.mkx.empty() ? std::vector<double>{0} : M.mkx, s);
-  I.mky.upload(M.mky.empty() ? std::vector<double>{0} : M.mky, s);
-  I.mkz.upload(M.mkz.empty() ? std::vector<double>{0} : M.mkz, s);
-  I.mkWhen.upload(M.mkWhen.empty() ? std::vector<std::uint8_t>{0} : M.mkWhen, s);
-  check(cudaStreamSynchronize(s), "model upload");
 
-  DevModel& d = I.dm;
-  d.ncol = S.columns();
-  d.colXY = I.colXY.get(); d.colLH = I.colLH.get(); d.colA = I.colA.get();
-  d.colXYf = I.colXYf.get(); d.colLHf = I.colLHf.get(); d.colAf = I.colAf.get();
-  d.nseg = S.segments();
-  d.segXY = I.segXY.get(); d.segLH = I.segLH.get(); d.segAr = I.segAr.get();
-  d.segXYf = I.segXYf.get(); d.segLHf = I.segLHf.get(); d.segArf = I.segArf.get();
-  d.nn = I.NN;
-  d.mu = I.mu.get(); d.vmax = I.vmax.get(); d.amin = I.amin.get(); d.aov = I.aov.get();
-  d.segStart = I.segStart.get(); d.segCount = I.segCount.get();
-  d.ng = I.NG;
-  d.gStart = I.gStart.get(); d.gCount = I.gCount.get(); d.gNodes = I.gNodes.get(); d.gMode = I.gMode.get();
-  d.gpx = I.gpx.get(); d.gpy = I.gpy.get(); d.gpz = I.gpz.get(); d.gMargin = M.gMargin; d.maxGroup = I.maxGroup;
-  d.nc = I.NC;
-  d.ca = I.ca.get(); d.cb = I.cb.get(); d.skip = I.skip.get(); d.law = I.law.get();
-  d.kx = I.kx.get(); d.ky = I.ky.get(); d.kz = I.kz.get(); d.coef = I.coef.get();
-  d.incStart = I.incStart.get(); d.incCount = I.incCount.get(); d.incConn = I.incConn.get(); d.incSide = I.incSide.get();
-  d.nsea = static_cast<std::int32_t>(I.inc.sea.size()); d.sea = I.sea.get();
-  d.nmon = I.nmon; d.monThreshold = M.monitorThreshold;
-  d.monStart = I.monStart.get(); d.monCount = I.monCount.get(); d.monConn = I.monConn.get();
-  d.nmark = I.nmark; d.mkx = I.mkx.get(); d.mky = I.mky.get(); d.mkz = I.mkz.get(); d.mkWhen = I.mkWhen.get();
-  d.hullTopBelow = M.hullTopBelow; d.pitchAbsAbove = M.pitchAbsAbove; d.buoyancyBelow = M.buoyancyBelow; d.minT = M.minT;
-  d.rho = M.rho; d.g = M.g; d.sq2g = std::sqrt(2 * M.g); d.dt = M.dt;
-  d.ms = M.body[0]; d.g0x = M.body[2]; d.g0y = M.body[3]; d.g0z = M.body[4]; d.XO = M.body[5]; d.YO = M.body[6];
-  d.mh0 = M.body[7]; d.Ith0 = M.body[8]; d.Iph0 = M.body[9]; d.cDz = M.body[10]; d.cDth = M.body[11]; d.cDph = M.body[12];
-  d.qz = M.body[13]; d.qth = M.body[14]; d.qph = M.body[15];
-  d.xFP = M.xFP; d.xAP = M.xAP;
-  d.evCap = I.evCap;
-
-  // per-instance staging: the compiled connection table and initial state in every instance
-  const auto count = static_cast<std::size_t>(opt_.count);
-  I.hEn = repeat(M.cEn, count); I.hArea = repeat(M.cArea, count); I.hTOn = repeat(M.cTOn, count);
+  // per-instance staging: the compiled connection table and initial state of every instance's model
+  I.hEn.resize(static_cast<std::size_t>(I.connOff[count])); I.hArea.resize(I.hEn.size()); I.hTOn.resize(I.hEn.size());
+  const auto nodesTotal = static_cast<std::size_t>(I.nodeOff[count]);
+  I.hVol.resize(nodesTotal); I.hLevel.resize(nodesTotal); I.hCx.resize(nodesTotal); I.hCy.resize(nodesTotal); I.hCz.resize(nodesTotal);
   I.hSt.resize(count * 8);
   for (std::size_t i = 0; i < count; ++i) {
+    const CompiledSim& M = I.model(i).sim;
     double* p = &I.hSt[i * 8];
     p[0] = M.t0; p[1] = M.zO0; p[2] = M.pitch0; p[3] = M.roll0; p[4] = M.vz0; p[5] = M.wth0; p[6] = M.wph0; p[7] = 0;
+    std::copy(M.cEn.begin(), M.cEn.end(), I.hEn.begin() + I.connOff[i]);
+    std::copy(M.cArea.begin(), M.cArea.end(), I.hArea.begin() + I.connOff[i]);
+    std::copy(M.cTOn.begin(), M.cTOn.end(), I.hTOn.begin() + I.connOff[i]);
+    std::copy(M.vol0.begin(), M.vol0.end(), I.hVol.begin() + I.nodeOff[i]);
+    std::copy(M.level0.begin(), M.level0.end(), I.hLevel.begin() + I.nodeOff[i]);
+    std::copy(M.cx0.begin(), M.cx0.end(), I.hCx.begin() + I.nodeOff[i]);
+    std::copy(M.cy0.begin(), M.cy0.end(), I.hCy.begin() + I.nodeOff[i]);
+    std::copy(M.cz0.begin(), M.cz0.end(), I.hCz.begin() + I.nodeOff[i]);
   }
-  I.hVol = repeat(M.vol0, count); I.hLevel = repeat(M.level0, count);
-  I.hCx = repeat(M.cx0, count); I.hCy = repeat(M.cy0, count); I.hCz = repeat(M.cz0, count);
 }
 
 Batch::~Batch() {
@@ -370,8 +443,15 @@ Batch::~Batch() {
   }
 }
 
-std::int32_t Batch::nodes() const { return I_->NN; }
-std::int32_t Batch::connections() const { return I_->NC; }
+std::int32_t Batch::nodes() const { return I_->m0().NN; }
+std::int32_t Batch::connections() const { return I_->m0().NC; }
+std::int32_t Batch::models() const { return static_cast<std::int32_t>(I_->models.size()); }
+
+Batch::InstanceShape Batch::instance_shape(std::int32_t inst) const {
+  if (inst < 0 || inst >= opt_.count) throw std::out_of_range("Batch: instance " + std::to_string(inst) + " out of range");
+  const ModelDev& d = I_->model(static_cast<std::size_t>(inst));
+  return InstanceShape{I_->instModel[static_cast<std::size_t>(inst)], d.NN, d.NC};
+}
 std::size_t Batch::slot_bytes() const { return cfg_.slotBytes; }
 
 static void check_inst(const BatchOptions& o, std::int32_t inst) {
@@ -383,48 +463,50 @@ void Batch::restore(std::int32_t inst, const double* rec) {
   if (I.uploaded) throw std::logic_error("Batch: restore after run");
   check_inst(opt_, inst);
   const auto i = static_cast<std::size_t>(inst);
-  const auto N = static_cast<std::size_t>(I.NN);
+  const auto N = static_cast<std::size_t>(I.model(i).NN);
+  const auto o = static_cast<std::size_t>(I.nodeOff[i]);
   for (int k = 0; k < 7; ++k) I.hSt[i * 8 + static_cast<std::size_t>(k)] = rec[k];
   I.hSt[i * 8 + 7] = 0;
   for (std::size_t n = 0; n < N; ++n) {
-    I.hVol[i * N + n] = rec[10 + n];
-    I.hLevel[i * N + n] = rec[10 + N + n];
-    I.hCx[i * N + n] = rec[10 + 2 * N + n];
-    I.hCy[i * N + n] = rec[10 + 3 * N + n];
-    I.hCz[i * N + n] = rec[10 + 4 * N + n];
+    I.hVol[o + n] = rec[10 + n];
+    I.hLevel[o + n] = rec[10 + N + n];
+    I.hCx[o + n] = rec[10 + 2 * N + n];
+    I.hCy[o + n] = rec[10 + 3 * N + n];
+    I.hCz[o + n] = rec[10 + 4 * N + n];
   }
 }
 
 void Batch::set_connection_enabled(std::int32_t inst, std::int32_t c, bool en) {
   if (I_->uploaded) throw std::logic_error("Batch: set after run");
   check_inst(opt_, inst);
-  if (c < 0 || c >= I_->NC) throw std::out_of_range("Batch: connection " + std::to_string(c));
-  I_->hEn[static_cast<std::size_t>(inst) * I_->NC + static_cast<std::size_t>(c)] = en ? 1 : 0;
+  if (c < 0 || c >= I_->model(static_cast<std::size_t>(inst)).NC) throw std::out_of_range("Batch: connection " + std::to_string(c));
+  I_->hEn[static_cast<std::size_t>(I_->connOff[static_cast<std::size_t>(inst)] + c)] = en ? 1 : 0;
 }
 
 void Batch::set_connection_area(std::int32_t inst, std::int32_t c, double area) {
   if (I_->uploaded) throw std::logic_error("Batch: set after run");
   check_inst(opt_, inst);
-  if (c < 0 || c >= I_->NC) throw std::out_of_range("Batch: connection " + std::to_string(c));
-  I_->hArea[static_cast<std::size_t>(inst) * I_->NC + static_cast<std::size_t>(c)] = area;
+  if (c < 0 || c >= I_->model(static_cast<std::size_t>(inst)).NC) throw std::out_of_range("Batch: connection " + std::to_string(c));
+  I_->hArea[static_cast<std::size_t>(I_->connOff[static_cast<std::size_t>(inst)] + c)] = area;
 }
 
 void Batch::set_connection_activation(std::int32_t inst, std::int32_t c, double tOn) {
   if (I_->uploaded) throw std::logic_error("Batch: set after run");
   check_inst(opt_, inst);
-  if (c < 0 || c >= I_->NC) throw std::out_of_range("Batch: connection " + std::to_string(c));
-  I_->hTOn[static_cast<std::size_t>(inst) * I_->NC + static_cast<std::size_t>(c)] = tOn;
+  if (c < 0 || c >= I_->model(static_cast<std::size_t>(inst)).NC) throw std::out_of_range("Batch: connection " + std::to_string(c));
+  I_->hTOn[static_cast<std::size_t>(I_->connOff[static_cast<std::size_t>(inst)] + c)] = tOn;
 }
 
 void Batch::apply_sweep(const Sweep& sw, std::int32_t first) {
   Impl& I = *I_;
   if (I.uploaded) throw std::logic_error("Batch: set after run");
+  if (I.fleet()) throw std::invalid_argument("Batch: a sweep applies to a batch of one model");
   if (first < 0 || static_cast<std::size_t>(first) + static_cast<std::size_t>(opt_.count) > sw.instances.size())
     throw std::invalid_argument("Batch: sweep instances " + std::to_string(first) + " .. " + std::to_string(first + opt_.count - 1) +
                                 " do not exist (the sweep has " + std::to_string(sw.instances.size()) + ")");
   for (std::int32_t i = 0; i < opt_.count; ++i) {
-    const std::size_t o = static_cast<std::size_t>(i) * I.NC;
-    apply_instance(sw.instances[static_cast<std::size_t>(first + i)], I.sim, I.hEn.data() + o, I.hArea.data() + o, I.hTOn.data() + o);
+    const auto o = static_cast<std::size_t>(I.connOff[static_cast<std::size_t>(i)]);
+    apply_instance(sw.instances[static_cast<std::size_t>(first + i)], I.m0().sim, I.hEn.data() + o, I.hArea.data() + o, I.hTOn.data() + o);
   }
   sweepFirst_ = first;
 }
@@ -441,11 +523,11 @@ void Batch::upload() {
   I.vol.upload(I.hVol, s); I.level.upload(I.hLevel, s); I.cx.upload(I.hCx, s); I.cy.upload(I.hCy, s); I.cz.upload(I.hCz, s);
   // outputs and bookkeeping start at zero / -1 on the device
   I.out.alloc(count * 7); check(cudaMemsetAsync(I.out.get(), 0, I.out.bytes(), s), "memset");
-  I.evT.alloc(count * static_cast<std::size_t>(I.evCap)); I.evId.alloc(count * static_cast<std::size_t>(I.evCap));
-  I.evKind.alloc(count * static_cast<std::size_t>(I.evCap));
+  const auto events = static_cast<std::size_t>(I.evOff[count]);
+  I.evT.alloc(events); I.evId.alloc(events); I.evKind.alloc(events);
   I.evCount.alloc(count); check(cudaMemsetAsync(I.evCount.get(), 0, I.evCount.bytes(), s), "memset");
-  I.overT.upload(std::vector<double>(std::max<std::size_t>(count * static_cast<std::size_t>(I.nmon), 1), -1), s);
-  I.markT.upload(std::vector<double>(std::max<std::size_t>(count * static_cast<std::size_t>(I.nmark), 1), -1), s);
+  I.overT.upload(std::vector<double>(std::max<std::size_t>(static_cast<std::size_t>(I.monOff[count]), 1), -1), s);
+  I.markT.upload(std::vector<double>(std::max<std::size_t>(static_cast<std::size_t>(I.markOff[count]), 1), -1), s);
   I.foundered.alloc(count); check(cudaMemsetAsync(I.foundered.get(), 0, I.foundered.bytes(), s), "memset");
   I.founderT.upload(std::vector<double>(count, -1), s);
   I.steps.alloc(count); check(cudaMemsetAsync(I.steps.get(), 0, I.steps.bytes(), s), "memset");
@@ -490,7 +572,7 @@ float Batch::launch() {
       DevBatch db = I.devBatch(opt_, maxSteps, first);
       db.yieldBelow = p.yieldBelow;
       db.phaseSteps = I.phaseSteps.get() + k;
-      check(launch_batch_kernel(opt_.mixedPrecision, p.teamWarps, I.dm, db, p.layout, p.blocks, p.teamsPerBlock, s), "kernel launch");
+      check(launch_batch_kernel(opt_.mixedPrecision, p.teamWarps, I.m0().dm, db, p.layout, p.blocks, p.teamsPerBlock, s), "kernel launch");
       check(cudaEventRecord(I.phaseEv[k + 1], s), "cudaEventRecord");
       first = 0;
     }
@@ -603,15 +685,16 @@ void Batch::state(std::int32_t inst, double* rec) const {
   if (!I.downloaded) throw std::logic_error("Batch: result before run");
   check_inst(opt_, inst);
   const auto i = static_cast<std::size_t>(inst);
-  const auto N = static_cast<std::size_t>(I.NN);
+  const auto N = static_cast<std::size_t>(I.model(i).NN);
+  const auto o = static_cast<std::size_t>(I.nodeOff[i]);
   for (int k = 0; k < 7; ++k) rec[k] = I.r.st[i * 8 + static_cast<std::size_t>(k)];
   rec[7] = I.r.out[i * 7]; rec[8] = I.r.out[i * 7 + 1]; rec[9] = I.r.out[i * 7 + 2];
   for (std::size_t n = 0; n < N; ++n) {
-    rec[10 + n] = I.r.vol[i * N + n];
-    rec[10 + N + n] = I.r.level[i * N + n];
-    rec[10 + 2 * N + n] = I.r.cx[i * N + n];
-    rec[10 + 3 * N + n] = I.r.cy[i * N + n];
-    rec[10 + 4 * N + n] = I.r.cz[i * N + n];
+    rec[10 + n] = I.r.vol[o + n];
+    rec[10 + N + n] = I.r.level[o + n];
+    rec[10 + 2 * N + n] = I.r.cx[o + n];
+    rec[10 + 3 * N + n] = I.r.cy[o + n];
+    rec[10 + 4 * N + n] = I.r.cz[o + n];
   }
 }
 
@@ -619,7 +702,7 @@ std::vector<int> Batch::event_kinds(std::int32_t inst) const {
   const Impl& I = *I_;
   const auto i = static_cast<std::size_t>(inst);
   std::vector<int> out;
-  for (std::int32_t k = 0; k < I.r.evCount[i]; ++k) out.push_back(I.r.evKind[i * static_cast<std::size_t>(I.evCap) + static_cast<std::size_t>(k)]);
+  for (std::int32_t k = 0; k < I.r.evCount[i]; ++k) out.push_back(I.r.evKind[static_cast<std::size_t>(I.evOff[i] + k)]);
   return out;
 }
 
@@ -627,16 +710,17 @@ std::vector<int> Batch::event_ids(std::int32_t inst) const {
   const Impl& I = *I_;
   const auto i = static_cast<std::size_t>(inst);
   std::vector<int> out;
-  for (std::int32_t k = 0; k < I.r.evCount[i]; ++k) out.push_back(I.r.evId[i * static_cast<std::size_t>(I.evCap) + static_cast<std::size_t>(k)]);
+  for (std::int32_t k = 0; k < I.r.evCount[i]; ++k) out.push_back(I.r.evId[static_cast<std::size_t>(I.evOff[i] + k)]);
   return out;
 }
 
-const CompiledSim& Batch::sim() const { return I_->sim; }
+const CompiledSim& Batch::sim() const { return I_->m0().sim; }
 
 void Batch::run_noalloc(const NoAllocRun& run, cudaStream_t stream) const {
   const Impl& I = *I_;
+  if (I.fleet()) throw std::invalid_argument("run_noalloc: a batch of one model only");
   if (run.count < 1) throw std::invalid_argument("run_noalloc: count must be at least 1");
-  const std::size_t need = noalloc_scratch_bytes(I.dm, run.count), cap = noalloc_scratch_capacity();
+  const std::size_t need = noalloc_scratch_bytes(I.m0().dm, run.count), cap = noalloc_scratch_capacity();
   if (need > cap)
     throw std::invalid_argument("run_noalloc: " + std::to_string(run.count) + " instances of this model need " + std::to_string(need) +
                                 " bytes of scratch; the fixed scratch array holds " + std::to_string(cap) + " (at most " +
@@ -661,7 +745,7 @@ void Batch::run_noalloc(const NoAllocRun& run, cudaStream_t stream) const {
   check(batch_kernel_occupancy(opt_.mixedPrecision, r.teamWarps, r.teamsPerBlock, smem, &perSM), "occupancy");
   if (perSM < 1) throw std::runtime_error("run_noalloc: the kernel cannot be resident");
   r.blocks = std::min((r.count + r.teamsPerBlock - 1) / r.teamsPerBlock, perSM * sms);
-  check(run_batch_noalloc(opt_.mixedPrecision, I.dm, L, r, stream), "kernel launch");
+  check(run_batch_noalloc(opt_.mixedPrecision, I.m0().dm, L, r, stream), "kernel launch");
 }
 
 std::vector<EventRecord> Batch::events(std::int32_t inst) const {
@@ -670,12 +754,13 @@ std::vector<EventRecord> Batch::events(std::int32_t inst) const {
   check_inst(opt_, inst);
   const auto i = static_cast<std::size_t>(inst);
   std::vector<EventRecord> out;
+  const CompiledSim& sim = I.model(i).sim;
   for (std::int32_t k = 0; k < I.r.evCount[i]; ++k) {
-    const std::size_t j = i * static_cast<std::size_t>(I.evCap) + static_cast<std::size_t>(k);
+    const auto j = static_cast<std::size_t>(I.evOff[i] + k);
     const std::int32_t id = I.r.evId[j];
     switch (I.r.evKind[j]) {
-      case 0: out.push_back(EventRecord{I.r.evT[j], I.sim.monitorId[static_cast<std::size_t>(id)], I.sim.monitorLabel[static_cast<std::size_t>(id)]}); break;
-      case 1: out.push_back(EventRecord{I.r.evT[j], I.sim.markId[static_cast<std::size_t>(id)], I.sim.markLabel[static_cast<std::size_t>(id)]}); break;
+      case 0: out.push_back(EventRecord{I.r.evT[j], sim.monitorId[static_cast<std::size_t>(id)], sim.monitorLabel[static_cast<std::size_t>(id)]}); break;
+      case 1: out.push_back(EventRecord{I.r.evT[j], sim.markId[static_cast<std::size_t>(id)], sim.markLabel[static_cast<std::size_t>(id)]}); break;
       default: out.push_back(EventRecord{I.r.evT[j], "founder", "Foundered"}); break;
     }
   }
@@ -713,25 +798,26 @@ Trace Batch::trace(std::int32_t inst) const {
   if (inst < 0 || inst >= opt_.tracedInstances) throw std::out_of_range("Batch: instance was not traced");
   const auto i = static_cast<std::size_t>(inst);
   Trace tr;
-  tr.ship = I.ship->id; tr.sim = I.sim.id; tr.title = I.sim.title;
+  tr.ship = I.m0().ship->id; tr.sim = I.m0().sim.id; tr.title = I.m0().sim.title;
   tr.producer = opt_.mixedPrecision ? "sinksim-b200 CUDA engine, numerics portable32" : "sinksim-b200 CUDA engine, numerics portable";
   tr.engine = "sinksim-b200 0.1.0 on " + I.info.name;
-  tr.dt = I.sim.dt; tr.nodes = I.NN; tr.denseSteps = opt_.denseSteps; tr.sampleEvery = opt_.sampleEvery;
+  tr.dt = I.m0().sim.dt; tr.nodes = I.m0().NN; tr.denseSteps = opt_.denseSteps; tr.sampleEvery = opt_.sampleEvery;
   const Summary s = summary(inst);
   tr.steps = s.steps; tr.tEnd = s.tEnd; tr.foundered = s.foundered; tr.founderT = s.founderT;
   for (const EventRecord& e : events(inst)) tr.events.push_back(TraceEvent{e.t, e.id, e.label});
   const auto rec = static_cast<std::size_t>(I.recSize);
   const std::size_t db = i * static_cast<std::size_t>(opt_.denseSteps + 1) * rec, sb = i * static_cast<std::size_t>(I.maxSamples) * rec;
-  for (std::int32_t k = 0; k < I.r.denseCount[i]; ++k) tr.dense.push_record(&I.r.denseRec[db + static_cast<std::size_t>(k) * rec], I.NN);
-  for (std::int32_t k = 0; k < I.r.sampleCount[i]; ++k) tr.samples.push_record(&I.r.sampleRec[sb + static_cast<std::size_t>(k) * rec], I.NN);
+  for (std::int32_t k = 0; k < I.r.denseCount[i]; ++k) tr.dense.push_record(&I.r.denseRec[db + static_cast<std::size_t>(k) * rec], I.m0().NN);
+  for (std::int32_t k = 0; k < I.r.sampleCount[i]; ++k) tr.samples.push_record(&I.r.sampleRec[sb + static_cast<std::size_t>(k) * rec], I.m0().NN);
   return tr;
 }
 
 Results Batch::results(const Sweep* sw) const {
   const Impl& I = *I_;
+  if (I.fleet()) throw std::logic_error("Batch: batch-results hold one model; read a fleet's instances one by one");
   Results r;
-  r.ship = I.ship->id;
-  r.sim = I.sim.id;
+  r.ship = I.m0().ship->id;
+  r.sim = I.m0().sim.id;
   r.numerics = opt_.mixedPrecision ? "portable32" : "portable";
   r.engine = engine_name();
   r.tMax = opt_.tMax;

@@ -67,6 +67,11 @@ struct LaunchConfig {
 class Batch {
  public:
   Batch(std::shared_ptr<const CompiledShip> ship, const CompiledSim& sim, const BatchOptions& opt);
+  // A fleet: instance i steps models[instanceModel[i]] (opt.count is the number of instances). Every instance of every
+  // model runs in the same launches; per-instance setters and results work as for one model, except sweeps, traces,
+  // batch-results files and the no-allocation run, which hold one model.
+  Batch(std::vector<std::pair<std::shared_ptr<const CompiledShip>, CompiledSim>> models, std::vector<std::int32_t> instanceModel,
+        const BatchOptions& opt);
   ~Batch();
   Batch(const Batch&) = delete;
   Batch& operator=(const Batch&) = delete;
@@ -104,8 +109,13 @@ class Batch {
   };
   std::vector<PhaseStats> phase_stats() const;
   std::size_t slot_bytes() const;
-  std::int32_t nodes() const;
-  std::int32_t connections() const;
+  std::int32_t nodes() const;        // of the first model
+  std::int32_t connections() const;  // of the first model
+  std::int32_t models() const;
+  struct InstanceShape {
+    std::int32_t model, nodes, connections;
+  };
+  InstanceShape instance_shape(std::int32_t inst) const;
   // h2d and d2h bytes of one run() (the per-instance inputs and the results that download() reads back)
   std::size_t upload_bytes() const;
   std::size_t download_bytes() const;
@@ -135,6 +145,7 @@ class Batch {
   std::string engine_name() const;
 
  private:
+  void init(std::vector<std::pair<std::shared_ptr<const CompiledShip>, CompiledSim>> models, std::vector<std::int32_t> instanceModel);
   struct Impl;
   std::unique_ptr<Impl> I_;
   BatchOptions opt_;

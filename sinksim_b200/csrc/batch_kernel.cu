@@ -44,12 +44,13 @@ __device__ __forceinline__ void write_record(double* rec, const SimRegs& R, cons
 }
 
 // Runs one instance; returns true when the team paused it (yield) and must stop claiming.
-template <bool MIXED, int W>
+template <bool MIXED, int W, bool FLEET>
 __device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int inst, const Team<W>& T) {
   constexpr int kStride = 32 * W;
   if (B.stop[inst] != kRunning) return false;
   const int rank = T.rank;
-  const std::size_t iN = static_cast<std::size_t>(inst) * M.nn;
+  const InstPtrs<FLEET> I{M, B, inst};
+  const std::size_t iN = I.perNode();
   SimRegs R;
   {
     const double* st = B.st + static_cast<std::size_t>(inst) * 8;
@@ -60,7 +61,6 @@ __device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
     R.founderT = B.founderT[inst];
     R.evCount = B.evCount[inst];
   }
-  const InstPtrs I{M, B, inst};
   for (int n = rank; n < M.nn; n += kStride) {
     S.vol[n] = B.vol[iN + n]; S.level[n] = B.level[iN + n];
     S.cx[n] = B.cx[iN + n]; S.cy[n] = B.cy[iN + n]; S.cz[n] = B.cz[iN + n];
@@ -179,7 +179,9 @@ __device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
   return paused;
 }
 
-template <bool MIXED, int W>
+// The persistent batch kernel: teams claim instances from the work queue until it runs dry (or the phase yields). In a
+// fleet (FLEET), a team first copies its instance's model description into its slot and steps the instance with it.
+template <bool MIXED, int W, bool FLEET>
 __global__ void __launch_bounds__(kMaxWarpsPerBlock * 32, kMinBlocksPerSM) run_batch(DevModel M, DevBatch B, SlotLayout L) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int warpInBlock = threadIdx.x >> 5;
@@ -189,47 +191,59 @@ __global__ void __launch_bounds__(kMaxWarpsPerBlock * 32, kMinBlocksPerSM) run_b
   T.lane = threadIdx.x & 31;
   T.rank = T.warp * 32 + T.lane;
   T.bar = team + 1;
-  Slot S = carve_slot(smem + static_cast<std::size_t>(team) * L.bytes, L);
+  unsigned char* const slot = smem + static_cast<std::size_t>(team) * L.bytes;
+  Slot S = carve_slot(slot, L);
   for (;;) {
     if (T.leader()) S.misc[0] = atomicAdd(B.queue, 1);
     T.sync();
     const int inst = S.misc[0];
     T.sync();
     if (inst >= B.count) return;
-    if (run_instance<MIXED, W>(M, B, S, inst, T)) return;
+    if constexpr (FLEET) {
+      static_assert(sizeof(DevModel) % sizeof(unsigned) == 0, "the model description is copied in 32-bit words");
+      DevModel* const own = reinterpret_cast<DevModel*>(slot + L.model);
+      const unsigned* src = reinterpret_cast<const unsigned*>(B.models + B.model[inst]);
+      unsigned* dst = reinterpret_cast<unsigned*>(own);
+      for (int k = T.rank; k < static_cast<int>(sizeof(DevModel) / sizeof(unsigned)); k += 32 * W) dst[k] = src[k];
+      T.sync();
+      // run_instance ends with a team barrier, so no thread still reads this copy when the next claim overwrites it
+      if (run_instance<MIXED, W, true>(*own, B, S, inst, T)) return;
+    } else {
+      if (run_instance<MIXED, W, false>(M, B, S, inst, T)) return;
+    }
   }
 }
 
-template <bool MIXED>
+template <bool MIXED, bool FLEET>
 cudaError_t set_smem(int W, std::size_t bytes) {
   const int b = static_cast<int>(bytes);
   switch (W) {
-    case 1: return cudaFuncSetAttribute(run_batch<MIXED, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    case 2: return cudaFuncSetAttribute(run_batch<MIXED, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    case 4: return cudaFuncSetAttribute(run_batch<MIXED, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    case 8: return cudaFuncSetAttribute(run_batch<MIXED, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    case 1: return cudaFuncSetAttribute(run_batch<MIXED, 1, FLEET>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    case 2: return cudaFuncSetAttribute(run_batch<MIXED, 2, FLEET>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    case 4: return cudaFuncSetAttribute(run_batch<MIXED, 4, FLEET>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    case 8: return cudaFuncSetAttribute(run_batch<MIXED, 8, FLEET>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   }
   return cudaErrorInvalidValue;
 }
 
-template <bool MIXED>
+template <bool MIXED, bool FLEET>
 cudaError_t occupancy(int W, int threads, std::size_t bytes, int* perSM) {
   switch (W) {
-    case 1: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 1>, threads, bytes);
-    case 2: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 2>, threads, bytes);
-    case 4: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 4>, threads, bytes);
-    case 8: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 8>, threads, bytes);
+    case 1: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 1, FLEET>, threads, bytes);
+    case 2: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 2, FLEET>, threads, bytes);
+    case 4: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 4, FLEET>, threads, bytes);
+    case 8: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 8, FLEET>, threads, bytes);
   }
   return cudaErrorInvalidValue;
 }
 
-template <bool MIXED>
+template <bool MIXED, bool FLEET>
 void launch(int W, const DevModel& M, const DevBatch& B, const SlotLayout& L, int grid, int threads, std::size_t smem, cudaStream_t s) {
   switch (W) {
-    case 1: run_batch<MIXED, 1><<<grid, threads, smem, s>>>(M, B, L); break;
-    case 2: run_batch<MIXED, 2><<<grid, threads, smem, s>>>(M, B, L); break;
-    case 4: run_batch<MIXED, 4><<<grid, threads, smem, s>>>(M, B, L); break;
-    case 8: run_batch<MIXED, 8><<<grid, threads, smem, s>>>(M, B, L); break;
+    case 1: run_batch<MIXED, 1, FLEET><<<grid, threads, smem, s>>>(M, B, L); break;
+    case 2: run_batch<MIXED, 2, FLEET><<<grid, threads, smem, s>>>(M, B, L); break;
+    case 4: run_batch<MIXED, 4, FLEET><<<grid, threads, smem, s>>>(M, B, L); break;
+    case 8: run_batch<MIXED, 8, FLEET><<<grid, threads, smem, s>>>(M, B, L); break;
   }
 }
 
@@ -237,9 +251,10 @@ void launch(int W, const DevModel& M, const DevBatch& B, const SlotLayout& L, in
 
 bool valid_team_size(int W) { return W == 1 || W == 2 || W == 4 || W == 8; }
 
-cudaError_t configure_batch_kernel(bool mixed, int teamWarps, std::size_t smemBytes) {
+cudaError_t configure_batch_kernel(bool mixed, int teamWarps, std::size_t smemBytes, bool fleet) {
   if (!valid_team_size(teamWarps)) return cudaErrorInvalidValue;
-  return mixed ? set_smem<true>(teamWarps, smemBytes) : set_smem<false>(teamWarps, smemBytes);
+  if (fleet) return mixed ? set_smem<true, true>(teamWarps, smemBytes) : set_smem<false, true>(teamWarps, smemBytes);
+  return mixed ? set_smem<true, false>(teamWarps, smemBytes) : set_smem<false, false>(teamWarps, smemBytes);
 }
 
 cudaError_t launch_batch_kernel(bool mixed, int teamWarps, const DevModel& M, const DevBatch& B, const SlotLayout& L, int grid,
@@ -247,15 +262,22 @@ cudaError_t launch_batch_kernel(bool mixed, int teamWarps, const DevModel& M, co
   if (!valid_team_size(teamWarps) || teamsPerBlock * teamWarps > kMaxWarpsPerBlock) return cudaErrorInvalidValue;
   const std::size_t smem = static_cast<std::size_t>(teamsPerBlock) * L.bytes;
   const int threads = teamsPerBlock * teamWarps * 32;
-  if (mixed) launch<true>(teamWarps, M, B, L, grid, threads, smem, stream);
-  else launch<false>(teamWarps, M, B, L, grid, threads, smem, stream);
+  const bool fleet = B.models != nullptr;
+  if (fleet) {
+    if (mixed) launch<true, true>(teamWarps, M, B, L, grid, threads, smem, stream);
+    else launch<false, true>(teamWarps, M, B, L, grid, threads, smem, stream);
+  } else {
+    if (mixed) launch<true, false>(teamWarps, M, B, L, grid, threads, smem, stream);
+    else launch<false, false>(teamWarps, M, B, L, grid, threads, smem, stream);
+  }
   return cudaGetLastError();
 }
 
-cudaError_t batch_kernel_occupancy(bool mixed, int teamWarps, int teamsPerBlock, std::size_t smemBytes, int* blocksPerSM) {
+cudaError_t batch_kernel_occupancy(bool mixed, int teamWarps, int teamsPerBlock, std::size_t smemBytes, int* blocksPerSM, bool fleet) {
   if (!valid_team_size(teamWarps)) return cudaErrorInvalidValue;
   const int threads = teamsPerBlock * teamWarps * 32;
-  return mixed ? occupancy<true>(teamWarps, threads, smemBytes, blocksPerSM) : occupancy<false>(teamWarps, threads, smemBytes, blocksPerSM);
+  if (fleet) return mixed ? occupancy<true, true>(teamWarps, threads, smemBytes, blocksPerSM) : occupancy<false, true>(teamWarps, threads, smemBytes, blocksPerSM);
+  return mixed ? occupancy<true, false>(teamWarps, threads, smemBytes, blocksPerSM) : occupancy<false, false>(teamWarps, threads, smemBytes, blocksPerSM);
 }
 
 // ----------------------------------------------------------------------------- the batch run without device allocation

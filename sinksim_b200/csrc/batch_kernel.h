@@ -23,10 +23,10 @@ constexpr int kMinBlocksPerSM = SSB_MIN_BLOCKS;
 static_assert(kMaxWarpsPerBlock >= 8, "a block must hold an eight-warp team");
 
 bool valid_team_size(int teamWarps);
-cudaError_t configure_batch_kernel(bool mixed, int teamWarps, std::size_t smemBytes);
+cudaError_t configure_batch_kernel(bool mixed, int teamWarps, std::size_t smemBytes, bool fleet = false);
 cudaError_t launch_batch_kernel(bool mixed, int teamWarps, const DevModel& M, const DevBatch& B, const SlotLayout& L, int grid,
                                 int teamsPerBlock, cudaStream_t stream);
-cudaError_t batch_kernel_occupancy(bool mixed, int teamWarps, int teamsPerBlock, std::size_t smemBytes, int* blocksPerSM);
+cudaError_t batch_kernel_occupancy(bool mixed, int teamWarps, int teamsPerBlock, std::size_t smemBytes, int* blocksPerSM, bool fleet = false);
 
 // A batch run whose scratch lives in a fixed device array of the library (see batch_kernel.cu); every pointer here
 // is the caller's device memory. state is count x 8 (t, zO, pitch, roll, vz, wth, wph, and the settle timer, which

@@ -158,6 +158,40 @@ int ssb_batch_create(const char* ship_path, const char* sim_path, const ssb_batc
   });
 }
 
+int ssb_fleet_create(int32_t n_models, const char* const* ship_paths, const char* const* sim_paths, const int32_t* instance_model,
+                     const ssb_batch_options* opt, ssb_batch** out) {
+  return guard([&] {
+    need(ship_paths, "ship_paths"); need(sim_paths, "sim_paths"); need(instance_model, "instance_model"); need(opt, "opt"); need(out, "out");
+    *out = nullptr;
+    if (n_models < 1) throw std::invalid_argument("a fleet needs at least one model");
+    if (opt->count < 1) throw std::invalid_argument("count must be at least 1");
+    const ssb::BatchOptions bo = to_options(*opt);
+    need_device();
+    std::vector<std::pair<std::shared_ptr<const ssb::CompiledShip>, ssb::CompiledSim>> models;
+    for (int32_t m = 0; m < n_models; ++m) {
+      need(ship_paths[m], "ship path"); need(sim_paths[m], "sim path");
+      auto ship = ssb::load_ship(ship_paths[m]);
+      ssb::CompiledSim sim = ssb::load_sim(sim_paths[m]);
+      ssb::check_pairing(*ship, sim);
+      models.emplace_back(std::move(ship), std::move(sim));
+    }
+    std::vector<std::int32_t> im(instance_model, instance_model + opt->count);
+    auto h = std::make_unique<ssb_batch>();
+    h->batch = std::make_shared<ssb::Batch>(std::move(models), std::move(im), bo);
+    *out = h.release();
+  });
+}
+
+int ssb_batch_instance_shape(const ssb_batch* b, int32_t instance, int32_t* model, int32_t* nodes, int32_t* connections) {
+  return guard([&] {
+    need(b, "batch");
+    const ssb::Batch::InstanceShape s = b->batch->instance_shape(instance);
+    if (model) *model = s.model;
+    if (nodes) *nodes = s.nodes;
+    if (connections) *connections = s.connections;
+  });
+}
+
 void ssb_batch_destroy(ssb_batch* b) { delete b; }
 
 int ssb_batch_nodes(const ssb_batch* b, int32_t* nodes, int32_t* connections) {

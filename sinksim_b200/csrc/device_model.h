@@ -140,6 +140,12 @@ struct DevBatch {
   std::int32_t yieldBelow;
   // when not null: the steps this launch took, summed over its instances (the per-phase work figure of the timing)
   unsigned long long* phaseSteps;
+  // A fleet (instances of several models in one launch): instance i steps models[model[i]], and its per-node,
+  // per-connection, event, monitor and mark arrays start at the offsets below instead of i x the model's size.
+  // Null for a batch of one model, which the kernel's model parameter describes.
+  const DevModel* models;
+  const std::int32_t* model;
+  const long long *nodeOff, *connOff, *evOff, *monOff, *markOff;
 };
 
 // Pose R = Ry(pitch) Rx(roll) and translation (kernel/frame.hpp:9-21), with the single-precision copies the
@@ -183,11 +189,11 @@ constexpr int kMaxLevelGroupsPerWarp = 32 / (kLevelLanes<false> < kLevelLanes<tr
 // passes holds maxGroup node-pass results per level lane group of the team (up to kMaxLevelGroupsPerWarp per warp); hydro the
 // eight buoyancy tree results; misc two ints the team broadcasts (the claimed instance, the yield decision); pose and
 // buoy the step's pose and buoyancy result, which every phase reads (kept here rather than in each thread's registers);
-// parked the run's values during the hydrostatic phases.
+// parked the run's values during the hydrostatic phases; model (fleets only) the team's copy of its instance's model.
 // tmp is the sixth column of the loads' per-node terms (the other five reuse area, zmax, hEff, aEff and acc, which
 // are dead by then); kSlotAliasDV places it on dV when there are at least as many connections as nodes.
 struct SlotLayout {
-  std::uint32_t vol, level, cx, cy, cz, area, zmax, hEff, aEff, acc, deg, dV, q, tmp, passes, hydro, misc, merged, pose, buoy, parked, bytes;
+  std::uint32_t vol, level, cx, cy, cz, area, zmax, hEff, aEff, acc, deg, dV, q, tmp, passes, hydro, misc, merged, pose, buoy, parked, model, bytes;
 };
 constexpr std::uint32_t kSlotAliasDV = 0xFFFFFFFFu;
 

@@ -617,26 +617,63 @@ __device__ __forceinline__ void unpark(const Parked* P, SimRegs& R) {
   R.by = P->by; R.bz = P->bz; R.founderT = P->founderT; R.foundered = P->foundered;
 }
 
-// Instance `inst`'s per-instance arrays: each pointer is formed where it is used from the batch's base pointers (kernel
-// parameters), so a thread holds one index rather than eight pointers through the step.
-struct InstPtrs {
+// Instance `inst`'s per-instance arrays. In a batch of one model each pointer is formed where it is used from the
+// batch's base pointers (kernel parameters) and inst x the model's sizes, so a thread holds one index rather than
+// eight pointers through the step; in a fleet (FLEET) the instance's offsets are loaded once when it is claimed.
+template <bool FLEET>
+struct InstPtrs;
+
+template <>
+struct InstPtrs<false> {
   const DevModel& M;
   const DevBatch& B;
   int inst;
   __device__ __forceinline__ std::size_t perConn() const { return static_cast<std::size_t>(inst) * M.nc; }
   __device__ __forceinline__ std::size_t perEvent() const { return static_cast<std::size_t>(inst) * M.evCap; }
+  __device__ __forceinline__ std::size_t perNode() const { return static_cast<std::size_t>(inst) * M.nn; }
+  __device__ __forceinline__ std::size_t perMonitor() const { return static_cast<std::size_t>(inst) * M.nmon; }
+  __device__ __forceinline__ std::size_t perMark() const { return static_cast<std::size_t>(inst) * M.nmark; }
   __device__ __forceinline__ const std::uint8_t* en() const { return B.en + perConn(); }
   __device__ __forceinline__ const double* area() const { return B.area + perConn(); }
   __device__ __forceinline__ const double* tOn() const { return B.tOn + perConn(); }
   __device__ __forceinline__ double* evT() const { return B.evT + perEvent(); }
   __device__ __forceinline__ std::int32_t* evId() const { return B.evId + perEvent(); }
   __device__ __forceinline__ std::int32_t* evKind() const { return B.evKind + perEvent(); }
-  __device__ __forceinline__ double* overT() const { return B.overT + static_cast<std::size_t>(inst) * M.nmon; }
-  __device__ __forceinline__ double* markT() const { return B.markT + static_cast<std::size_t>(inst) * M.nmark; }
+  __device__ __forceinline__ double* overT() const { return B.overT + perMonitor(); }
+  __device__ __forceinline__ double* markT() const { return B.markT + perMark(); }
+};
+
+template <>
+struct InstPtrs<true> {
+  const DevModel& M;
+  const DevBatch& B;
+  int inst;
+  const std::uint8_t* en_;
+  const double *area_, *tOn_;
+  double *evT_, *overT_, *markT_;
+  std::int32_t *evId_, *evKind_;
+  std::size_t node_;
+  __device__ __forceinline__ InstPtrs(const DevModel& m, const DevBatch& b, int i) : M(m), B(b), inst(i) {
+    const std::size_t c = static_cast<std::size_t>(B.connOff[i]), e = static_cast<std::size_t>(B.evOff[i]);
+    en_ = B.en + c; area_ = B.area + c; tOn_ = B.tOn + c;
+    evT_ = B.evT + e; evId_ = B.evId + e; evKind_ = B.evKind + e;
+    overT_ = B.overT + B.monOff[i]; markT_ = B.markT + B.markOff[i];
+    node_ = static_cast<std::size_t>(B.nodeOff[i]);
+  }
+  __device__ __forceinline__ std::size_t perNode() const { return node_; }
+  __device__ __forceinline__ const std::uint8_t* en() const { return en_; }
+  __device__ __forceinline__ const double* area() const { return area_; }
+  __device__ __forceinline__ const double* tOn() const { return tOn_; }
+  __device__ __forceinline__ double* evT() const { return evT_; }
+  __device__ __forceinline__ std::int32_t* evId() const { return evId_; }
+  __device__ __forceinline__ std::int32_t* evKind() const { return evKind_; }
+  __device__ __forceinline__ double* overT() const { return overT_; }
+  __device__ __forceinline__ double* markT() const { return markT_; }
 };
 
 // The event log belongs to warp 0 of the team: only its lane 0 writes, only its count is stored.
-__device__ __forceinline__ void push_event(const DevModel& M, SimRegs& R, const InstPtrs& I, int id, int kind, int lane) {
+template <class IP>
+__device__ __forceinline__ void push_event(const DevModel& M, SimRegs& R, const IP& I, int id, int kind, int lane) {
   if (R.evCount < M.evCap) {
     if (lane == 0) { I.evT()[R.evCount] = R.t; I.evId()[R.evCount] = id; I.evKind()[R.evCount] = kind; }
     R.evCount++;
@@ -648,8 +685,8 @@ __device__ __forceinline__ void push_event(const DevModel& M, SimRegs& R, const 
 // per-connection work is spread over all 32 W threads of the team; scalars are computed redundantly and identically
 // by every thread, so every decision is uniform across the team.
 
-template <bool MIXED, int W>
-__device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimRegs& R, Slot& S, const InstPtrs& I, const Team<W>& T) {
+template <bool MIXED, int W, class IP>
+__device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimRegs& R, Slot& S, const IP& I, const Team<W>& T) {
   constexpr int kStride = 32 * W;
   const int lane = T.lane, rank = T.rank;
   const double tNow = R.t;

@@ -339,6 +339,28 @@ def sim_document(spec, sim_id, ship_id, ship_hash, cols, nodes, segs, hyd, conns
     }
 
 
+def fleet_specs(n, seed=20261204, columns=(1000, 20000), length=(100.0, 300.0), spaces=(16, 256)):
+    """n hull specs of a mixed fleet: column counts log-uniform over `columns` on a 5:1 (length:beam) grid, length
+    uniform over `length` (m) with the liner's proportions (beam, depth, sheer, draft, bottom rise and breach area
+    scaled by L / 269 m), compartments x decks between `spaces` (2-4 decks, at least two columns per compartment)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        cols = float(np.exp(rng.uniform(np.log(columns[0]), np.log(columns[1]))))
+        ny = max(3, int(round(math.sqrt(cols / 5.0))))
+        nx = max(10, int(round(cols / ny)))
+        L = float(rng.uniform(*length))
+        k = L / 269.0
+        decks = int(rng.integers(2, 5))
+        lo = max(2, -(-spaces[0] // decks))
+        hi = max(lo, min(spaces[1] // decks, nx // 2))
+        comps = int(rng.integers(lo, hi + 1))
+        out.append(HullSpec(L=L, B=28.0 * k, depth=18.0 * k, sheer=4.0 * k, nx=nx, ny=ny, n_comp=comps, n_decks=decks, draft=10.5 * k,
+                            gm=0.8 * k, end_rise=3.0 * k, breach_area=1.2 * k * k, bulkhead_top=13.5 * k, top_openings=3, breaches=min(6, comps - 1),
+                            reserve_breaches=min(2, max(0, comps - 1 - min(6, comps - 1)))))
+    return out
+
+
 def generate(spec=None, seed=20261203, ship_id="liner269", sim_id=None):
     """(ship document, sim document) of a parametric liner."""
     spec = spec or HullSpec()

@@ -67,3 +67,14 @@ def test_restatement_steps_the_liner_like_the_reference(liner, mixed):
         ref.step(chunk)
         ora.step(chunk)
         np.testing.assert_array_equal(ora.record(), ref.record())
+
+
+def test_fleet_specs_cover_the_configured_ranges():
+    specs = hullgen.fleet_specs(24, seed=5)
+    for i, sp in enumerate(specs):
+        ship, sim = hullgen.generate(sp, seed=i, ship_id=f"h{i}")
+        cols, spaces = ship["columns"]["n"], ship["nodes"]["n"]
+        assert 900 <= cols <= 21000, cols
+        assert 16 <= spaces <= 256, spaces
+        assert 3 <= sim["connections"]["n"] / spaces <= 5, sim["connections"]["n"] / spaces
+        assert 100 <= sp.L <= 300
