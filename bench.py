@@ -55,7 +55,42 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--model", default="titanic64", choices=("titanic64", "liner"),
                     help="titanic64: the reference's compiled model; liner: the generated benchmark liner")
+    ap.add_argument("--workload", default="uneven", choices=("uneven", "fleet"),
+                    help="uneven: one model, uneven run lengths; fleet: a mixed fleet of generated hulls in one batch")
+    ap.add_argument("--hulls", type=int, default=2048, help="fleet: hulls per GPU (one instance each)")
+    ap.add_argument("--fleet-tmax", type=float, default=7200.0, help="fleet: s; instances also stop when they founder or calm down")
     return ap.parse_args()
+
+
+def estimated_ops_per_step(columns, segments, nodes, connections):
+    """FP64 operations of one step of a model, estimated from its sizes with titanic64's measured per-step ratios (92.1%
+    of columns wet, 1.082 segment visits per segment with 44.3% of them wet, 1.109 node-pass trees per node, weir pows on
+    9.3% of the connections) and the per-unit counts of FP64_OPS_PER_STEP; gives 233,388 for titanic64."""
+    visits = 1.0822 * segments
+    return (7 * columns + 11 * 0.9206 * columns + 10 * visits + 11.5 * 0.4430 * visits + 31 * 1.109 * nodes + 191
+            + 75 * 0.0931 * connections + 30 * connections + 40 * nodes)
+
+
+def _write_hull(job):
+    """One generated fleet hull (run in a spawned worker): (index, seed, spec args, directory) -> (ship, sim) paths."""
+    i, seed, spec, out = job
+    from sinksim_b200 import hullgen
+
+    return hullgen.write(out, spec=hullgen.HullSpec(**spec), seed=seed, ship_id=f"hull{i:05d}")
+
+
+def fleet_models(count, first, seed=20261204):
+    """The fleet's hulls first .. first+count-1, written in parallel; returns [(ship, sim)] and their sizes."""
+    import multiprocessing
+
+    from sinksim_b200 import hullgen
+
+    specs = hullgen.fleet_specs(first + count, seed=seed)[first:]
+    out = os.path.join(tempfile.gettempdir(), f"sinksim_b200_fleet_{seed}")
+    jobs = [(first + k, seed + first + k, vars(sp), out) for k, sp in enumerate(specs)]
+    with multiprocessing.get_context("spawn").Pool(os.cpu_count() or 1) as pool:
+        paths = pool.map(_write_hull, jobs, chunksize=8)
+    return paths
 
 
 MODELS = {
@@ -136,6 +171,33 @@ def make_batch(ssb, ship_p, sim_p, sim, rule, count, first, args, device):
     return b
 
 
+def cpu_fleet_rate(hulls, numerics, threads, t_max):
+    """The reference CPU engine on the fleet's first `threads` hulls, one sinksim_sweep process per hull in parallel;
+    returns (aggregate steps/s, steps, s, hulls): the steps of all processes over the longest of their own run times
+    (each process times its run, without its start-up and model loading)."""
+    tool = os.path.join(ROOT, "oracle", "_ref", "sinksim_sweep")
+    sample = hulls[:threads]
+    with tempfile.TemporaryDirectory() as d:
+        procs = []
+        for k, (ship_p, sim_p) in enumerate(sample):
+            sw = {"format": "sinksim.sweep", "formatVersion": 1, "ship": "", "sim": "", "tMax": t_max, "every": 30, "stopWhenStable": True,
+                  "instances": [{"id": f"hull{k}"}]}
+            p = os.path.join(d, f"h{k}.sweep.json")
+            with open(p, "w") as f:
+                json.dump(sw, f)
+            procs.append(subprocess.Popen([tool, ship_p, sim_p, p, "--numerics", numerics, "--threads", "1"], stdout=subprocess.PIPE,
+                                          stderr=subprocess.STDOUT, text=True))
+        outs = [pr.communicate()[0] for pr in procs]
+    steps, longest = 0, 0.0
+    for pr, o in zip(procs, outs):
+        if pr.returncode != 0:
+            raise RuntimeError(o)
+        m = re.search(r"(\d+) steps in ([0-9.]+) s", o)
+        steps += int(m.group(1))
+        longest = max(longest, float(m.group(2)))
+    return steps / longest, steps, longest, len(sample)
+
+
 def cpu_reference_rate(ship_p, sim_p, sim, numerics, instances, t_max, threads, first=0):
     """The reference CPU engine's own sweep tool on `instances` instances of the workload; returns (steps/s, steps, s)."""
     from sinksim_b200.workloads import batch_uneven
@@ -187,6 +249,13 @@ def reference_arm(args):
 
 
 def workload_config(args):
+    if args.workload == "fleet":
+        return {"workload": f"mixed fleet of {args.hulls} generated hulls per GPU, one instance each, in one batch",
+                "model": "hulls of 1,000-20,000 columns (log-uniform, 5:1 grid), 16-256 spaces, 3-5 connections per space, L U(100, 300) m",
+                "global_batch": args.hulls * args.gpus, "numerics": args.numerics, "t_max_s": args.fleet_tmax, "dt_s": 0.25,
+                "retire": "founder | the reference's calm rule (stopWhenStable) | tMax",
+                "parallelism": f"hulls sharded over {args.gpus} GPU(s), no collective in the step",
+                "l2": "working set exceeds L2 for the largest hulls' geometry only; every step is a full batch from initial state"}
     return {"workload": f"{args.model} uneven-run-length batch, {args.count} instances per GPU", "model": MODELS[args.model],
             "global_batch": args.count * args.gpus, "numerics": args.numerics, "t_max_s": args.tmax, "dt_s": 0.25,
             "retire": "founder | sink (|trim|>15 deg, bow deck edge under) | settle (|pitch rate|<1e-5 rad/s for 600 s) | tMax",
@@ -209,13 +278,23 @@ def main():
     # one process per GPU; each rank steps its own contiguous block of the instances (weak scaling: count per GPU)
     ranks = Ranks(backend="nccl", timeout_s=600)
     world, rank, local = ranks.world, ranks.rank, ranks.local
-    ship_p, sim_p = model_paths(args.model)
-    ship, sim = load_model(ship_p, sim_p)
-    rule = deck_edge_rule(ship)
     barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum
-
-    first, _ = shard_bounds(args.count * world, world, rank)
-    batch = make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local)
+    if args.workload == "fleet":
+        first, _ = shard_bounds(args.hulls * world, world, rank)
+        hulls = fleet_models(args.hulls, first)
+        batch = ssb.Batch.fleet(hulls, list(range(len(hulls))), numerics=args.numerics, t_max=args.fleet_tmax, device=local,
+                                stop_when_stable=True)
+        hull_ops = []
+        for ship_p, sim_p in hulls:
+            s_doc, m_doc = load_model(ship_p, sim_p)
+            hull_ops.append(estimated_ops_per_step(len(s_doc["x"]), len(s_doc["segCol"]), len(s_doc["segCount"]), len(m_doc["ca"])))
+        ship_p, sim_p = hulls[0]
+    else:
+        ship_p, sim_p = model_paths(args.model)
+        ship, sim = load_model(ship_p, sim_p)
+        rule = deck_edge_rule(ship)
+        first, _ = shard_bounds(args.count * world, world, rank)
+        batch = make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local)
     # warm-up: full batches, untimed
     for _ in range(args.warmup):
         batch.reset()
@@ -257,7 +336,11 @@ def main():
         # the dominant kernel: the launch phase with the most device time; its work over its own CUDA-event time
         top = max(range(len(phase_ms)), key=lambda k: phase_ms[k])
         top_warps = batch.phase_stats()[top]["team_warps"]
-        achieved = FP64_OPS_PER_STEP * phase_steps[top] / (phase_ms[top] / 1e3)
+        ops_per_step = FP64_OPS_PER_STEP
+        if args.workload == "fleet":  # the steps' mix of hulls: ops per step weighted by each instance's steps
+            steps_i = [batch.summary(i)["steps"] for i in range(len(hull_ops))]
+            ops_per_step = sum(o * s for o, s in zip(hull_ops, steps_i)) / max(sum(steps_i), 1)
+        achieved = ops_per_step * phase_steps[top] / (phase_ms[top] / 1e3)
         phases = [{"team_warps": p["team_warps"], "device_ms_per_run": m / args.steps, "share": m / sum(phase_ms),
                    "sim_steps_per_run": s / args.steps} for p, m, s in zip(batch.phase_stats(), phase_ms, phase_steps)]
         out = {"metric": "sim-steps/s", "value": value, "unit": "sim-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -270,10 +353,16 @@ def main():
                             "kernel": f"run_batch<{args.numerics}, {top_warps}-warp teams> (launch phase {top})",
                             "phases": phases,
                             "peak_source": "measured on this GPU: separately rounded FP64 add+mul microbenchmark (no FMA, as the bits require)",
-                            "fp32_peak": fp32_peak / 1e12, "ops_per_sim_step": FP64_OPS_PER_STEP,
+                            "fp32_peak": fp32_peak / 1e12, "ops_per_sim_step": ops_per_step,
                             "note": "the step is issue/latency bound; HBM traffic is negligible (L2-resident working set)"},
                "clocks": clk}
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and args.workload == "fleet":
+            threads = os.cpu_count() or 1
+            v, s, secs, n = cpu_fleet_rate(hulls, args.numerics, threads, 1800.0)
+            out["cpu_baseline"] = {"value": v, "unit": "sim-steps/s", "cores": threads, "kind": "reference",
+                                   "sample": f"the first {n} hulls of the fleet, one reference sinksim_sweep process each (in parallel), each to its "
+                                             f"founder or 1800 s ({s} steps in {secs:.1f} s)"}
+        elif world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             n, t_max = 16 * threads, 3600.0
             v, s, secs = cpu_reference_rate(ship_p, sim_p, sim, args.numerics, n, t_max, threads)

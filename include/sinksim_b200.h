@@ -219,6 +219,11 @@ int ssb_batch_run_noalloc(const ssb_batch* b, int32_t count, const uint8_t* en, 
  * denominator of the engine's roofline; operations per second through *ops_per_s. No counterpart in the reference. */
 int ssb_measure_add_mul_peak(int32_t fp64, int32_t device, double* ops_per_s);
 
+/* FNV-1a 64-bit over n bytes, continuing from `state` (0xcbf29ce484222325 to start): the hash the compiled-file
+ * loaders verify (the reference's engine/include/sinksim/hash.hpp and tools/js/lib/fnv.js), for writers of compiled
+ * files such as the hull compiler. Needs no device. */
+uint64_t ssb_fnv1a64(uint64_t state, const void* data, size_t n);
+
 #ifdef __cplusplus
 }
 #endif

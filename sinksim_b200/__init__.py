@@ -98,7 +98,14 @@ _SIGNATURES = {
     "ssb_portable_math_device": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64]),
     "ssb_measure_add_mul_peak": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     "ssb_batch_run_noalloc": (C.c_int, [C.c_void_p, C.c_int32] + [C.c_void_p] * 13),
+    "ssb_fnv1a64": (C.c_uint64, [C.c_uint64, C.c_void_p, C.c_size_t]),
 }
+
+
+def fnv1a64(state, data):
+    """FNV-1a 64-bit of the bytes `data`, continuing from `state` (the compiled files' hash)."""
+    buf = bytes(data)
+    return int(lib().ssb_fnv1a64(state, buf, len(buf)))
 
 
 def add_mul_peak(fp64=True, device=0):

@@ -491,4 +491,13 @@ int ssb_measure_add_mul_peak(int32_t fp64, int32_t device, double* ops_per_s) {
   });
 }
 
+uint64_t ssb_fnv1a64(uint64_t state, const void* data, size_t n) {
+  const auto* p = static_cast<const unsigned char*>(data);
+  for (size_t i = 0; i < n; ++i) {
+    state ^= p[i];
+    state *= 1099511628211ULL;
+  }
+  return state;
+}
+
 }  // extern "C"

@@ -55,9 +55,14 @@ def _packed(kind, values):
 
 
 def _fnv(h, data):
-    for byte in data:
-        h = ((h ^ byte) * FNV_PRIME) & MASK64
-    return h
+    """FNV-1a 64-bit over data from state h: the library's routine when it is built, else the same loop here."""
+    try:
+        from . import fnv1a64
+        return fnv1a64(h, data)
+    except (ImportError, OSError, RuntimeError):
+        for byte in data:
+            h = ((h ^ byte) * FNV_PRIME) & MASK64
+        return h
 
 
 def hash_arrays(entries):
