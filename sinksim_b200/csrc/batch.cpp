@@ -380,6 +380,11 @@ void Batch::init(std::vector<std::pair<std::shared_ptr<const CompiledShip>, Comp
     // 7.8 M steps/s in two-warp teams, 6.4 and 5.5 M in single-warp teams).
     const int fit = (sms * 16) / std::max(opt_.count, 1);
     W1 = fit >= 8 ? 8 : fit >= 4 ? 4 : fit >= 2 ? 2 : fit >= 1 ? 1 : 2;
+    // Large slots (a fleet's largest hull sets the slot) fit few simulations per SM: start with teams big enough that
+    // the simulations that fit carry about 16 warps (a fleet of 2,048 hulls up to 256 spaces: 5 slots of 41.7 KB
+    // per SM, so 4-warp teams).
+    const int slotsPerSM = std::max(1, static_cast<int>(optin / cfg_.slotBytes));
+    while (W1 < 8 && W1 * slotsPerSM < 16) W1 *= 2;
   }
   cfg_.phases.push_back(plan(W1, opt_.teamsPerBlock, opt_.count));
   if (opt_.blocks > 0) cfg_.phases[0].blocks = opt_.blocks;
