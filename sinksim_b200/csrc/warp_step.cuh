@@ -700,19 +700,19 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
     const double v = S.vol[n];
     S.hEff[n] = v > kEmptyVolume ? S.level[n] : kNoHead;
     S.aEff[n] = v >= __ldg(M.vmax + n) ? __ldg(M.aov + n) : jmax(S.area[n], __ldg(M.amin + n));
+    S.deg[n] = 0;
   }
   T.sync();
-  for (int n = rank; n < M.nn; n += kStride) {
-    const int k0 = __ldg(M.incStart + n), k1 = k0 + __ldg(M.incCount + n);
-    int d = 0;
-    for (int k = k0; k < k1; ++k) {
-      const int c = __ldg(M.incConn + k);
-      if (!__ldg(I.en() + c)) continue;
-      const int a = __ldg(M.ca + c), b = __ldg(M.cb + c);
-      if (a >= 0 && S.hEff[a] < kNoHeadTest && S.hEff[b] < kNoHeadTest) continue;
-      ++d;
-    }
-    S.deg[n] = d;
+  // A node's degree is the number of its incident connections that are enabled and not between two empty spaces. Each
+  // such connection counts once at each of its nodes (the incidence lists hold it once at a when a >= 0 and once at b),
+  // counted per connection with shared-memory atomics: an integer count, the same in any order, and one round of
+  // independent loads instead of a walk down every node's incidence list.
+  for (int c = rank; c < M.nc; c += kStride) {
+    if (!__ldg(I.en() + c)) continue;
+    const int a = __ldg(M.ca + c), b = __ldg(M.cb + c);
+    if (a >= 0 && S.hEff[a] < kNoHeadTest && S.hEff[b] < kNoHeadTest) continue;
+    if (a >= 0) atomicAdd(&S.deg[a], 1);
+    atomicAdd(&S.deg[b], 1);
   }
   T.sync();
   for (int c = rank; c < M.nc; c += kStride) {
