@@ -1,18 +1,21 @@
-// One time step of one simulation, computed by one warp. The physics is the reference's kernel::step in the
-// "portable" (double precision) and "portable32" (single-precision column partials) numerics
+// One time step of one simulation, computed by a team of W warps (W = 1, 2, 4 or 8). The physics is the reference's
+// kernel::step in the "portable" (double precision) and "portable32" (single-precision column partials) numerics
 // (engine/include/sinksim/kernel/step.hpp:41-54), reproduced bit for bit:
 //
 //   * the buoyancy integral keeps the reference's 256 partial sums (partial p sums columns p, p+256, ... in
 //     order), reduces each group of 32 partials with the halving tree (offsets 16..1) and adds the eight group
-//     results in order (kernel/reduce.hpp:12-79, hydro.hpp:241-258). One warp computes all of them: lane l holds
-//     partial w*32+l of group w, and a shuffle butterfly performs the tree, each pair combined as (lower, upper);
+//     results in order (kernel/reduce.hpp:12-79, hydro.hpp:241-258). The team's warps share the eight groups: lane l
+//     holds partial w*32+l of group w, and a shuffle butterfly performs the tree, each pair combined as (lower, upper);
 //   * a node pass keeps the reference's 32 lane partials over strided segments and the same tree
-//     (hydro.hpp:305-316, reduce.hpp:52-71);
+//     (hydro.hpp:305-316, reduce.hpp:52-71); a group of kLevelLanes lanes forms them, each lane combining several
+//     tree lanes' partials in the tree's order before the shuffles, so a warp solves 32 / kLevelLanes groups at once;
 //   * every other reduction (group sums, incidence gathers, sea inflow, excess, loads, monitors, water) runs in
 //     the reference's serial order, and every expression keeps its operation order (no contraction: -fmad=false).
+//     The one count that is not a floating-point sum, a node's degree, is formed with shared-memory atomics.
 //
-// All 32 lanes hold identical copies of every scalar, so control flow stays uniform and no lane waits on another
-// except at __syncwarp points between phases that exchange per-node or per-connection arrays through shared memory.
+// Every thread of the team holds identical copies of the scalars it uses, so control flow stays uniform; the team's
+// threads wait on one another only at the team barrier (Team::sync: __syncwarp for one warp, a named barrier for
+// more) between phases that exchange per-node or per-connection arrays through shared memory.
 #pragma once
 
 #include <cstdint>
