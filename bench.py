@@ -336,10 +336,15 @@ def main():
         # the dominant kernel: the launch phase with the most device time; its work over its own CUDA-event time
         top = max(range(len(phase_ms)), key=lambda k: phase_ms[k])
         top_warps = batch.phase_stats()[top]["team_warps"]
-        ops_per_step = FP64_OPS_PER_STEP
+        ops_per_step, ops_source = FP64_OPS_PER_STEP, "exact unit counts of titanic64 (the C restatement's counters)"
+        traffic = KERNEL_DRAM_BYTES_PER_LAUNCH
         if args.workload == "fleet":  # the steps' mix of hulls: ops per step weighted by each instance's steps
             steps_i = [batch.summary(i)["steps"] for i in range(len(hull_ops))]
             ops_per_step = sum(o * s for o, s in zip(hull_ops, steps_i)) / max(sum(steps_i), 1)
+            ops_source, traffic = "estimated from each hull's size with titanic64's per-step ratios", None
+        elif args.model != "titanic64":
+            ops_per_step = estimated_ops_per_step(len(ship["x"]), len(ship["segCol"]), len(ship["segCount"]), len(sim["ca"]))
+            ops_source, traffic = "estimated from the model's size with titanic64's per-step ratios", None
         achieved = ops_per_step * phase_steps[top] / (phase_ms[top] / 1e3)
         phases = [{"team_warps": p["team_warps"], "device_ms_per_run": m / args.steps, "share": m / sum(phase_ms),
                    "sim_steps_per_run": s / args.steps} for p, m, s in zip(batch.phase_stats(), phase_ms, phase_steps)]
@@ -349,7 +354,7 @@ def main():
                "e2e": {"value": e2e, "unit": "sim-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                "gpu_launches": args.steps * info["phases"], "launch": info, "sim_steps_per_launch": steps_per_launch,
                "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
-                            "frac": achieved / fp64_peak, "traffic": KERNEL_DRAM_BYTES_PER_LAUNCH,
+                            "frac": achieved / fp64_peak, "traffic": traffic, "ops_source": ops_source,
                             "kernel": f"run_batch<{args.numerics}, {top_warps}-warp teams> (launch phase {top})",
                             "phases": phases,
                             "peak_source": "measured on this GPU: separately rounded FP64 add+mul microbenchmark (no FMA, as the bits require)",
