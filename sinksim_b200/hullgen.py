@@ -382,13 +382,16 @@ def generate(spec=None, seed=20261203, ship_id="liner269", sim_id=None):
 
 
 def write(out_dir, spec=None, seed=20261203, ship_id="liner269"):
-    """Writes <out_dir>/<ship_id>.ship.json and .sim.json; returns their paths."""
+    """Writes <out_dir>/<ship_id>.ship.json and .sim.json; returns their paths. Each file is written under a name of
+    this process's and then renamed, so processes writing the same hull at once (one per GPU) never read half a file."""
     ship, sim = generate(spec, seed, ship_id)
     os.makedirs(out_dir, exist_ok=True)
     paths = (os.path.join(out_dir, f"{ship_id}.ship.json"), os.path.join(out_dir, f"{ship_id}.sim.json"))
     for doc, p in zip((ship, sim), paths):
-        with open(p, "w") as f:
+        tmp = f"{p}.{os.getpid()}.tmp"
+        with open(tmp, "w") as f:
             json.dump(doc, f)
+        os.replace(tmp, p)
     return paths
 
 
