@@ -59,6 +59,7 @@ def parse():
                     help="uneven: one model, uneven run lengths; fleet: a mixed fleet of generated hulls in one batch")
     ap.add_argument("--hulls", type=int, default=2048, help="fleet: hulls per GPU (one instance each)")
     ap.add_argument("--fleet-tmax", type=float, default=7200.0, help="fleet: s; instances also stop when they founder or calm down")
+    ap.add_argument("--autotune", action="store_true", help="pick the launch shape by timing candidates first (outside the timed region)")
     return ap.parse_args()
 
 
@@ -159,10 +160,10 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_batch(ssb, ship_p, sim_p, sim, rule, count, first, args, device):
+def make_batch(ssb, ship_p, sim_p, sim, rule, count, first, args, device, **shape):
     from sinksim_b200.workloads import batch_uneven
 
-    b = ssb.Batch(ship_p, sim_p, count=count, numerics=args.numerics, t_max=args.tmax, device=device, rule=rule)
+    b = ssb.Batch(ship_p, sim_p, count=count, numerics=args.numerics, t_max=args.tmax, device=device, rule=rule, **shape)
     for i, (area, enabled) in enumerate(batch_uneven(sim, count, first=first)):
         for c, a in area.items():
             b.set_connection_area(i, c, a)
@@ -294,7 +295,12 @@ def main():
         ship, sim = load_model(ship_p, sim_p)
         rule = deck_edge_rule(ship)
         first, _ = shard_bounds(args.count * world, world, rank)
-        batch = make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local)
+        shape = {}
+        if args.autotune:
+            from sinksim_b200.autotune import tune
+
+            shape, _ = tune(lambda **s: make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local, **s))
+        batch = make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local, **shape)
     # warm-up: full batches, untimed
     for _ in range(args.warmup):
         batch.reset()
@@ -352,7 +358,7 @@ def main():
                "ms_per_step": dev_s_max * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                "dtype": "f64" if args.numerics == "portable" else "f32+f64", "data": "synthetic", "config": workload_config(args),
                "e2e": {"value": e2e, "unit": "sim-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-               "gpu_launches": args.steps * info["phases"], "launch": info, "sim_steps_per_launch": steps_per_launch,
+               "gpu_launches": args.steps * (info["phases"] + 1), "launch": info, "sim_steps_per_launch": steps_per_launch,
                "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
                             "frac": achieved / fp64_peak, "traffic": traffic, "ops_source": ops_source,
                             "kernel": f"run_batch<{args.numerics}, {top_warps}-warp teams> (launch phase {top})",

@@ -240,6 +240,11 @@ struct Batch::Impl {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> phaseEv;           // launch phase k ends at phaseEv[k + 1]; phaseEv[0] starts a round
+  // one run's launch chain as a CUDA graph (runs to the end in one launch per phase), captured at the first launch;
+  // graphKey holds the kernel arguments it was captured with, so that a moved buffer captures it again
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graphExec = nullptr;
+  std::vector<unsigned char> graphKey;
   DevBuf<unsigned long long> phaseSteps;      // steps per launch phase in the last launch()
   std::vector<float> lastPhaseMs;
   std::vector<unsigned long long> lastPhaseSteps;
@@ -444,6 +449,8 @@ Batch::~Batch() {
     if (I_->ev0) cudaEventDestroy(I_->ev0);
     if (I_->ev1) cudaEventDestroy(I_->ev1);
     for (cudaEvent_t e : I_->phaseEv) if (e) cudaEventDestroy(e);
+    if (I_->graphExec) cudaGraphExecDestroy(I_->graphExec);
+    if (I_->graph) cudaGraphDestroy(I_->graph);
     if (I_->stream) cudaStreamDestroy(I_->stream);
   }
 }
@@ -563,9 +570,58 @@ float Batch::launch() {
   cudaStream_t s = I.stream;
   const long long maxSteps = opt_.stepsPerLaunch > 0 ? opt_.stepsPerLaunch : LLONG_MAX;
   const std::size_t nph = cfg_.phases.size();
-  check(cudaMemcpyAsync(I.remaining.get(), &opt_.count, sizeof(std::int32_t), cudaMemcpyHostToDevice, s), "copy to device");
-  check(cudaMemsetAsync(I.phaseSteps.get(), 0, I.phaseSteps.bytes(), s), "memset");
   I.lastPhaseMs.assign(nph, 0.0f);
+  if (opt_.stepsPerLaunch <= 0) {
+    // the whole run in one CUDA graph: the counters, then per phase the queue reset, the kernel and its end event
+    std::vector<DevBatch> dbs(nph);
+    for (std::size_t k = 0; k < nph; ++k) {
+      dbs[k] = I.devBatch(opt_, maxSteps, k == 0 ? 1 : 0);
+      dbs[k].yieldBelow = cfg_.phases[k].yieldBelow;
+      dbs[k].phaseSteps = I.phaseSteps.get() + k;
+    }
+    const auto* kb = reinterpret_cast<const unsigned char*>(dbs.data());
+    std::vector<unsigned char> key(kb, kb + dbs.size() * sizeof(DevBatch));
+    if (!I.graphExec || key != I.graphKey) {
+      if (I.graphExec) { cudaGraphExecDestroy(I.graphExec); I.graphExec = nullptr; }
+      if (I.graph) { cudaGraphDestroy(I.graph); I.graph = nullptr; }
+      check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+      cudaError_t e = launch_start_run(I.remaining.get(), opt_.count, I.phaseSteps.get(), static_cast<int>(nph), s);
+      // the phase events are recorded by the graph itself (external records), so the phases stay timed one by one
+      if (e == cudaSuccess) e = cudaEventRecordWithFlags(I.phaseEv[0], s, cudaEventRecordExternal);
+      for (std::size_t k = 0; k < nph && e == cudaSuccess; ++k) {
+        const PhaseConfig& p = cfg_.phases[k];
+        e = cudaMemsetAsync(I.queue.get(), 0, sizeof(std::int32_t), s);
+        if (e == cudaSuccess) e = launch_batch_kernel(opt_.mixedPrecision, p.teamWarps, I.m0().dm, dbs[k], p.layout, p.blocks, p.teamsPerBlock, s);
+        if (e == cudaSuccess) e = cudaEventRecordWithFlags(I.phaseEv[k + 1], s, cudaEventRecordExternal);
+      }
+      cudaGraph_t g = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(s, &g);  // always ends the capture, also after a failed step
+      if (e == cudaSuccess) e = ec;
+      if (e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        check(e, "capturing the run's launches");
+      }
+      I.graph = g;
+      check(cudaGraphInstantiate(&I.graphExec, I.graph, 0), "cudaGraphInstantiate");
+      I.graphKey = std::move(key);
+    }
+    check(cudaEventRecord(I.ev0, s), "cudaEventRecord");
+    check(cudaGraphLaunch(I.graphExec, s), "cudaGraphLaunch");
+    check(cudaEventRecord(I.ev1, s), "cudaEventRecord");
+    check(cudaEventSynchronize(I.ev1), "kernel execution");
+    for (std::size_t k = 0; k < nph; ++k) {
+      float pm = 0;
+      check(cudaEventElapsedTime(&pm, I.phaseEv[k], I.phaseEv[k + 1]), "cudaEventElapsedTime");
+      I.lastPhaseMs[k] = pm;
+    }
+    float ms = 0;
+    check(cudaEventElapsedTime(&ms, I.ev0, I.ev1), "cudaEventElapsedTime");
+    I.phaseSteps.download(I.lastPhaseSteps, s);
+    check(cudaStreamSynchronize(s), "copy to host");
+    return ms;
+  }
+  // bounded launches: every round launches the phases again until no instance runs
+  check(launch_start_run(I.remaining.get(), opt_.count, I.phaseSteps.get(), static_cast<int>(nph), s), "kernel launch");
   check(cudaEventRecord(I.ev0, s), "cudaEventRecord");
   int first = 1;
   for (;;) {
@@ -587,7 +643,6 @@ float Batch::launch() {
       check(cudaEventElapsedTime(&pm, I.phaseEv[k], I.phaseEv[k + 1]), "cudaEventElapsedTime");
       I.lastPhaseMs[k] += pm;
     }
-    if (opt_.stepsPerLaunch <= 0) break;
     std::vector<std::int32_t> stops;
     I.stop.download(stops, s);
     check(cudaStreamSynchronize(s), "kernel execution");

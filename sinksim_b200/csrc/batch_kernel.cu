@@ -273,6 +273,18 @@ cudaError_t launch_batch_kernel(bool mixed, int teamWarps, const DevModel& M, co
   return cudaGetLastError();
 }
 
+namespace {
+__global__ void start_run(std::int32_t* remaining, std::int32_t count, unsigned long long* phaseSteps, int phases) {
+  if (threadIdx.x == 0) *remaining = count;
+  for (int k = static_cast<int>(threadIdx.x); k < phases; k += blockDim.x) phaseSteps[k] = 0;
+}
+}  // namespace
+
+cudaError_t launch_start_run(std::int32_t* remaining, std::int32_t count, unsigned long long* phaseSteps, int phases, cudaStream_t stream) {
+  start_run<<<1, 32, 0, stream>>>(remaining, count, phaseSteps, phases);
+  return cudaGetLastError();
+}
+
 cudaError_t batch_kernel_occupancy(bool mixed, int teamWarps, int teamsPerBlock, std::size_t smemBytes, int* blocksPerSM, bool fleet) {
   if (!valid_team_size(teamWarps)) return cudaErrorInvalidValue;
   const int threads = teamsPerBlock * teamWarps * 32;

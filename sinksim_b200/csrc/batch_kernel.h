@@ -27,6 +27,9 @@ cudaError_t configure_batch_kernel(bool mixed, int teamWarps, std::size_t smemBy
 cudaError_t launch_batch_kernel(bool mixed, int teamWarps, const DevModel& M, const DevBatch& B, const SlotLayout& L, int grid,
                                 int teamsPerBlock, cudaStream_t stream);
 cudaError_t batch_kernel_occupancy(bool mixed, int teamWarps, int teamsPerBlock, std::size_t smemBytes, int* blocksPerSM, bool fleet = false);
+// The counters a run starts from: `remaining` = count, the phases' step counters zero (a kernel, so that the run's
+// whole launch chain can be captured in a CUDA graph).
+cudaError_t launch_start_run(std::int32_t* remaining, std::int32_t count, unsigned long long* phaseSteps, int phases, cudaStream_t stream);
 
 // A batch run whose scratch lives in a fixed device array of the library (see batch_kernel.cu); every pointer here
 // is the caller's device memory. state is count x 8 (t, zO, pitch, roll, vz, wth, wph, and the settle timer, which
