@@ -258,6 +258,28 @@ __device__ __forceinline__ SegPartial<T> segment_partial(const typename Vec2<T>:
   return p;
 }
 
+// The partials of two tree lanes 16 apart (first segments fa and fa + 16), in one loop: each iteration takes the next
+// segment of each, so the two accumulation chains run side by side; each keeps its own segments' order. fa's lane has
+// at most one segment more than the other's.
+template <class T>
+__device__ __forceinline__ void segment_pair(const typename Vec2<T>::type* xy, const typename Vec2<T>::type* ab, const T* area, int fa,
+                                             int end, T R20, T R21, T R22, T tz, T iR, T h, SegPartial<T>& pa, SegPartial<T>& pb) {
+  pa = SegPartial<T>{T(0), T(0), T(0), T(0), T(0), T(1e9), T(-1e9)};
+  pb = pa;
+  int ja = fa;
+  for (; ja + 16 < end; ja += kLanes) {
+    const int jb = ja + 16;
+    const auto a0 = __ldg(xy + ja), b0 = __ldg(ab + ja), a1 = __ldg(xy + jb), b1 = __ldg(ab + jb);
+    const T A0 = __ldg(area + ja), A1 = __ldg(area + jb);
+    clip_segment<T>(a0.x, a0.y, b0.x, b0.y, A0, R20, R21, R22, tz, iR, h, pa);
+    clip_segment<T>(a1.x, a1.y, b1.x, b1.y, A1, R20, R21, R22, tz, iR, h, pb);
+  }
+  if (ja < end) {
+    const auto a0 = __ldg(xy + ja), b0 = __ldg(ab + ja);
+    clip_segment<T>(a0.x, a0.y, b0.x, b0.y, __ldg(area + ja), R20, R21, R22, tz, iR, h, pa);
+  }
+}
+
 // One level of the tree inside a lane: the lower tree lane's partial `lo` takes in the upper one's, with the operand
 // order of the butterfly steps.
 template <class T>
@@ -278,13 +300,19 @@ __device__ __forceinline__ PassR node_pass_body(const int* segStart, const int* 
   const int s0 = __ldg(segStart + n), s1 = s0 + __ldg(segCount + n);
   const T hT = static_cast<T>(h);
   const int f = s0 + L.sub;
-  SegPartial<T> p = segment_partial<T>(xy, ab, area, f, s1, R20, R21, R22, tz, iR, hT);
-  if constexpr (LANES == 16) {
-    tree_pair(p, segment_partial<T>(xy, ab, area, f + 16, s1, R20, R21, R22, tz, iR, hT));
+  SegPartial<T> p;
+  if constexpr (LANES == 32) {
+    p = segment_partial<T>(xy, ab, area, f, s1, R20, R21, R22, tz, iR, hT);
+  } else if constexpr (LANES == 16) {
+    SegPartial<T> b;
+    segment_pair<T>(xy, ab, area, f, s1, R20, R21, R22, tz, iR, hT, p, b);   // tree lanes sub and sub + 16
+    tree_pair(p, b);
   } else if constexpr (LANES == 8) {
-    tree_pair(p, segment_partial<T>(xy, ab, area, f + 16, s1, R20, R21, R22, tz, iR, hT));
-    SegPartial<T> q = segment_partial<T>(xy, ab, area, f + 8, s1, R20, R21, R22, tz, iR, hT);
-    tree_pair(q, segment_partial<T>(xy, ab, area, f + 24, s1, R20, R21, R22, tz, iR, hT));
+    SegPartial<T> b, q, d;
+    segment_pair<T>(xy, ab, area, f, s1, R20, R21, R22, tz, iR, hT, p, b);      // sub and sub + 16
+    tree_pair(p, b);
+    segment_pair<T>(xy, ab, area, f + 8, s1, R20, R21, R22, tz, iR, hT, q, d);  // sub + 8 and sub + 24
+    tree_pair(q, d);
     tree_pair(p, q);
   }
 #pragma unroll
