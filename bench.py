@@ -53,14 +53,20 @@ def parse():
     ap.add_argument("--count", type=int, default=4096, help="instances per GPU")
     ap.add_argument("--tmax", type=float, default=5 * 3600.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--model", default="titanic64", choices=("titanic64", "liner"),
-                    help="titanic64: the reference's compiled model; liner: the generated benchmark liner")
-    ap.add_argument("--workload", default="uneven", choices=("uneven", "fleet"),
-                    help="uneven: one model, uneven run lengths; fleet: a mixed fleet of generated hulls in one batch")
+    ap.add_argument("--model", default=None, choices=("titanic64", "liner"),
+                    help="titanic64: the reference's compiled model; liner: the generated benchmark liner "
+                         "(default: liner for --workload gradient, else titanic64)")
+    ap.add_argument("--workload", default="uneven", choices=("uneven", "fleet", "gradient"),
+                    help="uneven: one model, uneven run lengths; fleet: a mixed fleet of generated hulls in one batch; "
+                         "gradient: central-difference gradients of a trajectory objective, all stencils in one batch")
     ap.add_argument("--hulls", type=int, default=2048, help="fleet: hulls per GPU (one instance each)")
     ap.add_argument("--fleet-tmax", type=float, default=7200.0, help="fleet: s; instances also stop when they founder or calm down")
+    ap.add_argument("--points", type=int, default=256, help="gradient: parameter points per GPU (one gradient each)")
     ap.add_argument("--autotune", action="store_true", help="pick the launch shape by timing candidates first (outside the timed region)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.model is None:
+        args.model = "liner" if args.workload == "gradient" else "titanic64"
+    return args
 
 
 def estimated_ops_per_step(columns, segments, nodes, connections):
@@ -199,15 +205,9 @@ def cpu_fleet_rate(hulls, numerics, threads, t_max):
     return steps / longest, steps, longest, len(sample)
 
 
-def cpu_reference_rate(ship_p, sim_p, sim, numerics, instances, t_max, threads, first=0):
-    """The reference CPU engine's own sweep tool on `instances` instances of the workload; returns (steps/s, steps, s)."""
-    from sinksim_b200.workloads import batch_uneven
-
-    sw = {"format": "sinksim.sweep", "formatVersion": 1, "ship": "", "sim": "", "tMax": t_max, "every": 30, "stopWhenStable": False,
-          "instances": []}
-    for i, (area, enabled) in enumerate(batch_uneven(sim, instances, first=first)):
-        conns = [{"conn": c, "area": a} for c, a in area.items()] + [{"conn": c, "enabled": True} for c in enabled]
-        sw["instances"].append({"id": f"i{first + i}", "connections": conns})
+def _reference_sweep(ship_p, sim_p, sw, numerics, threads):
+    """Runs the reference CPU engine's own sweep tool on the sweep document `sw`; returns (steps, s) as the tool reports
+    them (its run time, without start-up and model loading)."""
     with tempfile.TemporaryDirectory() as d:
         p = os.path.join(d, "sample.sweep.json")
         with open(p, "w") as f:
@@ -217,8 +217,74 @@ def cpu_reference_rate(ship_p, sim_p, sim, numerics, instances, t_max, threads, 
     if r.returncode != 0:
         raise RuntimeError(r.stdout + r.stderr)
     m = re.search(r"(\d+) steps in ([0-9.]+) s \((\d+) steps/s aggregate\)", r.stdout)
-    steps, secs = int(m.group(1)), float(m.group(2))
+    return int(m.group(1)), float(m.group(2))
+
+
+def cpu_reference_rate(ship_p, sim_p, sim, numerics, instances, t_max, threads, first=0):
+    """The reference CPU engine's own sweep tool on `instances` instances of the workload; returns (steps/s, steps, s)."""
+    from sinksim_b200.workloads import batch_uneven
+
+    sw = {"format": "sinksim.sweep", "formatVersion": 1, "ship": "", "sim": "", "tMax": t_max, "every": 30, "stopWhenStable": False,
+          "instances": []}
+    for i, (area, enabled) in enumerate(batch_uneven(sim, instances, first=first)):
+        conns = [{"conn": c, "area": a} for c, a in area.items()] + [{"conn": c, "enabled": True} for c in enabled]
+        sw["instances"].append({"id": f"i{first + i}", "connections": conns})
+    steps, secs = _reference_sweep(ship_p, sim_p, sw, numerics, threads)
     return steps / secs, steps, secs
+
+
+# The gradient workload: gradients of a trajectory objective by central differences over 10 parameters, every point's
+# 2 P + 1 = 21 runs in one batch (the finite-difference arm; the hand-written adjoint is not built).
+GRADIENT_KINDS = ("door", "over", "down", "top")
+GRADIENT_BREACHES = 6
+GRADIENT_SEED = 20261205
+
+
+def gradient_space(sim):
+    """The gradient workload's 10 parameters: log scale factors of the door, overflow, deck-opening and
+    weather-deck-opening connections, then the areas (m2) of the first six open breaches."""
+    import numpy as np
+
+    from sinksim_b200.calibrate import ParamSpace
+
+    names = list(sim["kindNames"])
+    kind, en = np.asarray(sim["kind"]), np.asarray(sim["en"])
+    breaches = np.nonzero((kind == names.index("breach")) & (en != 0))[0][:GRADIENT_BREACHES]
+    return ParamSpace(sim, kinds=GRADIENT_KINDS, conns=[int(c) for c in breaches])
+
+
+def gradient_point(space, i):
+    """Point i of the seeded stream (i = -1: the hidden point behind the target trajectory): kind log scales N(0, 0.3)
+    (lognormal(0, 0.3) factors), breach areas U(0.1, 0.4) m2. Each point has its own generator, so a rank's block of
+    points does not depend on the number of ranks."""
+    import numpy as np
+
+    rng = np.random.default_rng([GRADIENT_SEED, i + 1])
+    nk = len(space.kinds)
+    return np.concatenate([rng.normal(0.0, 0.3, nk), rng.uniform(0.1, 0.4, space.dim - nk)])
+
+
+def gradient_times():
+    """The objective's 8 times, 990 s apart, to 2.2 h (7,920 s), and the curve interval that records exactly them."""
+    from sinksim_b200.calibrate import default_times
+
+    times = default_times()
+    return times, times[1] - times[0]
+
+
+def cpu_gradient_rate(ship_p, sim_p, space, thetas, h_rel, numerics, threads):
+    """The reference CPU engine's sweep tool on the central-difference stencils of the rows of `thetas` (2 P + 1 runs
+    each, to founder or the last objective time); returns (gradients/s, steps, s)."""
+    from sinksim_b200.calibrate import fd_stencil
+
+    times, every = gradient_times()
+    pts = fd_stencil(thetas, h_rel)
+    sw = {"format": "sinksim.sweep", "formatVersion": 1, "ship": "", "sim": "", "tMax": times[-1], "every": every,
+          "stopWhenStable": False,
+          "instances": [{"id": f"p{k}", "connections": [{"conn": c, "area": a} for c, a in space.areas(row).items()]}
+                        for k, row in enumerate(pts)]}
+    steps, secs = _reference_sweep(ship_p, sim_p, sw, numerics, threads)
+    return len(thetas) / secs, steps, secs
 
 
 def reference_arm(args):
@@ -230,6 +296,8 @@ def reference_arm(args):
 
     _, sim = load_model(ship_p, sim_p)
     threads = os.cpu_count() or 1
+    if args.workload == "gradient":
+        return reference_gradient_arm(args, ship_p, sim_p, sim, threads)
     n, t_max = 4 * threads, 1800.0
     for _ in range(args.warmup):
         cpu_reference_rate(ship_p, sim_p, sim, args.numerics, n, t_max, threads)
@@ -249,7 +317,48 @@ def reference_arm(args):
     return 0
 
 
+def reference_gradient_arm(args, ship_p, sim_p, sim, threads):
+    """--impl reference for the gradient workload: the reference CPU engine's sweep tool on the stencils of a sample of
+    the points, all host threads; prints the reference line in gradients/s."""
+    import numpy as np
+
+    from sinksim_b200.calibrate import DEFAULT_FD_STEP
+
+    space = gradient_space(sim)
+    k = max(1, threads // 2)
+    thetas = np.stack([gradient_point(space, i) for i in range(k)])
+    for _ in range(args.warmup):
+        cpu_gradient_rate(ship_p, sim_p, space, thetas, DEFAULT_FD_STEP, args.numerics, threads)
+    tot_s = 0.0
+    for _ in range(args.steps):
+        _, _, secs = cpu_gradient_rate(ship_p, sim_p, space, thetas, DEFAULT_FD_STEP, args.numerics, threads)
+        tot_s += secs
+    v = k * args.steps / tot_s
+    sample = (f"the stencils of the first {k} points ({k * (2 * space.dim + 1)} runs) per step, "
+              f"reference sinksim_sweep --threads {threads}")
+    print(json.dumps({"impl": "reference", "metric": "gradients/s", "value": v, "unit": "gradients/s", "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.numerics == "portable" else "f32+f64",
+                      "data": "synthetic", "config": workload_config(args),
+                      "cpu_baseline": {"value": v, "unit": "gradients/s", "cores": threads, "kind": "reference", "sample": sample},
+                      "e2e": {"value": v, "unit": "gradients/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
 def workload_config(args):
+    if args.workload == "gradient":
+        return {"workload": f"central-difference gradients of a trajectory objective on {args.model}, {args.points} points per GPU",
+                "model": MODELS[args.model], "global_batch": args.points * args.gpus,
+                "parameters": "10: log scale factors of the door, overflow, deck-opening and weather-deck-opening connections; "
+                              "areas of the first 6 open breaches",
+                "points": "kind scales lognormal(0, 0.3), breach areas U(0.1, 0.4) m2 (seeded); the target trajectory is the run at "
+                          "a hidden point from the same distribution",
+                "objective": "sum of squared trim (deg) and heave (m) residuals at 8 times, 990 s apart, to 7,920 s",
+                "gradient": "central differences, relative step 1e-2, 21 runs per gradient, all points' stencils in one batch",
+                "adjoint": "not built (finite-difference arm only)",
+                "numerics": args.numerics, "t_max_s": 7920.0, "dt_s": 0.25, "retire": "founder | tMax",
+                "parallelism": f"points sharded over {args.gpus} GPU(s), no collective in the step",
+                "l2": "working set (geometry 0.6 MB, per-instance state) is L2-resident by design; every step is a full batch from initial state"}
     if args.workload == "fleet":
         return {"workload": f"mixed fleet of {args.hulls} generated hulls per GPU, one instance each, in one batch",
                 "model": "hulls of 1,000-20,000 columns (log-uniform, 5:1 grid), 16-256 spaces, 3-5 connections per space, L U(100, 300) m",
@@ -264,10 +373,95 @@ def workload_config(args):
             "l2": "working set (geometry 0.6 MB, per-instance state) is L2-resident by design; every step is a full batch from initial state"}
 
 
+def gradient_bench(args):
+    """The gradient workload on the GPU: each step is one public value_and_grad call over the rank's points (their
+    stencils in one batch); value from the CUDA-event time of its launch, e2e from its host time."""
+    import numpy as np
+
+    import sinksim_b200 as ssb
+    from sinksim_b200.calibrate import DEFAULT_FD_STEP, BatchEvaluator, TrajectoryObjective, value_and_grad
+    from sinksim_b200.files import load_model
+    from sinksim_b200.shard import Ranks, shard_bounds
+
+    ranks = Ranks(backend="nccl", timeout_s=600)
+    world, rank, local = ranks.world, ranks.rank, ranks.local
+    ship_p, sim_p = model_paths(args.model)
+    ship, sim = load_model(ship_p, sim_p)
+    space = gradient_space(sim)
+    times, every = gradient_times()
+    ev = BatchEvaluator(ship_p, sim_p, space=space, numerics=args.numerics, t_max=times[-1], curve_every=every, device=local)
+    target = TrajectoryObjective.from_target(ev.run(gradient_point(space, -1)[None, :])[0], times)
+    first, _ = shard_bounds(args.points * world, world, rank)
+    thetas = np.stack([gradient_point(space, first + k) for k in range(args.points)])
+    h = DEFAULT_FD_STEP
+    for _ in range(args.warmup):
+        value_and_grad(ev, target, thetas, h)
+    ranks.barrier()
+    dev_ms, e2e_s, sim_steps = 0.0, 0.0, 0
+    phase_ms, phase_steps = None, None
+    with Clocks(local) as clocks:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            f, g = value_and_grad(ev, target, thetas, h)
+            e2e_s += time.perf_counter() - t0
+            last = ev.last
+            dev_ms += last["device_ms"]
+            sim_steps += last["steps"]
+            ps = last["phases"]
+            phase_ms = [p["device_ms"] for p in ps] if phase_ms is None else [a + p["device_ms"] for a, p in zip(phase_ms, ps)]
+            phase_steps = [p["steps"] for p in ps] if phase_steps is None else [a + p["steps"] for a, p in zip(phase_steps, ps)]
+    ranks.barrier()
+    if not (np.all(np.isfinite(f)) and np.all(np.isfinite(g))):
+        raise RuntimeError("non-finite objective or gradient")
+    dev_s_max = ranks.max(dev_ms / 1e3)
+    e2e_max = ranks.max(e2e_s)
+    grads = ranks.sum(float(args.points * args.steps))
+    all_steps = ranks.sum(float(sim_steps))
+    clk = clocks.summary()
+    if rank == 0:
+        h2d, d2h = last["transfer"]
+        fp64_peak = ssb.add_mul_peak(True, local)
+        top = max(range(len(phase_ms)), key=lambda k: phase_ms[k])
+        if args.model == "titanic64":
+            ops_per_step, ops_source = FP64_OPS_PER_STEP, "exact unit counts of titanic64 (the C restatement's counters)"
+        else:
+            ops_per_step = estimated_ops_per_step(len(ship["x"]), len(ship["segCol"]), len(ship["segCount"]), len(sim["ca"]))
+            ops_source = "estimated from the model's size with titanic64's per-step ratios"
+        achieved = ops_per_step * phase_steps[top] / (phase_ms[top] / 1e3)
+        phases = [{"team_warps": p["team_warps"], "device_ms_per_run": m / args.steps, "share": m / sum(phase_ms),
+                   "sim_steps_per_run": s / args.steps} for p, m, s in zip(last["phases"], phase_ms, phase_steps)]
+        out = {"metric": "gradients/s", "value": grads / dev_s_max, "unit": "gradients/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": dev_s_max * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64" if args.numerics == "portable" else "f32+f64", "data": "synthetic",
+               "config": workload_config(args),
+               "e2e": {"value": grads / e2e_max, "unit": "gradients/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+               "gpu_launches": args.steps * (last["launch"]["phases"] + 1), "launch": last["launch"],
+               "sim_steps_per_s": all_steps / dev_s_max, "runs_per_step": args.points * (2 * space.dim + 1),
+               "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
+                            "frac": achieved / fp64_peak, "traffic": None, "ops_source": ops_source,
+                            "kernel": f"run_batch<{args.numerics}, {phases[top]['team_warps']}-warp teams> (launch phase {top})",
+                            "phases": phases,
+                            "peak_source": "measured on this GPU: separately rounded FP64 add+mul microbenchmark (no FMA, as the bits require)",
+                            "ops_per_sim_step": ops_per_step},
+               "clocks": clk}
+        if world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            k = max(1, threads // 2)
+            v, s, secs = cpu_gradient_rate(ship_p, sim_p, space, thetas[:k], h, args.numerics, threads)
+            out["cpu_baseline"] = {"value": v, "unit": "gradients/s", "cores": threads, "kind": "reference",
+                                   "sample": f"the stencils of the first {k} points ({k * (2 * space.dim + 1)} runs, {s} steps in {secs:.1f} s), "
+                                             f"reference sinksim_sweep --numerics {args.numerics} --threads {threads}"}
+        print(json.dumps(out))
+    ranks.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload == "gradient":
+        return gradient_bench(args)
     import numpy as np
 
     import sinksim_b200 as ssb

@@ -128,6 +128,12 @@ int ssb_batch_restore(ssb_batch* b, int32_t instance, const double* record);
 int ssb_batch_set_connection_enabled(ssb_batch* b, int32_t instance, int32_t connection, int32_t enabled);
 int ssb_batch_set_connection_area(ssb_batch* b, int32_t instance, int32_t connection, double area);
 int ssb_batch_set_connection_activation(ssb_batch* b, int32_t instance, int32_t connection, double t_on);
+/* ssb_batch_set_connection_area over a block of instances: the area of connection connections[j] of instance first + i
+ * is areas[i * n_connections + j] (row-major, count x n_connections). Every index is checked before anything is
+ * written: on an error (SSB_EINVAL, or SSB_ESTATE after the run) nothing changes. No counterpart in the
+ * reference, whose setters take one value per call; one call here replaces count x n_connections of them. */
+int ssb_batch_set_connection_areas(ssb_batch* b, int32_t first, int32_t count, int32_t n_connections, const int32_t* connections,
+                                   const double* areas);
 /* Instance i takes instance i of a sweep file: sweep::apply (engine/include/sinksim/sweep.hpp:49-65) through the
  * setters above, as sinksim_cuda_run --sweep does (apps/sinksim_cuda_run.cpp:37-41). The sweep must have exactly
  * opt->count instances. */

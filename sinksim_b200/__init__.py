@@ -70,6 +70,7 @@ _SIGNATURES = {
     "ssb_batch_set_connection_enabled": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     "ssb_batch_set_connection_area": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double]),
     "ssb_batch_set_connection_activation": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double]),
+    "ssb_batch_set_connection_areas": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
     "ssb_batch_apply_sweep": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ssb_fleet_create": (C.c_int, [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), C.POINTER(C.c_int32), C.c_void_p, C.POINTER(C.c_void_p)]),
     "ssb_batch_instance_shape": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
@@ -251,6 +252,16 @@ class Batch:
 
     def set_connection_activation(self, instance, connection, t_on):
         _check(lib().ssb_batch_set_connection_activation(self._h, instance, connection, float(t_on)))
+
+    def set_connection_areas(self, first, connections, areas):
+        """Areas of a block of instances in one call: areas[i, j] (a [count, len(connections)] array) becomes the area
+        of connection connections[j] of instance first + i."""
+        conns = np.ascontiguousarray(connections, dtype=np.int32)
+        a = np.ascontiguousarray(areas, dtype=np.float64)
+        if a.ndim != 2 or a.shape[1] != conns.size:
+            raise SinksimError(-1, f"areas must be [count, {conns.size}], got {list(a.shape)}")
+        _check(lib().ssb_batch_set_connection_areas(self._h, int(first), a.shape[0], conns.size,
+                                                     conns.ctypes.data, a.ctypes.data))
 
     def apply_sweep(self, sweep_path, first=None):
         """Instance i takes sweep instance i; with `first`, sweep instance first + i (a shard of a longer sweep)."""

@@ -64,6 +64,26 @@ class ParamSpace:
             out[c] = theta[len(self.kinds) + j]
         return out
 
+    def area_matrix(self, thetas):
+        """(connections, areas [M, len(connections)]): areas(row) of every row of thetas as one array, with the same
+        values bit for bit (one exp per point and kind, then the single product per connection)."""
+        thetas = np.atleast_2d(np.asarray(thetas, dtype=np.float64))
+        if thetas.shape[1] != self.dim:
+            raise ValueError(f"theta has {thetas.shape[1]} values, the space {self.dim}")
+        cols, index = [], {}
+        for c in [c for members in self.members for c in members] + list(self.conns):
+            if c not in index:
+                index[c] = len(cols)
+                cols.append(c)
+        out = np.empty((thetas.shape[0], len(cols)))
+        area0 = np.asarray(self.area0)
+        for k, members in enumerate(self.members):
+            factor = np.array([math.exp(float(v)) for v in thetas[:, k]])
+            out[:, [index[c] for c in members]] = area0[members][None, :] * factor[:, None]
+        for j, c in enumerate(self.conns):
+            out[:, index[c]] = thetas[:, len(self.kinds) + j]
+        return cols, out
+
     def scales(self, theta):
         """The kind-scale factors of one point, as a sweep instance's "scale" would hold them."""
         return {k: math.exp(float(theta[i])) for i, k in enumerate(self.kinds)}
@@ -116,13 +136,18 @@ class BatchEvaluator:
         b = Batch(self.ship_path, self.sim_path, count=m, numerics=self.numerics, traced_instances=0, t_max=self.t_max,
                   curve_every=self.curve_every, device=self.device, rule=self.rule, stop_when_stable=self.stop_when_stable)
         try:
-            for i in range(m):
-                for c, a in self.space.areas(thetas[i]).items():
-                    b.set_connection_area(i, c, a)
+            cols, areas = self.space.area_matrix(thetas)
+            if cols:
+                b.set_connection_areas(0, cols, areas)
             b.upload()
-            self.device_ms += b.launch()
+            ms = b.launch()
+            self.device_ms += ms
             b.download()
             res = _results_from_batch(b, self.sim_doc, m)
+            # the last batch's shape and counts, for callers that report them (device ms, sim-steps, launch phases,
+            # bytes moved between host and device)
+            self.last = {"device_ms": ms, "steps": b.total_steps(), "phases": b.phase_stats(), "launch": b.launch_info(),
+                         "transfer": b.transfer_bytes()}
         finally:
             b.close()
         self.runs += 1

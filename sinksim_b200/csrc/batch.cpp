@@ -509,6 +509,28 @@ void Batch::set_connection_activation(std::int32_t inst, std::int32_t c, double 
   I_->hTOn[static_cast<std::size_t>(I_->connOff[static_cast<std::size_t>(inst)] + c)] = tOn;
 }
 
+void Batch::set_connection_areas(std::int32_t first, std::int32_t count, std::int32_t nConns, const std::int32_t* conns,
+                                 const double* areas) {
+  Impl& I = *I_;
+  if (I.uploaded) throw std::logic_error("Batch: set after run");
+  if (count < 0 || nConns < 0) throw std::invalid_argument("Batch: negative instance or connection count");
+  if (count == 0 || nConns == 0) return;
+  if (conns == nullptr || areas == nullptr) throw std::invalid_argument("Batch: null connection or area array");
+  if (first < 0 || static_cast<std::int64_t>(first) + count > opt_.count)
+    throw std::out_of_range("Batch: instances " + std::to_string(first) + " .. " +
+                            std::to_string(static_cast<std::int64_t>(first) + count - 1) + " out of range");
+  for (std::int32_t i = first; i < first + count; ++i) {
+    const std::int32_t nc = I.model(static_cast<std::size_t>(i)).NC;
+    for (std::int32_t j = 0; j < nConns; ++j)
+      if (conns[j] < 0 || conns[j] >= nc) throw std::out_of_range("Batch: connection " + std::to_string(conns[j]));
+  }
+  for (std::int32_t i = 0; i < count; ++i) {
+    const auto o = static_cast<std::size_t>(I.connOff[static_cast<std::size_t>(first + i)]);
+    const double* row = areas + static_cast<std::size_t>(i) * static_cast<std::size_t>(nConns);
+    for (std::int32_t j = 0; j < nConns; ++j) I.hArea[o + static_cast<std::size_t>(conns[j])] = row[j];
+  }
+}
+
 void Batch::apply_sweep(const Sweep& sw, std::int32_t first) {
   Impl& I = *I_;
   if (I.uploaded) throw std::logic_error("Batch: set after run");

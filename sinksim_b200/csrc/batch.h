@@ -81,6 +81,9 @@ class Batch {
   void set_connection_enabled(std::int32_t inst, std::int32_t c, bool en);
   void set_connection_area(std::int32_t inst, std::int32_t c, double area);
   void set_connection_activation(std::int32_t inst, std::int32_t c, double tOn);
+  // set_connection_area over a block: area of connection conns[j] of instance first + i = areas[i * nConns + j]. Every
+  // index is checked before anything is written, so a call that throws changes nothing.
+  void set_connection_areas(std::int32_t first, std::int32_t count, std::int32_t nConns, const std::int32_t* conns, const double* areas);
   // Instance i takes sweep instance first + i (a shard of a larger sweep when first > 0 or the sweep is longer);
   // results() then names the instances by those sweep instances' ids.
   void apply_sweep(const Sweep& sw, std::int32_t first = 0);

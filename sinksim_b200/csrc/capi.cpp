@@ -228,6 +228,14 @@ int ssb_batch_set_connection_area(ssb_batch* b, int32_t instance, int32_t c, dou
   return guard([&] { need(b, "batch"); b->batch->set_connection_area(instance, c, area); });
 }
 
+int ssb_batch_set_connection_areas(ssb_batch* b, int32_t first, int32_t count, int32_t n_connections, const int32_t* connections,
+                                   const double* areas) {
+  return guard([&] {
+    need(b, "batch");
+    b->batch->set_connection_areas(first, count, n_connections, connections, areas);
+  });
+}
+
 int ssb_batch_set_connection_activation(ssb_batch* b, int32_t instance, int32_t c, double t_on) {
   return guard([&] { need(b, "batch"); b->batch->set_connection_activation(instance, c, t_on); });
 }

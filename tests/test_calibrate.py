@@ -53,6 +53,23 @@ def test_param_space_is_the_sweep_product():
         sp.areas([0.0])
 
 
+def test_area_matrix_is_areas_row_by_row():
+    _, sim = load_model(*titanic())
+    member = int(np.nonzero(np.asarray(sim["kind"]) == list(sim["kindNames"]).index("breach"))[0][0])
+    sp = ParamSpace(sim, conns=(3, member))  # a breach set absolutely after its kind's scale, as a sweep override is
+    rng = np.random.default_rng(7)
+    thetas = np.concatenate([rng.normal(0.0, 0.3, (50, 4)), rng.uniform(0.1, 0.4, (50, 2))], axis=1)
+    cols, A = sp.area_matrix(thetas)
+    assert A.shape == (50, len(cols))
+    for r in range(50):
+        d = sp.areas(thetas[r])
+        assert list(d) == cols
+        assert np.array_equal(np.array(list(d.values())), A[r])  # the same bits
+    assert A[:, cols.index(member)].tolist() == thetas[:, 5].tolist()
+    with pytest.raises(ValueError):
+        sp.area_matrix(np.zeros((2, 3)))
+
+
 def test_central_differences_of_a_quadratic():
     A = np.array([[3.0, 0.5, 0.0], [0.5, 2.0, 0.1], [0.0, 0.1, 1.0]])
     thetas = np.array([[0.3, -0.2, 1.5], [2.0, 0.1, -3.0]])

@@ -1,0 +1,45 @@
+"""The block area setter (ssb_batch_set_connection_areas): a batch whose areas come from one block call runs bit for
+bit as the same batch set one connection at a time through the reference's per-value setter; a block call with a bad
+connection or instance range raises and writes nothing."""
+import numpy as np
+import pytest
+
+import sinksim_b200 as ssb
+from _support import load_model, titanic
+
+pytestmark = pytest.mark.gpu
+
+COUNT = 6
+
+
+def _run(setup):
+    b = ssb.Batch(*titanic(), count=COUNT, t_max=900.0, curve_every=60.0)
+    try:
+        setup(b)
+        b.run()
+        return ([b.state(i).tolist() for i in range(COUNT)], [b.summary(i) for i in range(COUNT)],
+                [b.curve(i).tolist() for i in range(COUNT)])
+    finally:
+        b.close()
+
+
+def test_block_area_setter_equals_single_setters():
+    _, sim = load_model(*titanic())
+    n = len(sim["area"])
+    rng = np.random.default_rng(11)
+    conns = [int(c) for c in rng.choice(n, 40, replace=False)]
+    areas = np.asarray(sim["area"], dtype=np.float64)[conns][None, :] * rng.lognormal(0.0, 0.3, (4, 40))
+
+    def single(b):
+        for i in range(4):
+            for j, c in enumerate(conns):
+                b.set_connection_area(1 + i, c, areas[i, j])
+
+    def block(b):
+        b.set_connection_areas(1, conns, areas)
+        with pytest.raises(ssb.SinksimError):  # a connection out of range: nothing is written
+            b.set_connection_areas(1, conns[:-1] + [n], 3.0 * areas)
+        with pytest.raises(ssb.SinksimError):  # instances 3 .. 6 of 6: nothing is written
+            b.set_connection_areas(3, conns, np.ones((4, 40)))
+
+    assert _run(single) == _run(block)
