@@ -435,7 +435,7 @@ def gradient_bench(args):
                "vs_baseline": None, "dtype": "f64" if args.numerics == "portable" else "f32+f64", "data": "synthetic",
                "config": workload_config(args),
                "e2e": {"value": grads / e2e_max, "unit": "gradients/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-               "gpu_launches": args.steps * (last["launch"]["phases"] + 1), "launch": last["launch"],
+               "gpu_launches": args.steps * last["launch"]["kernels"], "launch": last["launch"],
                "sim_steps_per_s": all_steps / dev_s_max, "runs_per_step": args.points * (2 * space.dim + 1),
                "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
                             "frac": achieved / fp64_peak, "traffic": None, "ops_source": ops_source,
@@ -552,7 +552,7 @@ def main():
                "ms_per_step": dev_s_max * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                "dtype": "f64" if args.numerics == "portable" else "f32+f64", "data": "synthetic", "config": workload_config(args),
                "e2e": {"value": e2e, "unit": "sim-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-               "gpu_launches": args.steps * (info["phases"] + 1), "launch": info, "sim_steps_per_launch": steps_per_launch,
+               "gpu_launches": args.steps * info["kernels"], "launch": info, "sim_steps_per_launch": steps_per_launch,
                "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
                             "frac": achieved / fp64_peak, "traffic": traffic, "ops_source": ops_source,
                             "kernel": f"run_batch<{args.numerics}, {top_warps}-warp teams> (launch phase {top})",

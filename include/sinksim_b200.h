@@ -64,6 +64,10 @@ typedef struct ssb_batch_options {
   /* a launch phase hands its unfinished instances to the next (twice the warps per simulation) once they number at
    * most this multiple of the next phase's resident simulations; 0: the default (2) */
   double handover_factor;
+  /* the claim order of the launch phases after the first: 0 (the default) the unfinished instances with the fewest
+   * steps done first, so that the runs with the most work left get the larger teams first; 1 by index. The results
+   * are the same either way. */
+  int32_t claim_by_index;
 } ssb_batch_options;
 
 typedef struct ssb_device_info {
@@ -89,7 +93,9 @@ typedef struct ssb_launch_info {
   int32_t team_warps, teams_per_block, blocks, blocks_per_sm, yield_below;
   int32_t tail_team_warps, tail_teams_per_block, tail_blocks, tail_blocks_per_sm;
   uint64_t slot_bytes;  /* shared memory of one simulation */
-  int32_t phases;       /* kernel launches of one run: the phases from the main team size up to the tail's */
+  int32_t phases;       /* launch phases of one run: from the main team size up to the tail's */
+  int32_t kernels;      /* kernel launches of one run to the end: the counters' reset, the phases and, before each
+                           phase after the first, the two kernels of its claim order */
 } ssb_launch_info;
 
 /* The message of the last failure on this thread. */

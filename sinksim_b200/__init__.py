@@ -35,7 +35,8 @@ class _Options(C.Structure):
                 ("team_warps", C.c_int32), ("tail_team_warps", C.c_int32), ("teams_per_block", C.c_int32), ("yield_below", C.c_int32),
                 ("blocks", C.c_int32), ("device", C.c_int32), ("rule_enabled", C.c_int32),
                 ("rule_pitch", C.c_double), ("rule_x", C.c_double), ("rule_y", C.c_double), ("rule_z", C.c_double),
-                ("rule_wth", C.c_double), ("rule_settle", C.c_double), ("stop_when_stable", C.c_int32), ("handover_factor", C.c_double)]
+                ("rule_wth", C.c_double), ("rule_settle", C.c_double), ("stop_when_stable", C.c_int32), ("handover_factor", C.c_double),
+                ("claim_by_index", C.c_int32)]
 
 
 class _DeviceInfo(C.Structure):
@@ -51,7 +52,8 @@ class _Summary(C.Structure):
 
 class _LaunchInfo(C.Structure):
     _fields_ = [(k, C.c_int32) for k in ("team_warps", "teams_per_block", "blocks", "blocks_per_sm", "yield_below", "tail_team_warps",
-                                         "tail_teams_per_block", "tail_blocks", "tail_blocks_per_sm")] + [("slot_bytes", C.c_uint64), ("phases", C.c_int32)]
+                                         "tail_teams_per_block", "tail_blocks", "tail_blocks_per_sm")] + [("slot_bytes", C.c_uint64), ("phases", C.c_int32),
+                                                                                            ("kernels", C.c_int32)]
 
 
 _lib = None
@@ -173,7 +175,7 @@ class Batch:
 
     def __init__(self, ship_path, sim_path, count=1, numerics="portable32", traced_instances=0, dense_steps=400, sample_every=60.0,
                  curve_every=0.0, t_max=5 * 3600.0, steps_per_launch=0, team_warps=0, tail_team_warps=-1, teams_per_block=0, yield_below=-1,
-                 blocks=0, device=0, rule=None, stop_when_stable=False, handover_factor=0.0, _fleet=None):
+                 blocks=0, device=0, rule=None, stop_when_stable=False, handover_factor=0.0, claim_by_index=False, _fleet=None):
         if numerics not in NUMERICS:
             raise SinksimError(-4, f"numerics {numerics!r} is not available on the GPU (portable or portable32)")
         o = _Options()
@@ -184,6 +186,7 @@ class Batch:
         o.blocks, o.device = blocks, device
         o.stop_when_stable = 1 if stop_when_stable else 0
         o.handover_factor = handover_factor
+        o.claim_by_index = 1 if claim_by_index else 0
         if rule:
             o.rule_enabled = 1
             o.rule_pitch, o.rule_x, o.rule_y, o.rule_z = rule["pitch"], rule["x"], rule["y"], rule["z"]

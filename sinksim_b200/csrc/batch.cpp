@@ -246,6 +246,8 @@ struct Batch::Impl {
   cudaGraphExec_t graphExec = nullptr;
   std::vector<unsigned char> graphKey;
   DevBuf<unsigned long long> phaseSteps;      // steps per launch phase in the last launch()
+  // claim order of the phases after the first (launch_order_unfinished): unfinished instances, their order, its length
+  DevBuf<std::int32_t> orderList, order, orderCount;
   std::vector<float> lastPhaseMs;
   std::vector<unsigned long long> lastPhaseSteps;
 
@@ -580,7 +582,28 @@ void Batch::upload() {
   I.queue.alloc(1);
   I.remaining.alloc(1);
   I.phaseSteps.alloc(cfg_.phases.size());
+  I.orderList.alloc(count); I.order.alloc(count); I.orderCount.alloc(1);
   I.error.alloc(1); check(cudaMemsetAsync(I.error.get(), 0, I.error.bytes(), s), "memset");
+}
+
+namespace {
+// Above this bound on the unfinished instances a phase claims by index: ranking them takes O(n^2) compares.
+constexpr int kMaxOrderedInstances = 16384;
+}  // namespace
+
+bool ordered_phase(const BatchOptions& opt, const LaunchConfig& cfg, std::size_t k) {
+  // a phase after the first of a run that goes to the end in one graph; the phase before hands over once at most
+  // yieldBelow instances remain, which bounds the instances to rank
+  if (k == 0 || k >= cfg.phases.size() || opt.claimByIndex || opt.stepsPerLaunch > 0) return false;
+  const int bound = cfg.phases[k - 1].yieldBelow;
+  return bound > 0 && bound <= kMaxOrderedInstances;
+}
+
+int kernels_per_run(const BatchOptions& opt, const LaunchConfig& cfg) {
+  int n = 1 + static_cast<int>(cfg.phases.size());  // start_run and one kernel per phase
+  for (std::size_t k = 1; k < cfg.phases.size(); ++k)
+    if (ordered_phase(opt, cfg, k)) n += 2;            // compact_unfinished and rank_unfinished
+  return n;
 }
 
 float Batch::launch() {
@@ -600,6 +623,7 @@ float Batch::launch() {
       dbs[k] = I.devBatch(opt_, maxSteps, k == 0 ? 1 : 0);
       dbs[k].yieldBelow = cfg_.phases[k].yieldBelow;
       dbs[k].phaseSteps = I.phaseSteps.get() + k;
+      if (ordered_phase(opt_, cfg_, k)) { dbs[k].order = I.order.get(); dbs[k].orderCount = I.orderCount.get(); }
     }
     const auto* kb = reinterpret_cast<const unsigned char*>(dbs.data());
     std::vector<unsigned char> key(kb, kb + dbs.size() * sizeof(DevBatch));
@@ -613,6 +637,9 @@ float Batch::launch() {
       for (std::size_t k = 0; k < nph && e == cudaSuccess; ++k) {
         const PhaseConfig& p = cfg_.phases[k];
         e = cudaMemsetAsync(I.queue.get(), 0, sizeof(std::int32_t), s);
+        if (e == cudaSuccess && dbs[k].order)
+          e = launch_order_unfinished(I.stop.get(), I.steps.get(), opt_.count, cfg_.phases[k - 1].yieldBelow, I.orderList.get(),
+                                      I.order.get(), I.orderCount.get(), s);
         if (e == cudaSuccess) e = launch_batch_kernel(opt_.mixedPrecision, p.teamWarps, I.m0().dm, dbs[k], p.layout, p.blocks, p.teamsPerBlock, s);
         if (e == cudaSuccess) e = cudaEventRecordWithFlags(I.phaseEv[k + 1], s, cudaEventRecordExternal);
       }

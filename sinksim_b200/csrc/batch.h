@@ -35,6 +35,7 @@ struct BatchOptions {
   std::int32_t blocks = 0;         // 0: persistent grid sized to the device
   RetireRule rule{};
   bool stopWhenStable = false;     // the reference's calm rule (a sweep's "stopWhenStable"); exclusive with `rule`
+  bool claimByIndex = false;       // phases after the first claim by index instead of fewest steps done first
   int device = 0;
 };
 
@@ -63,6 +64,12 @@ struct LaunchConfig {
   const PhaseConfig& main() const { return phases.front(); }
   PhaseConfig tail() const { return phases.size() > 1 ? phases.back() : PhaseConfig{}; }
 };
+
+// Does launch phase k claim its instances fewest steps done first (launch_order_unfinished) rather than by index?
+// Phases after the first of a run that goes to the end in one graph, unless opt.claimByIndex.
+bool ordered_phase(const BatchOptions& opt, const LaunchConfig& cfg, std::size_t k);
+// Kernel launches of one run that goes to the end in one graph: start_run, the phases, the claim-order kernels.
+int kernels_per_run(const BatchOptions& opt, const LaunchConfig& cfg);
 
 class Batch {
  public:

@@ -194,7 +194,10 @@ __global__ void __launch_bounds__(kMaxWarpsPerBlock * 32, kMinBlocksPerSM) run_b
   unsigned char* const slot = smem + static_cast<std::size_t>(team) * L.bytes;
   Slot S = carve_slot(slot, L);
   for (;;) {
-    if (T.leader()) S.misc[0] = atomicAdd(B.queue, 1);
+    if (T.leader()) {
+      const int q = atomicAdd(B.queue, 1);
+      S.misc[0] = B.order == nullptr ? q : (q < *B.orderCount ? B.order[q] : B.count);
+    }
     T.sync();
     const int inst = S.misc[0];
     T.sync();
@@ -282,6 +285,62 @@ __global__ void start_run(std::int32_t* remaining, std::int32_t count, unsigned 
 
 cudaError_t launch_start_run(std::int32_t* remaining, std::int32_t count, unsigned long long* phaseSteps, int phases, cudaStream_t stream) {
   start_run<<<1, 32, 0, stream>>>(remaining, count, phaseSteps, phases);
+  return cudaGetLastError();
+}
+
+// Claim order of a launch phase after the first. The phase before paused its instances; the one with the most work
+// left should get a larger team first, or it waits behind others for a free one and ends last. The work left is not
+// known, but a run's length is bounded (tMax, and in practice the founder/settle times), so the fewer steps an
+// instance has done, the more it has left: the order is by steps done, ascending, ties by index.
+namespace {
+constexpr int kOrderThreads = 256;
+
+__global__ void compact_unfinished(const std::int32_t* stop, std::int32_t count, std::int32_t* list, std::int32_t* n) {
+  for (std::int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    if (stop[i] == kRunning) list[atomicAdd(n, 1)] = i;
+}
+
+// order[rank of (steps[i], i) among the listed instances] = i: ranks of distinct keys, so a permutation of 0 .. n-1
+// whatever order the compaction listed them in.
+__global__ void __launch_bounds__(kOrderThreads) rank_unfinished(const long long* steps, const std::int32_t* list, const std::int32_t* n,
+                                                                 std::int32_t* order) {
+  __shared__ long long keyS[kOrderThreads];
+  __shared__ std::int32_t keyI[kOrderThreads];
+  const std::int32_t R = *n;
+  for (std::int32_t base = blockIdx.x * kOrderThreads; base < R; base += gridDim.x * kOrderThreads) {
+    const std::int32_t k = base + static_cast<std::int32_t>(threadIdx.x);
+    const bool mine = k < R;
+    const std::int32_t me = mine ? list[k] : 0;
+    const long long ms = mine ? steps[me] : 0;
+    std::int32_t rank = 0;
+    for (std::int32_t t0 = 0; t0 < R; t0 += kOrderThreads) {
+      __syncthreads();
+      const std::int32_t m = t0 + static_cast<std::int32_t>(threadIdx.x);
+      if (m < R) {
+        const std::int32_t j = list[m];
+        keyI[threadIdx.x] = j;
+        keyS[threadIdx.x] = steps[j];
+      }
+      __syncthreads();
+      const std::int32_t lim = min(kOrderThreads, R - t0);
+      if (mine)
+        for (std::int32_t j = 0; j < lim; ++j) rank += (keyS[j] < ms || (keyS[j] == ms && keyI[j] < me)) ? 1 : 0;
+    }
+    if (mine) order[rank] = me;
+  }
+}
+}  // namespace
+
+cudaError_t launch_order_unfinished(const std::int32_t* stop, const long long* steps, std::int32_t count, std::int32_t bound,
+                                    std::int32_t* list, std::int32_t* order, std::int32_t* n, cudaStream_t stream) {
+  if (count < 1 || bound < 1) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(n, 0, sizeof(std::int32_t), stream);
+  if (e != cudaSuccess) return e;
+  const int compactBlocks = static_cast<int>(std::min<std::int64_t>((static_cast<std::int64_t>(count) + 255) / 256, 1024));
+  compact_unfinished<<<compactBlocks, 256, 0, stream>>>(stop, count, list, n);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const int rankBlocks = static_cast<int>(std::min<std::int64_t>((static_cast<std::int64_t>(std::min(bound, count)) + kOrderThreads - 1) / kOrderThreads, 1024));
+  rank_unfinished<<<rankBlocks, kOrderThreads, 0, stream>>>(steps, list, n, order);
   return cudaGetLastError();
 }
 

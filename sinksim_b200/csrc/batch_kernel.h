@@ -30,6 +30,11 @@ cudaError_t batch_kernel_occupancy(bool mixed, int teamWarps, int teamsPerBlock,
 // The counters a run starts from: `remaining` = count, the phases' step counters zero (a kernel, so that the run's
 // whole launch chain can be captured in a CUDA graph).
 cudaError_t launch_start_run(std::int32_t* remaining, std::int32_t count, unsigned long long* phaseSteps, int phases, cudaStream_t stream);
+// The claim order of a launch phase after the first (DevBatch::order): the unfinished instances (stop == running),
+// fewest steps done first, ties by index, into order[0 .. *n). list and order hold count entries. `bound` is an upper
+// bound on the unfinished instances (it sizes the ranking grid; the ranking takes O(n^2) compares).
+cudaError_t launch_order_unfinished(const std::int32_t* stop, const long long* steps, std::int32_t count, std::int32_t bound,
+                                    std::int32_t* list, std::int32_t* order, std::int32_t* n, cudaStream_t stream);
 
 // A batch run whose scratch lives in a fixed device array of the library (see batch_kernel.cu); every pointer here
 // is the caller's device memory. state is count x 8 (t, zO, pitch, roll, vz, wth, wph, and the settle timer, which

@@ -91,6 +91,7 @@ ssb::BatchOptions to_options(const ssb_batch_options& o) {
   b.rule.settleTime = o.rule_settle;
   b.stopWhenStable = o.stop_when_stable != 0;
   if (o.handover_factor > 0) b.handoverFactor = o.handover_factor;
+  b.claimByIndex = o.claim_by_index != 0;
   return b;
 }
 
@@ -213,6 +214,7 @@ int ssb_batch_launch_info(const ssb_batch* b, ssb_launch_info* out) {
     out->tail_blocks_per_sm = t.blocksPerSM;
     out->slot_bytes = c.slotBytes;
     out->phases = static_cast<int32_t>(c.phases.size());
+    out->kernels = ssb::kernels_per_run(b->batch->options(), c);
   });
 }
 

@@ -140,6 +140,11 @@ struct DevBatch {
   std::int32_t yieldBelow;
   // when not null: the steps this launch took, summed over its instances (the per-phase work figure of the timing)
   unsigned long long* phaseSteps;
+  // when not null: queue position k claims instance order[k] (k < *orderCount) instead of instance k. Launch phases
+  // after the first take the unfinished instances with the fewest steps done first, so that the runs with the most
+  // work left to do are the first to get the larger teams.
+  const std::int32_t* order;
+  const std::int32_t* orderCount;
   // A fleet (instances of several models in one launch): instance i steps models[model[i]], and its per-node,
   // per-connection, event, monitor and mark arrays start at the offsets below instead of i x the model's size.
   // Null for a batch of one model, which the kernel's model parameter describes.

@@ -117,10 +117,17 @@ def test_launch_shape_does_not_change_bits(model):
     ref = None
     shapes = [dict(), dict(team_warps=1, tail_team_warps=0, teams_per_block=1), dict(team_warps=1, teams_per_block=16, blocks=1),
               dict(steps_per_launch=777), dict(team_warps=2), dict(team_warps=4), dict(team_warps=8),
-              dict(team_warps=1, tail_team_warps=4, yield_below=20), dict(team_warps=2, tail_team_warps=8, yield_below=20)]
+              dict(team_warps=1, tail_team_warps=4, yield_below=20), dict(team_warps=2, tail_team_warps=8, yield_below=20),
+              # 4 teams for 20 instances, handing over once 19 remain: the next phase claims the 16 not yet started
+              # before the 3 the first phase paused (fewest steps done first), or by index
+              dict(team_warps=1, teams_per_block=4, blocks=1, tail_team_warps=4, yield_below=19),
+              dict(team_warps=1, teams_per_block=4, blocks=1, tail_team_warps=4, yield_below=19, claim_by_index=True)]
     for kw in shapes:
         b, _ = _perturbed_batch(ship_p, sim_p, sim, 20, "portable", 1800.0, **kw)
         b.run()
+        info = b.launch_info()
+        ordered = 0 if kw.get("claim_by_index") or kw.get("steps_per_launch") else info["phases"] - 1
+        assert info["kernels"] == 1 + info["phases"] + 2 * ordered, kw
         states = np.stack([b.state(i) for i in range(20)])
         steps = [b.summary(i)["steps"] for i in range(20)]
         b.close()
