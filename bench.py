@@ -272,18 +272,22 @@ def gradient_times():
     return times, times[1] - times[0]
 
 
-def cpu_gradient_rate(ship_p, sim_p, space, thetas, h_rel, numerics, threads):
-    """The reference CPU engine's sweep tool on the central-difference stencils of the rows of `thetas` (2 P + 1 runs
-    each, to founder or the last objective time); returns (gradients/s, steps, s)."""
+def gradient_sweep(space, thetas, h_rel):
+    """The sweep document of the central-difference stencils of the rows of `thetas` (2 P + 1 instances each, in
+    fd_stencil's order): each instance sets the areas its point gives, to founder or the last objective time."""
     from sinksim_b200.calibrate import fd_stencil
 
     times, every = gradient_times()
-    pts = fd_stencil(thetas, h_rel)
-    sw = {"format": "sinksim.sweep", "formatVersion": 1, "ship": "", "sim": "", "tMax": times[-1], "every": every,
-          "stopWhenStable": False,
-          "instances": [{"id": f"p{k}", "connections": [{"conn": c, "area": a} for c, a in space.areas(row).items()]}
-                        for k, row in enumerate(pts)]}
-    steps, secs = _reference_sweep(ship_p, sim_p, sw, numerics, threads)
+    return {"format": "sinksim.sweep", "formatVersion": 1, "ship": "", "sim": "", "tMax": times[-1], "every": every,
+            "stopWhenStable": False,
+            "instances": [{"id": f"p{k}", "connections": [{"conn": c, "area": a} for c, a in space.areas(row).items()]}
+                          for k, row in enumerate(fd_stencil(thetas, h_rel))]}
+
+
+def cpu_gradient_rate(ship_p, sim_p, space, thetas, h_rel, numerics, threads):
+    """The reference CPU engine's sweep tool on the central-difference stencils of the rows of `thetas`; returns
+    (gradients/s, steps, s)."""
+    steps, secs = _reference_sweep(ship_p, sim_p, gradient_sweep(space, thetas, h_rel), numerics, threads)
     return len(thetas) / secs, steps, secs
 
 
