@@ -14,6 +14,7 @@ connections, set after the kind scales as a sweep's connection overrides are.
 
     python -m sinksim_b200.calibrate search  --observations obs.json [--rounds 5 --batch 264 --span 0.3]
     python -m sinksim_b200.calibrate lbfgs   [--restarts 64 --iters 30 --seed 1]
+    torchrun --nproc-per-node N -m sinksim_b200.calibrate lbfgs ...   (each evaluation's runs spread over N GPUs)
 """
 import argparse
 import json
@@ -290,10 +291,21 @@ def fd_reduce(thetas, values, h_rel):
     return f, g
 
 
-def value_and_grad(evaluator, objective, thetas, h_rel=DEFAULT_FD_STEP):
-    """Objective and its central-difference gradient at every row of thetas, all from one batch."""
+def value_and_grad(evaluator, objective, thetas, h_rel=DEFAULT_FD_STEP, ranks=None):
+    """Objective and its central-difference gradient at every row of thetas, all from one batch.
+
+    With `ranks` (sinksim_b200.shard.Ranks) of several processes, one per GPU, each rank runs a contiguous block of
+    the stencil's runs and the objective values are all-gathered (one collective per call), so every rank returns the
+    same values and gradients and an optimiser replicated on the ranks takes the same steps on each."""
     pts = fd_stencil(thetas, h_rel)
-    vals = [objective(inst) for inst in evaluator.run(pts)]
+    if ranks is None or ranks.world == 1:
+        vals = [objective(inst) for inst in evaluator.run(pts)]
+    else:
+        from .shard import shard_bounds
+
+        first, n = shard_bounds(len(pts), ranks.world, ranks.rank)
+        mine = [objective(inst) for inst in evaluator.run(pts[first:first + n])] if n else []
+        vals = ranks.all_gather(mine)
     return fd_reduce(thetas, vals, h_rel)
 
 
@@ -477,18 +489,28 @@ def main(argv=None):
                           "device_s": ev.device_ms / 1e3}))
         return 0
     # lbfgs: hidden kind scales drawn from the seed, the target trajectory from them, restarts from lognormal draws
+    # under torchrun (one process per GPU) every rank runs its block of each evaluation's stencil and the objective
+    # values are all-gathered, so every rank iterates the same L-BFGS
+    from .shard import Ranks
+
+    ranks = Ranks(backend="nccl")
     times = default_times()
     rng = np.random.default_rng(args.seed)
-    ev = BatchEvaluator(ship, sim, numerics=args.numerics, t_max=times[-1], curve_every=times[1] - times[0])
+    ev = BatchEvaluator(ship, sim, numerics=args.numerics, t_max=times[-1], curve_every=times[1] - times[0], device=ranks.local)
     hidden = rng.normal(0.0, 0.3, size=ev.space.dim)
     target = TrajectoryObjective.from_target(ev.run(hidden[None, :])[0], times)
     x0 = rng.normal(0.0, 0.3, size=(args.restarts, ev.space.dim))
     t0 = time.time()
-    x, fx, info = lbfgs_batched(lambda X: value_and_grad(ev, target, X, args.h), x0, max_iter=args.iters)
+    x, fx, info = lbfgs_batched(lambda X: value_and_grad(ev, target, X, args.h, ranks=ranks), x0, max_iter=args.iters)
+    wall = ranks.max(time.time() - t0)
+    device_s = ranks.max(ev.device_ms / 1e3)
+    instances = ranks.sum(float(ev.instances))
     best = int(np.argmin(fx))
-    print(json.dumps({"restarts": args.restarts, "best_objective": float(fx[best]), "recovery_error": float(np.max(np.abs(x[best] - hidden))),
-                      "evaluations": info["evaluations"], "instances": ev.instances, "wall_s": time.time() - t0,
-                      "device_s": ev.device_ms / 1e3}))
+    if ranks.rank == 0:
+        print(json.dumps({"restarts": args.restarts, "gpus": ranks.world, "best_objective": float(fx[best]),
+                          "recovery_error": float(np.max(np.abs(x[best] - hidden))), "evaluations": info["evaluations"],
+                          "instances": instances, "wall_s": wall, "device_s": device_s}))
+    ranks.close()
     return 0
 
 

@@ -90,6 +90,27 @@ class Ranks:
         self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
         return float(t.item())
 
+    def all_gather(self, values):
+        """Every rank's 1-D float64 values concatenated in rank order, on every rank: one all-gather of the lengths,
+        one of the values padded to the longest (NCCL on GPUs, gloo on the host)."""
+        import numpy as np
+
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        if not self.dist:
+            return v.copy()
+        import torch
+
+        device = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        n = torch.tensor([v.size], dtype=torch.int64, device=device)
+        sizes = [torch.empty_like(n) for _ in range(self.world)]
+        self.dist.all_gather(sizes, n)
+        lens = [int(s.item()) for s in sizes]
+        buf = torch.zeros(max(max(lens), 1), dtype=torch.float64, device=device)
+        buf[:v.size] = torch.from_numpy(v).to(device)
+        parts = [torch.empty_like(buf) for _ in range(self.world)]
+        self.dist.all_gather(parts, buf)
+        return np.concatenate([p[:k].cpu().numpy() for p, k in zip(parts, lens)])
+
     def gather(self, obj):
         """Every rank's object, in rank order, on rank 0 (None on the others)."""
         if not self.dist:

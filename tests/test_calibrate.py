@@ -108,3 +108,25 @@ def test_trajectory_objective():
     assert obj(inst) == 0.0
     other = {"curve": dict(inst["curve"], trim=[0.02 * k for k in range(9)])}
     assert obj(other) == pytest.approx(sum((0.01 * k) ** 2 for k in range(1, 9)))
+
+
+def test_two_gloo_ranks_split_the_stencil_and_agree(tmp_path):
+    import socket
+    import subprocess
+    import sys
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = str(s.getsockname()[1])
+    here = os.path.dirname(os.path.abspath(__file__))
+    outs = [tmp_path / f"rank{r}.json" for r in range(2)]
+    procs = [subprocess.Popen([sys.executable, os.path.join(here, "_calibrate_worker.py"), str(r), "2", port, str(outs[r])])
+             for r in range(2)]
+    for p in procs:
+        assert p.wait(timeout=180) == 0
+    res = [json.loads(o.read_text()) for o in outs]
+    # 7 points x (2 x 3 + 1) = 49 stencil runs: 25 on rank 0, 24 on rank 1
+    assert [r["rows_first_call"] for r in res] == [25, 24]
+    assert all(r["same_values"] and r["same_lbfgs"] for r in res)  # the same bits as one process, on every rank
+    assert res[0]["x"] == res[1]["x"]
+    assert res[0]["parts"] == res[1]["parts"] == [0.0, 2.5]  # rank 1 sent nothing
