@@ -13,7 +13,12 @@ complete batch: every instance from its initial state to its end, in one persist
 The CPU baseline is the reference CPU engine (oracle/_ref, built from the reference's own sources) run by its own
 sweep tool on a bounded sample of the same workload with all host cores. --impl reference times that tool alone.
 
+Other workloads: --workload fleet (a mixed fleet of generated hulls, one instance each, in one batch) and
+--workload gradient (gradients/s: central-difference gradients of a 10-parameter trajectory objective on the
+generated liner, 21 runs per gradient, every point's stencil in one batch; one step is one public value_and_grad call).
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--numerics portable|portable32]
+                    [--model titanic64|liner] [--workload uneven|fleet|gradient]
 """
 import argparse
 import json
