@@ -140,6 +140,12 @@ int ssb_batch_set_connection_activation(ssb_batch* b, int32_t instance, int32_t 
  * reference, whose setters take one value per call; one call here replaces count x n_connections of them. */
 int ssb_batch_set_connection_areas(ssb_batch* b, int32_t first, int32_t count, int32_t n_connections, const int32_t* connections,
                                    const double* areas);
+/* The order in which the first launch phase claims the instances: order[0 .. n) a permutation of 0 .. count-1
+ * (n == count; SSB_EINVAL otherwise, SSB_ESTATE after the run). A caller who knows which runs are long (an earlier
+ * evaluation of similar points) lists them first, so that they do not start last and end the batch late; the
+ * default is by index. The results do not depend on it. No counterpart in the reference, which launches every
+ * instance of a chunk at once. */
+int ssb_batch_set_claim_order(ssb_batch* b, const int32_t* order, int32_t n);
 /* Instance i takes instance i of a sweep file: sweep::apply (engine/include/sinksim/sweep.hpp:49-65) through the
  * setters above, as sinksim_cuda_run --sweep does (apps/sinksim_cuda_run.cpp:37-41). The sweep must have exactly
  * opt->count instances. */

@@ -73,6 +73,7 @@ _SIGNATURES = {
     "ssb_batch_set_connection_area": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double]),
     "ssb_batch_set_connection_activation": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double]),
     "ssb_batch_set_connection_areas": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
+    "ssb_batch_set_claim_order": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     "ssb_batch_apply_sweep": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ssb_fleet_create": (C.c_int, [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), C.POINTER(C.c_int32), C.c_void_p, C.POINTER(C.c_void_p)]),
     "ssb_batch_instance_shape": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
@@ -265,6 +266,12 @@ class Batch:
             raise SinksimError(-1, f"areas must be [count, {conns.size}], got {list(a.shape)}")
         _check(lib().ssb_batch_set_connection_areas(self._h, int(first), a.shape[0], conns.size,
                                                      conns.ctypes.data, a.ctypes.data))
+
+    def set_claim_order(self, order):
+        """The first launch phase claims the instances in this order (a permutation of range(count)), e.g. the
+        longest expected runs first."""
+        o = np.ascontiguousarray(order, dtype=np.int32)
+        _check(lib().ssb_batch_set_claim_order(self._h, o.ctypes.data, o.size))
 
     def apply_sweep(self, sweep_path, first=None):
         """Instance i takes sweep instance i; with `first`, sweep instance first + i (a shard of a longer sweep)."""

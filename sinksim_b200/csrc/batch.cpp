@@ -248,6 +248,9 @@ struct Batch::Impl {
   DevBuf<unsigned long long> phaseSteps;      // steps per launch phase in the last launch()
   // claim order of the phases after the first (launch_order_unfinished): unfinished instances, their order, its length
   DevBuf<std::int32_t> orderList, order, orderCount;
+  // the caller's claim order of the first phase (set_claim_order; empty: by index) and its device copy
+  std::vector<std::int32_t> hOrder0;
+  DevBuf<std::int32_t> order0, order0Count;
   std::vector<float> lastPhaseMs;
   std::vector<unsigned long long> lastPhaseSteps;
 
@@ -533,6 +536,20 @@ void Batch::set_connection_areas(std::int32_t first, std::int32_t count, std::in
   }
 }
 
+void Batch::set_claim_order(const std::int32_t* order, std::int32_t n) {
+  Impl& I = *I_;
+  if (I.uploaded) throw std::logic_error("Batch: set after run");
+  if (n != opt_.count) throw std::invalid_argument("Batch: a claim order lists every instance once (" + std::to_string(opt_.count) + ")");
+  if (order == nullptr) throw std::invalid_argument("Batch: null claim order");
+  std::vector<char> seen(static_cast<std::size_t>(n), 0);
+  for (std::int32_t k = 0; k < n; ++k) {
+    if (order[k] < 0 || order[k] >= n || seen[static_cast<std::size_t>(order[k])])
+      throw std::invalid_argument("Batch: the claim order is not a permutation of the instances (position " + std::to_string(k) + ")");
+    seen[static_cast<std::size_t>(order[k])] = 1;
+  }
+  I.hOrder0.assign(order, order + n);
+}
+
 void Batch::apply_sweep(const Sweep& sw, std::int32_t first) {
   Impl& I = *I_;
   if (I.uploaded) throw std::logic_error("Batch: set after run");
@@ -583,6 +600,10 @@ void Batch::upload() {
   I.remaining.alloc(1);
   I.phaseSteps.alloc(cfg_.phases.size());
   I.orderList.alloc(count); I.order.alloc(count); I.orderCount.alloc(1);
+  if (!I.hOrder0.empty()) {
+    I.order0.upload(I.hOrder0, s);
+    I.order0Count.upload(std::vector<std::int32_t>{opt_.count}, s);
+  }
   I.error.alloc(1); check(cudaMemsetAsync(I.error.get(), 0, I.error.bytes(), s), "memset");
 }
 
@@ -624,6 +645,7 @@ float Batch::launch() {
       dbs[k].yieldBelow = cfg_.phases[k].yieldBelow;
       dbs[k].phaseSteps = I.phaseSteps.get() + k;
       if (ordered_phase(opt_, cfg_, k)) { dbs[k].order = I.order.get(); dbs[k].orderCount = I.orderCount.get(); }
+      if (k == 0 && !I.hOrder0.empty()) { dbs[k].order = I.order0.get(); dbs[k].orderCount = I.order0Count.get(); }
     }
     const auto* kb = reinterpret_cast<const unsigned char*>(dbs.data());
     std::vector<unsigned char> key(kb, kb + dbs.size() * sizeof(DevBatch));
@@ -682,6 +704,7 @@ float Batch::launch() {
       DevBatch db = I.devBatch(opt_, maxSteps, first);
       db.yieldBelow = p.yieldBelow;
       db.phaseSteps = I.phaseSteps.get() + k;
+      if (k == 0 && !I.hOrder0.empty()) { db.order = I.order0.get(); db.orderCount = I.order0Count.get(); }
       check(launch_batch_kernel(opt_.mixedPrecision, p.teamWarps, I.m0().dm, db, p.layout, p.blocks, p.teamsPerBlock, s), "kernel launch");
       check(cudaEventRecord(I.phaseEv[k + 1], s), "cudaEventRecord");
       first = 0;

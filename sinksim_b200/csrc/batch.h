@@ -91,6 +91,10 @@ class Batch {
   // set_connection_area over a block: area of connection conns[j] of instance first + i = areas[i * nConns + j]. Every
   // index is checked before anything is written, so a call that throws changes nothing.
   void set_connection_areas(std::int32_t first, std::int32_t count, std::int32_t nConns, const std::int32_t* conns, const double* areas);
+  // The first launch phase claims the instances in this order (a permutation of 0 .. count-1) instead of by index:
+  // a caller who knows which runs are long (an earlier evaluation of similar points) lists them first, so that they
+  // do not start last and end the batch late. The results do not depend on it.
+  void set_claim_order(const std::int32_t* order, std::int32_t n);
   // Instance i takes sweep instance first + i (a shard of a larger sweep when first > 0 or the sweep is longer);
   // results() then names the instances by those sweep instances' ids.
   void apply_sweep(const Sweep& sw, std::int32_t first = 0);

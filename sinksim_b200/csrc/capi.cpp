@@ -238,6 +238,13 @@ int ssb_batch_set_connection_areas(ssb_batch* b, int32_t first, int32_t count, i
   });
 }
 
+int ssb_batch_set_claim_order(ssb_batch* b, const int32_t* order, int32_t n) {
+  return guard([&] {
+    need(b, "batch");
+    b->batch->set_claim_order(order, n);
+  });
+}
+
 int ssb_batch_set_connection_activation(ssb_batch* b, int32_t instance, int32_t c, double t_on) {
   return guard([&] { need(b, "batch"); b->batch->set_connection_activation(instance, c, t_on); });
 }

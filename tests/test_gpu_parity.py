@@ -121,9 +121,15 @@ def test_launch_shape_does_not_change_bits(model):
               # 4 teams for 20 instances, handing over once 19 remain: the next phase claims the 16 not yet started
               # before the 3 the first phase paused (fewest steps done first), or by index
               dict(team_warps=1, teams_per_block=4, blocks=1, tail_team_warps=4, yield_below=19),
-              dict(team_warps=1, teams_per_block=4, blocks=1, tail_team_warps=4, yield_below=19, claim_by_index=True)]
+              dict(team_warps=1, teams_per_block=4, blocks=1, tail_team_warps=4, yield_below=19, claim_by_index=True),
+              # the caller's claim order for the first phase (last instance first)
+              dict(team_warps=1, teams_per_block=4, blocks=1, tail_team_warps=4, yield_below=19, _order=list(range(19, -1, -1)))]
     for kw in shapes:
+        kw = dict(kw)
+        order = kw.pop("_order", None)
         b, _ = _perturbed_batch(ship_p, sim_p, sim, 20, "portable", 1800.0, **kw)
+        if order is not None:
+            b.set_claim_order(order)
         b.run()
         info = b.launch_info()
         ordered = 0 if kw.get("claim_by_index") or kw.get("steps_per_launch") else info["phases"] - 1

@@ -43,3 +43,18 @@ def test_block_area_setter_equals_single_setters():
             b.set_connection_areas(3, conns, np.ones((4, 40)))
 
     assert _run(single) == _run(block)
+
+
+def test_claim_order_must_be_a_permutation():
+    b = ssb.Batch(*titanic(), count=4, t_max=60.0)
+    try:
+        for bad in ([0, 1, 2], [0, 1, 1, 3], [0, 1, 2, 4], [-1, 0, 1, 2]):
+            with pytest.raises(ssb.SinksimError):
+                b.set_claim_order(bad)
+        b.set_claim_order([3, 2, 1, 0])
+        b.run()
+        assert all(b.summary(i)["steps"] == 240 for i in range(4))
+        with pytest.raises(ssb.SinksimError):  # after the run
+            b.set_claim_order([0, 1, 2, 3])
+    finally:
+        b.close()
