@@ -127,6 +127,14 @@ int ssb_batch_instance_shape(const ssb_batch* b, int32_t instance, int32_t* mode
 void ssb_batch_destroy(ssb_batch* b);
 int ssb_batch_nodes(const ssb_batch* b, int32_t* nodes, int32_t* connections);
 int ssb_batch_launch_info(const ssb_batch* b, ssb_launch_info* out);
+/* The kernel launches that one run to the end captures into its CUDA graph, in order, for a batch with these options
+ * and phases whose hand-over bounds are yield_below[0 .. n_phases-1] (phase k pauses once at most yield_below[k]
+ * instances remain; the last phase's is 0). kinds[i] is 0 for the counters' reset, 1 for the claim-order pair of
+ * kernels (list and rank the unfinished instances) and 2 for a phase's batch kernel; phases[i] is the phase it belongs
+ * to (-1 for the reset). *n receives the step count; at most cap steps are written (SSB_EINVAL if cap is too small).
+ * Host-only: needs no device. No counterpart in the reference, which launches in host-driven chunks. */
+int ssb_launch_plan(const ssb_batch_options* opt, int32_t n_phases, const int32_t* yield_below, int32_t* kinds, int32_t* phases,
+                    int32_t cap, int32_t* n);
 
 /* Per-instance setup before the run: cuda::Batch::restore / set_connection_enabled / set_connection_area /
  * set_connection_activation (engine/cuda/batch.cu:217-243). */
@@ -219,16 +227,18 @@ int ssb_portable_math_device(int32_t op, const double* x, const double* y, doubl
  * 0 for the settle timer of the retire rule), vol, level, cx, cy, cz (count x N each) are read as the initial states
  * and overwritten with the final ones; en (bytes), area, t_on (count x connections each) are the connection fields;
  * final_readouts (count x 7) receives each instance's final readouts, steps (int64) its step count and stop_reason its
- * stop (1 foundered, 2 t_max, 3 sink rule, 4 settle rule). Numerics, t_max and the retire rule are the batch's options;
- * curves and traces are not recorded. `stream` is a cudaStream_t (NULL: the default stream); the call returns once the
- * work is queued on it.
+ * stop (1 foundered, 2 t_max, 3 sink rule, 4 settle rule, 5 stable under the calm rule). Numerics, t_max, the retire
+ * rule and the calm rule (stop_when_stable) are the batch's options; curves and traces are not recorded. `stream` is a
+ * cudaStream_t (NULL: the default stream); the call returns once the work is queued on it.
  *
  * The kernel's scratch (the work-queue head, the count of unfinished instances, each instance's outputs, event log,
  * overflow and mark times) lives in a fixed 4 MiB device array of the library, which every GPU that loads the library
  * holds until the process exits; a count whose scratch does not fit returns SSB_EINVAL with the largest count that
- * would. The first call on a device looks up that array's device address (cudaGetSymbolAddress) and sets kernel
- * attributes, so make it before any stream capture. Every call shares the array and clears what must start at zero;
- * calls that overlap on the GPU race on it. The batch handle must have been created beforehand (which allocates). */
+ * would. The first call on a device sets up that array's device address (cudaGetSymbolAddress with the device
+ * current), so make it before any stream capture; later calls query the address again (no allocation). Every call also
+ * makes host-side runtime calls that allocate nothing (cudaSetDevice, cudaFuncSetAttribute for the team size it picks,
+ * an occupancy query). Every call shares the array and clears what must start at zero; calls that overlap on the GPU
+ * race on it. The batch handle must have been created beforehand (which allocates). */
 int ssb_batch_run_noalloc(const ssb_batch* b, int32_t count, const uint8_t* en, const double* area, const double* t_on, double* state,
                           double* vol, double* level, double* cx, double* cy, double* cz, double* final_readouts, int64_t* steps,
                           int32_t* stop_reason, void* stream);

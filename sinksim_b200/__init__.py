@@ -103,7 +103,27 @@ _SIGNATURES = {
     "ssb_measure_add_mul_peak": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     "ssb_batch_run_noalloc": (C.c_int, [C.c_void_p, C.c_int32] + [C.c_void_p] * 13),
     "ssb_fnv1a64": (C.c_uint64, [C.c_uint64, C.c_void_p, C.c_size_t]),
+    "ssb_launch_plan": (C.c_int, [C.POINTER(_Options), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
 }
+
+PLAN_KINDS = {0: "start_run", 1: "claim_order", 2: "phase"}
+
+
+def launch_plan(yield_below, steps_per_launch=0, claim_by_index=False):
+    """The kernels one run to the end captures in its CUDA graph, for launch phases whose hand-over bounds are
+    `yield_below` (one per phase, the last 0): [(kind, phase), ...] with kind start_run (1 kernel), claim_order (the 2
+    kernels that rank the unfinished instances) or phase (the phase's batch kernel). Host-only."""
+    o = _Options()
+    lib().ssb_batch_options_init(C.byref(o))
+    o.steps_per_launch = steps_per_launch
+    o.claim_by_index = 1 if claim_by_index else 0
+    y = np.ascontiguousarray(yield_below, dtype=np.int32)
+    cap = 2 * y.size + 1
+    kinds = np.empty(cap, dtype=np.int32)
+    phases = np.empty(cap, dtype=np.int32)
+    n = C.c_int32()
+    _check(lib().ssb_launch_plan(C.byref(o), y.size, y.ctypes.data, kinds.ctypes.data, phases.ctypes.data, cap, C.byref(n)))
+    return [(PLAN_KINDS[int(kinds[i])], int(phases[i])) for i in range(n.value)]
 
 
 def fnv1a64(state, data):

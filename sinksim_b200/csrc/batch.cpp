@@ -620,10 +620,18 @@ bool ordered_phase(const BatchOptions& opt, const LaunchConfig& cfg, std::size_t
   return bound > 0 && bound <= kMaxOrderedInstances;
 }
 
+std::vector<PlanStep> run_plan(const BatchOptions& opt, const LaunchConfig& cfg) {
+  std::vector<PlanStep> plan{{PlanStep::kStartRun, -1}};
+  for (std::size_t k = 0; k < cfg.phases.size(); ++k) {
+    if (ordered_phase(opt, cfg, k)) plan.push_back({PlanStep::kClaimOrder, static_cast<int>(k)});
+    plan.push_back({PlanStep::kPhase, static_cast<int>(k)});
+  }
+  return plan;
+}
+
 int kernels_per_run(const BatchOptions& opt, const LaunchConfig& cfg) {
-  int n = 1 + static_cast<int>(cfg.phases.size());  // start_run and one kernel per phase
-  for (std::size_t k = 1; k < cfg.phases.size(); ++k)
-    if (ordered_phase(opt, cfg, k)) n += 2;            // compact_unfinished and rank_unfinished
+  int n = 0;
+  for (const PlanStep& p : run_plan(opt, cfg)) n += p.kind == PlanStep::kClaimOrder ? 2 : 1;
   return n;
 }
 
@@ -653,15 +661,24 @@ float Batch::launch() {
       if (I.graphExec) { cudaGraphExecDestroy(I.graphExec); I.graphExec = nullptr; }
       if (I.graph) { cudaGraphDestroy(I.graph); I.graph = nullptr; }
       check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
-      cudaError_t e = launch_start_run(I.remaining.get(), opt_.count, I.phaseSteps.get(), static_cast<int>(nph), s);
-      // the phase events are recorded by the graph itself (external records), so the phases stay timed one by one
-      if (e == cudaSuccess) e = cudaEventRecordWithFlags(I.phaseEv[0], s, cudaEventRecordExternal);
-      for (std::size_t k = 0; k < nph && e == cudaSuccess; ++k) {
-        const PhaseConfig& p = cfg_.phases[k];
-        e = cudaMemsetAsync(I.queue.get(), 0, sizeof(std::int32_t), s);
-        if (e == cudaSuccess && dbs[k].order)
+      cudaError_t e = cudaSuccess;
+      for (const PlanStep& step : run_plan(opt_, cfg_)) {
+        if (e != cudaSuccess) break;
+        if (step.kind == PlanStep::kStartRun) {
+          e = launch_start_run(I.remaining.get(), opt_.count, I.phaseSteps.get(), static_cast<int>(nph), s);
+          // the phase events are recorded by the graph itself (external records), so the phases stay timed one by one
+          if (e == cudaSuccess) e = cudaEventRecordWithFlags(I.phaseEv[0], s, cudaEventRecordExternal);
+          continue;
+        }
+        const auto k = static_cast<std::size_t>(step.phase);
+        if (step.kind == PlanStep::kClaimOrder) {
+          // the previous phase's hand-over bound (k >= 1 here: ordered_phase never holds for the first phase)
           e = launch_order_unfinished(I.stop.get(), I.steps.get(), opt_.count, cfg_.phases[k - 1].yieldBelow, I.orderList.get(),
                                       I.order.get(), I.orderCount.get(), s);
+          continue;
+        }
+        const PhaseConfig& p = cfg_.phases[k];
+        e = cudaMemsetAsync(I.queue.get(), 0, sizeof(std::int32_t), s);
         if (e == cudaSuccess) e = launch_batch_kernel(opt_.mixedPrecision, p.teamWarps, I.m0().dm, dbs[k], p.layout, p.blocks, p.teamsPerBlock, s);
         if (e == cudaSuccess) e = cudaEventRecordWithFlags(I.phaseEv[k + 1], s, cudaEventRecordExternal);
       }
@@ -853,10 +870,17 @@ void Batch::run_noalloc(const NoAllocRun& run, cudaStream_t stream) const {
   if (I.fleet()) throw std::invalid_argument("run_noalloc: a batch of one model only");
   if (run.count < 1) throw std::invalid_argument("run_noalloc: count must be at least 1");
   const std::size_t need = noalloc_scratch_bytes(I.m0().dm, run.count), cap = noalloc_scratch_capacity();
-  if (need > cap)
+  if (need > cap) {
+    // the largest count that fits: the scratch grows with the count, so bisect on [0, run.count)
+    std::int32_t lo = 0, hi = run.count;
+    while (hi - lo > 1) {
+      const std::int32_t mid = lo + (hi - lo) / 2;
+      (noalloc_scratch_bytes(I.m0().dm, mid) <= cap ? lo : hi) = mid;
+    }
     throw std::invalid_argument("run_noalloc: " + std::to_string(run.count) + " instances of this model need " + std::to_string(need) +
                                 " bytes of scratch; the fixed scratch array holds " + std::to_string(cap) + " (at most " +
-                                std::to_string(run.count * (cap / need)) + " instances)");
+                                std::to_string(lo) + " instances)");
+  }
   if (!run.en || !run.area || !run.tOn || !run.state || !run.vol || !run.level || !run.cx || !run.cy || !run.cz || !run.finalRec || !run.steps ||
       !run.stop)
     throw std::invalid_argument("run_noalloc: a device pointer is NULL");
@@ -864,6 +888,7 @@ void Batch::run_noalloc(const NoAllocRun& run, cudaStream_t stream) const {
   NoAllocRun r = run;
   r.tMax = opt_.tMax;
   r.rule = opt_.rule;
+  r.stopWhenStable = opt_.stopWhenStable;
   // one launch, teams sized so that about 16 warps per SM carry the instances
   const int sms = I.info.multiprocessors;
   const int fit = std::max(1, (sms * 16) / r.count);

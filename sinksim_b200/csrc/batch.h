@@ -68,7 +68,17 @@ struct LaunchConfig {
 // Does launch phase k claim its instances fewest steps done first (launch_order_unfinished) rather than by index?
 // Phases after the first of a run that goes to the end in one graph, unless opt.claimByIndex.
 bool ordered_phase(const BatchOptions& opt, const LaunchConfig& cfg, std::size_t k);
-// Kernel launches of one run that goes to the end in one graph: start_run, the phases, the claim-order kernels.
+
+// The kernels of one run that goes to the end in one graph, in launch order: the counters' reset (start_run), then per
+// phase its claim-order kernels (compact_unfinished + rank_unfinished, only where ordered_phase holds) and the phase's
+// batch kernel. A caller's claim order for the first phase adds no kernel (it is uploaded, not computed). Batch::launch
+// captures exactly this list, and kernels_per_run counts it, so the two cannot disagree.
+struct PlanStep {
+  enum Kind { kStartRun = 0, kClaimOrder = 1, kPhase = 2 } kind;
+  int phase;  // the launch phase the step belongs to (-1 for kStartRun)
+};
+std::vector<PlanStep> run_plan(const BatchOptions& opt, const LaunchConfig& cfg);
+// Kernel launches of one run that goes to the end in one graph: start_run 1, each claim order 2, each phase 1.
 int kernels_per_run(const BatchOptions& opt, const LaunchConfig& cfg);
 
 class Batch {

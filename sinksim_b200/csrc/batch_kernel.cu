@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <mutex>
 
 #include "batch_kernel.h"
 #include "warp_step.cuh"
@@ -366,7 +367,23 @@ constexpr std::size_t kNoAllocScratchBytes = std::size_t(4) << 20;
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
 void* g_scratch_address[kMaxDevices] = {};
+
+// The device address of g_noalloc_scratch on the current device. The array's name in host code is a host-side stand-in,
+// not a device address, so the first call on a device looks the address up (cudaGetSymbolAddress, with that device
+// current). Later calls look it up again and replace the cached value if it moved: the query is cheap and allocates
+// nothing, and a cudaDeviceReset between calls reloads the module at a possibly different address. The mutex keeps host
+// threads that call at the same time from racing on the cache.
+cudaError_t scratch_address(int device, void** out) {
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  g_scratch_address[device] = p;
+  *out = p;
+  return cudaSuccess;
+}
 
 // The per-instance fields the batch kernel expects to find set before its first launch.
 __global__ void clear_noalloc_scratch(DevBatch B, int nmon, int nmark) {
@@ -409,15 +426,11 @@ cudaError_t run_batch_noalloc(bool mixed, const DevModel& M, const SlotLayout& L
   cudaError_t e = cudaGetDevice(&device);
   if (e != cudaSuccess) return e;
   if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-  if (!g_scratch_address[device]) {
-    // set-up, once per device with that device current: the host-side name of the array is not a device address
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch_address[device] = p;
-  }
   if (noalloc_scratch_bytes(M, r.count) > kNoAllocScratchBytes) return cudaErrorMemoryAllocation;
-  auto* base = static_cast<unsigned char*>(g_scratch_address[device]);
+  void* address = nullptr;
+  e = scratch_address(device, &address);
+  if (e != cudaSuccess) return e;
+  auto* base = static_cast<unsigned char*>(address);
   std::size_t off = 0;
   auto carve = [&](std::size_t bytes) { unsigned char* p = base + off; off += align256(bytes); return p; };
   const auto c = static_cast<std::size_t>(r.count);
@@ -444,6 +457,7 @@ cudaError_t run_batch_noalloc(bool mixed, const DevModel& M, const SlotLayout& L
   B.maxSteps = LLONG_MAX;
   B.firstLaunch = 1;
   B.rule = r.rule;
+  B.stopWhenStable = r.stopWhenStable ? 1 : 0;
   B.yieldBelow = 0;
   clear_noalloc_scratch<<<64, 256, 0, stream>>>(B, M.nmon, M.nmark);
   e = cudaGetLastError();

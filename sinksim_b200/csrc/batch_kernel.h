@@ -49,6 +49,7 @@ struct NoAllocRun {
   std::int32_t* stop;
   double tMax;
   RetireRule rule;
+  bool stopWhenStable;  // the reference's calm rule (stop reason 5), as in the batch's own runs
   int teamWarps, teamsPerBlock, blocks;
 };
 std::size_t noalloc_scratch_capacity();

@@ -218,6 +218,27 @@ int ssb_batch_launch_info(const ssb_batch* b, ssb_launch_info* out) {
   });
 }
 
+int ssb_launch_plan(const ssb_batch_options* opt, int32_t n_phases, const int32_t* yield_below, int32_t* kinds, int32_t* phases,
+                    int32_t cap, int32_t* n) {
+  return guard([&] {
+    need(opt, "opt"); need(yield_below, "yield_below"); need(n, "n");
+    if (n_phases < 1) throw std::invalid_argument("ssb_launch_plan: n_phases must be at least 1");
+    ssb::LaunchConfig c;
+    for (int32_t k = 0; k < n_phases; ++k) {
+      ssb::PhaseConfig p;
+      p.yieldBelow = yield_below[k];
+      c.phases.push_back(p);
+    }
+    const std::vector<ssb::PlanStep> plan = ssb::run_plan(to_options(*opt), c);
+    *n = static_cast<int32_t>(plan.size());
+    if (static_cast<int32_t>(plan.size()) > cap) throw std::invalid_argument("ssb_launch_plan: cap is below the plan's length");
+    for (std::size_t i = 0; i < plan.size(); ++i) {
+      if (kinds) kinds[i] = static_cast<int32_t>(plan[i].kind);
+      if (phases) phases[i] = plan[i].phase;
+    }
+  });
+}
+
 int ssb_batch_restore(ssb_batch* b, int32_t instance, const double* record) {
   return guard([&] { need(b, "batch"); need(record, "record"); b->batch->restore(instance, record); });
 }

@@ -30,7 +30,9 @@ POINTS = 6
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SINKSIM_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_calibration_fixtures.py <reference source tree> (or set SINKSIM_REFERENCE)")
     sys.path.insert(0, os.path.join(ref, "tools", "py"))
     import calibrate_gpu  # the reference's objective, used here only to score the fixture
 

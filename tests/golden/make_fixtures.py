@@ -59,4 +59,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SINKSIM_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_fixtures.py <reference source tree> (or set SINKSIM_REFERENCE)")
+    main(ref)

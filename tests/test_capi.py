@@ -57,3 +57,27 @@ def test_compare_results_on_host(tmp_path):
     assert ssb.compare_results(str(a), str(a))[1] == 0
     compared, differing, first = ssb.compare_results(str(a), str(b))
     assert differing == 1 and "curve[2] trim" in first
+
+
+def test_launch_plan_orders_only_phases_after_the_first():
+    """The kernels a run captures: the claim-order pair never precedes the first phase (it ranks what the phase before
+    left unfinished), with or without a caller's first-phase order, which adds no kernel."""
+    plan = ssb.launch_plan([512, 64, 0])
+    assert plan == [("start_run", -1), ("phase", 0), ("claim_order", 1), ("phase", 1), ("claim_order", 2), ("phase", 2)]
+    # one phase only: nothing to rank
+    assert ssb.launch_plan([0]) == [("start_run", -1), ("phase", 0)]
+    # claim by index, or bounded launches (which the host drives round by round): no ranking kernels
+    assert ssb.launch_plan([512, 0], claim_by_index=True) == [("start_run", -1), ("phase", 0), ("phase", 1)]
+    assert ssb.launch_plan([512, 0], steps_per_launch=2000) == [("start_run", -1), ("phase", 0), ("phase", 1)]
+    # a hand-over bound beyond what the ranking kernel takes: claim by index
+    assert ssb.launch_plan([100000, 0]) == [("start_run", -1), ("phase", 0), ("phase", 1)]
+
+
+def test_launch_plan_refuses_a_short_buffer():
+    o = ssb._Options()
+    ssb.lib().ssb_batch_options_init(C.byref(o))
+    y = (C.c_int32 * 3)(512, 64, 0)
+    kinds = (C.c_int32 * 2)()
+    n = C.c_int32()
+    rc = ssb.lib().ssb_launch_plan(C.byref(o), 3, y, kinds, None, 2, C.byref(n))
+    assert rc == -1 and n.value == 6
