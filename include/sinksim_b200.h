@@ -243,6 +243,38 @@ int ssb_batch_run_noalloc(const ssb_batch* b, int32_t count, const uint8_t* en, 
                           double* vol, double* level, double* cx, double* cy, double* cz, double* final_readouts, int64_t* steps,
                           int32_t* stop_reason, void* stream);
 
+/* ------------------------------------------------------------------------------------------------ the adjoint
+ * Gradients of a trajectory objective with respect to every connection area, for many instances of one compiled
+ * model, by a hand-written discrete adjoint of the portable (FP64) time step with checkpoints every K steps and
+ * recomputation in between. No counterpart in the reference, which has no gradients
+ * (docs/adr/0001-single-source-cpp-kernel.md:25-26); instances are set up like cuda::Batch's
+ * (engine/cuda/batch.cu:217-243).
+ *
+ * Each instance runs from the compiled initial state until t_max or its founder. The objective of instance i is
+ * J_i = sum_k (trim(s_k) - trim_i,k)^2 + (heave(s_k) - heave_i,k)^2 with trim in degrees (kernel/readouts.hpp:27) and
+ * heave the mean of the forward and aft drafts (:31-32), at the states s_k where a readout curve recorded every sample
+ * time would take its records (the first step start with t >= times[k]; the final state once the run has stopped).
+ * The gradient is d J_i / d area[c] along the branch path the run takes. */
+typedef struct ssb_adjoint ssb_adjoint;
+
+/* count instances; checkpoint_every steps between checkpoints (256 if 0); team_warps 4 or 8 (0: chosen). */
+int ssb_adjoint_create(const char* ship_path, const char* sim_path, int32_t count, double t_max, int32_t checkpoint_every,
+                       int32_t team_warps, int32_t device, ssb_adjoint** out);
+void ssb_adjoint_destroy(ssb_adjoint* a);
+int ssb_adjoint_set_connection_enabled(ssb_adjoint* a, int32_t instance, int32_t connection, int32_t enabled);
+/* As ssb_batch_set_connection_areas: areas[i * n_connections + j] for connection connections[j] of instance first + i. */
+int ssb_adjoint_set_connection_areas(ssb_adjoint* a, int32_t first, int32_t count, int32_t n_connections, const int32_t* connections,
+                                     const double* areas);
+/* n sample times (ascending) and the targets trim[i * n + k], heave[i * n + k] of every instance. */
+int ssb_adjoint_set_objective(ssb_adjoint* a, int32_t n, const double* times, const double* trim, const double* heave);
+/* Runs every instance forward and back. J (count), grad (count x connections, row-major), steps (count) and error
+ * (count; nonzero where a step took a branch without an adjoint) may be NULL; device_ms receives the kernel's time. */
+int ssb_adjoint_run(ssb_adjoint* a, double* J, double* grad, int64_t* steps, int32_t* error, float* device_ms);
+/* The run's trim and heave at the sample times (count x n each). */
+int ssb_adjoint_samples(const ssb_adjoint* a, double* trim, double* heave);
+/* Connections, team size and teams of the last run; bytes sent to and read back from the device in the last run. */
+int ssb_adjoint_info(const ssb_adjoint* a, int32_t* connections, int32_t* team_warps, int32_t* teams, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
+
 /* Measured rate of separately rounded adds and multiplies on the device (fp64 = 1: double, 0: float), the
  * denominator of the engine's roofline; operations per second through *ops_per_s. No counterpart in the reference. */
 int ssb_measure_add_mul_peak(int32_t fp64, int32_t device, double* ops_per_s);

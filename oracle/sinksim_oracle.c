@@ -88,6 +88,12 @@ struct sso_engine {
   int foundered;
   double founderT;
   sso_counters cnt;
+  /* the adjoint harness's hooks (tests only): every node pass, and the moment the levels are solved */
+  sso_pass_hook passHook;
+  sso_solved_hook solvedHook;
+  void* hookUser;
+  int32_t* passSlot;
+  double lastPose[14], lastBuoy[4];
 };
 
 #define DUP(dst, src, n, T)                                   \
@@ -279,6 +285,10 @@ static Pass node_pass(sso_engine* e, const Pose* F, int32_t n, double h) {
   r.dv = tot.dv * mu * iR;
   r.mx = tot.mx * mu; r.my = tot.my * mu; r.mz = tot.mz * mu;
   r.zmin = tot.zmin; r.zmax = tot.zmax;
+  if (e->passHook) {
+    const double rec[8] = {h, r.vol, r.dv, r.mx, r.my, r.mz, r.zmin, r.zmax};
+    e->passHook(e->hookUser, n, e->passSlot[n]++, rec);
+  }
   return r;
 }
 
@@ -602,7 +612,14 @@ static void body_and_events(sso_engine* e, const Pose* F, const Buoy* hb) {
 static void step_once(sso_engine* e) {
   const Pose F = pose_at(e, e->zO, e->pitch, e->roll);
   const Buoy hb = buoyancy(e, &F);
+  if (e->passHook) {
+    const double p[14] = {F.R00, F.R01, F.R02, F.R10, F.R11, F.R12, F.R20, F.R21, F.R22, F.tx, F.ty, F.tz, F.cth, 1 / F.R22};
+    memcpy(e->lastPose, p, sizeof p);
+    e->lastBuoy[0] = hb.V; e->lastBuoy[1] = hb.x; e->lastBuoy[2] = hb.y; e->lastBuoy[3] = hb.z;
+    for (int32_t n = 0; n < e->nn; ++n) e->passSlot[n] = 0;
+  }
   solve_levels(e, &F);
+  if (e->solvedHook) e->solvedHook(e->hookUser);
   const double seaIn = flows_and_volumes(e, &F);
   e->inflow = seaIn / e->dt;
   body_and_events(e, &F, &hb);
@@ -695,6 +712,7 @@ sso_engine* sso_create(const sso_ship* S, const sso_sim* M, int mixed) {
   ZERO(e->aEff, NN, double); ZERO(e->acc, NN, double); ZERO(e->excess, NN, double); ZERO(e->deg, NN, int32_t);
   ZERO(e->q, e->nc, double); ZERO(e->dV, e->nc, double); ZERO(e->over, e->nmon, double);
   ZERO(e->merged, e->ng, uint8_t); ZERO(e->passes, maxGroup, Pass);
+  ZERO(e->passSlot, NN, int32_t);
   e->evCap = e->nmon + e->nmark + 1;
   ZERO(e->evT, e->evCap, double); ZERO(e->evId, e->evCap, int32_t); ZERO(e->evKind, e->evCap, int32_t);
   ZERO(e->overT, e->nmon, double); ZERO(e->markT, e->nmark, double);
@@ -723,7 +741,8 @@ void sso_destroy(sso_engine* e) {
                   e->law, e->en, e->cx, e->cy, e->cz, e->area, e->coef, e->tOn, e->mkx, e->mky, e->mkz, e->mkWhen, e->vol0,
                   e->level0, e->cxs0, e->cys0, e->czs0, e->incStart, e->incCount, e->incConn, e->sea, e->incSide, e->vol,
                   e->level, e->wcx, e->wcy, e->wcz, e->areaN, e->zminN, e->zmaxN, e->hEff, e->aEff, e->acc, e->excess, e->q,
-                  e->dV, e->over, e->deg, e->merged, e->passes, e->evT, e->evId, e->evKind, e->overT, e->markT};
+                  e->dV, e->over, e->deg, e->merged, e->passes, e->evT, e->evId, e->evKind, e->overT, e->markT,
+                  e->passSlot};
   for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; ++i) free(bufs[i]);
   free(e);
 }
@@ -785,3 +804,20 @@ int sso_foundered(const sso_engine* e, double* founderT) {
 void sso_counters_get(const sso_engine* e, sso_counters* c) { *c = e->cnt; }
 
 void sso_flows(const sso_engine* e, double* q) { memcpy(q, e->q, (size_t)e->nc * sizeof(double)); }
+
+void sso_set_hooks(sso_engine* e, sso_pass_hook pass, sso_solved_hook solved, void* user) {
+  e->passHook = pass;
+  e->solvedHook = solved;
+  e->hookUser = user;
+}
+
+void sso_solved_state(const sso_engine* e, double* volS, double* levelS, double* areaS, double* cxS, double* cyS, double* czS, double* zmaxS,
+                      int32_t* merged, double* pose14, double* buoy4) {
+  for (int32_t n = 0; n < e->nn; ++n) {
+    volS[n] = e->vol[n]; levelS[n] = e->level[n]; areaS[n] = e->areaN[n];
+    cxS[n] = e->wcx[n]; cyS[n] = e->wcy[n]; czS[n] = e->wcz[n]; zmaxS[n] = e->zmaxN[n];
+  }
+  for (int32_t g = 0; g < e->ng; ++g) merged[g] = e->merged[g];
+  memcpy(pose14, e->lastPose, sizeof e->lastPose);
+  memcpy(buoy4, e->lastBuoy, sizeof e->lastBuoy);
+}

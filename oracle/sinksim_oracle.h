@@ -86,6 +86,16 @@ void sso_counters_get(const sso_engine* e, sso_counters* c);
 /* Last step's flow per connection. */
 void sso_flows(const sso_engine* e, double* q);
 
+/* Hooks for the adjoint's test harness: pass(user, node, k, rec) after the k-th node pass of a node in a step's level
+ * solve, rec = (level, vol, dv, mx, my, mz, zmin, zmax); solved(user) once the step's levels are solved, when
+ * sso_solved_state reads the solved volumes, levels, areas, centroids, extent tops, merge flags, the step's pose
+ * (R00 .. R22, tx, ty, tz, cth, 1 / R22) and buoyancy (V, x, y, z). */
+typedef void (*sso_pass_hook)(void* user, int32_t node, int32_t k, const double* rec);
+typedef void (*sso_solved_hook)(void* user);
+void sso_set_hooks(sso_engine* e, sso_pass_hook pass, sso_solved_hook solved, void* user);
+void sso_solved_state(const sso_engine* e, double* volS, double* levelS, double* areaS, double* cxS, double* cyS, double* czS, double* zmaxS,
+                      int32_t* merged, double* pose14, double* buoy4);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,7 +13,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Batch", "SinksimError", "available", "device_info", "run_sweep", "compare_results", "portable_math", "library_path",
+__all__ = ["Batch", "Adjoint", "SinksimError", "available", "device_info", "run_sweep", "compare_results", "portable_math", "library_path",
            "STOP_REASONS", "NUMERICS"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -103,6 +103,15 @@ _SIGNATURES = {
     "ssb_measure_add_mul_peak": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     "ssb_batch_run_noalloc": (C.c_int, [C.c_void_p, C.c_int32] + [C.c_void_p] * 13),
     "ssb_fnv1a64": (C.c_uint64, [C.c_uint64, C.c_void_p, C.c_size_t]),
+    "ssb_adjoint_create": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int32, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "ssb_adjoint_destroy": (None, [C.c_void_p]),
+    "ssb_adjoint_set_connection_enabled": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
+    "ssb_adjoint_set_connection_areas": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
+    "ssb_adjoint_set_objective": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ssb_adjoint_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_float)]),
+    "ssb_adjoint_samples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ssb_adjoint_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint64),
+                                   C.POINTER(C.c_uint64)]),
     "ssb_launch_plan": (C.c_int, [C.POINTER(_Options), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
 }
 
@@ -386,6 +395,79 @@ class Batch:
         once the work is queued on `stream` (a cudaStream_t as int, or None for the default stream)."""
         _check(lib().ssb_batch_run_noalloc(self._h, count, en, area, t_on, state, vol, level, cx, cy, cz, final_readouts, steps, stop_reason,
                                            stream))
+
+
+class Adjoint:
+    """Objective and gradient of a trajectory misfit for many instances of one compiled model, by the engine's discrete
+    adjoint (FP64, checkpoints every `checkpoint_every` steps, see include/sinksim_b200.h, ssb_adjoint_*).
+
+    Instance i runs from the compiled initial state until t_max or its founder; its objective is
+    sum_k (trim_k - trim_target[i, k])^2 + (heave_k - heave_target[i, k])^2 at the sample times, and run() returns it
+    with its gradient with respect to every connection area."""
+
+    def __init__(self, ship_path, sim_path, count=1, t_max=7920.0, checkpoint_every=256, team_warps=0, device=0):
+        h = C.c_void_p()
+        _check(lib().ssb_adjoint_create(_b(ship_path), _b(sim_path), count, float(t_max), checkpoint_every, team_warps, device, C.byref(h)))
+        self._h = h
+        self.count = count
+        nc = C.c_int32()
+        _check(lib().ssb_adjoint_info(self._h, C.byref(nc), None, None, None, None))
+        self.connections = nc.value
+        self.nsamples = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ssb_adjoint_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_connection_enabled(self, instance, connection, enabled):
+        _check(lib().ssb_adjoint_set_connection_enabled(self._h, instance, connection, 1 if enabled else 0))
+
+    def set_connection_areas(self, first, connections, areas):
+        conns = np.ascontiguousarray(connections, dtype=np.int32)
+        a = np.ascontiguousarray(areas, dtype=np.float64)
+        if a.ndim != 2 or a.shape[1] != conns.size:
+            raise SinksimError(-1, f"areas must be [count, {conns.size}], got {list(a.shape)}")
+        _check(lib().ssb_adjoint_set_connection_areas(self._h, int(first), a.shape[0], conns.size, conns.ctypes.data, a.ctypes.data))
+
+    def set_objective(self, times, trim_target, heave_target):
+        t = np.ascontiguousarray(times, dtype=np.float64)
+        tr = np.ascontiguousarray(np.broadcast_to(np.asarray(trim_target, dtype=np.float64), (self.count, t.size)))
+        hv = np.ascontiguousarray(np.broadcast_to(np.asarray(heave_target, dtype=np.float64), (self.count, t.size)))
+        _check(lib().ssb_adjoint_set_objective(self._h, t.size, t.ctypes.data, tr.ctypes.data, hv.ctypes.data))
+        self.nsamples = t.size
+
+    def run(self):
+        """(J [count], grad [count, connections], steps [count], error [count], device ms)."""
+        J = np.empty(self.count)
+        g = np.empty((self.count, self.connections))
+        steps = np.empty(self.count, dtype=np.int64)
+        err = np.empty(self.count, dtype=np.int32)
+        ms = C.c_float()
+        _check(lib().ssb_adjoint_run(self._h, J.ctypes.data, g.ctypes.data, steps.ctypes.data, err.ctypes.data, C.byref(ms)))
+        return J, g, steps, err, ms.value
+
+    def samples(self):
+        """The last run's (trim, heave) at the sample times, [count, n] each."""
+        tr = np.empty((self.count, self.nsamples))
+        hv = np.empty((self.count, self.nsamples))
+        _check(lib().ssb_adjoint_samples(self._h, tr.ctypes.data, hv.ctypes.data))
+        return tr, hv
+
+    def info(self):
+        nc, w, t = C.c_int32(), C.c_int32(), C.c_int32()
+        up, down = C.c_uint64(), C.c_uint64()
+        _check(lib().ssb_adjoint_info(self._h, C.byref(nc), C.byref(w), C.byref(t), C.byref(up), C.byref(down)))
+        return dict(connections=nc.value, team_warps=w.value, teams=t.value, h2d_bytes=up.value, d2h_bytes=down.value)
 
 
 def run_sweep(ship_path, sim_path, sweep_path, numerics="portable32", results_path=None):

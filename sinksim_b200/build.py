@@ -1,6 +1,7 @@
 """Builds the native parts of sinksim_b200 in the source tree.
 
-  libsinksim_b200.so      the engine: sm_100a kernels, the C++ host and the C ABI of include/sinksim_b200.h
+  libsinksim_b200.so      the engine: sm_100a kernels (the batch and its adjoint), the C++ host and the C ABI of
+                          include/sinksim_b200.h
   bin/sinksim_cuda_run    drop-in for the reference's GPU batch runner (apps/sinksim_cuda_run.cpp)
   bin/sinksim_sweep       drop-in for the reference's sweep runner (apps/sinksim_sweep.cpp), on the GPU
 
@@ -29,7 +30,8 @@ HOST_FLAGS = "-fPIC,-ffp-contract=off,-fno-fast-math,-fexcess-precision=standard
 NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-fmad=false", "-lineinfo", "-Xptxas", "-v", "-diag-suppress", "222",
                      "-Xcompiler", HOST_FLAGS, "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 
-SOURCES = ["batch_kernel.cu", "portable_math.cu", "probes.cu", "batch.cpp", "model.cpp", "json.cpp", "sweep.cpp", "capi.cpp"]
+SOURCES = ["batch_kernel.cu", "adjoint_kernel.cu", "portable_math.cu", "probes.cu", "batch.cpp", "adjoint.cpp", "model.cpp", "json.cpp",
+           "sweep.cpp", "capi.cpp"]
 APPS = ["sinksim_cuda_run", "sinksim_sweep"]
 
 

@@ -1,0 +1,358 @@
+// The adjoint kernel: the gradient of a trajectory objective with respect to every connection area, for a batch of
+// instances, by a hand-written discrete adjoint of the time step with checkpoints (no counterpart in the reference,
+// which has no gradients: docs/adr/0001-single-source-cpp-kernel.md:25-26).
+//
+// A persistent grid of teams (W warps each, one instance at a time from a work queue), per instance:
+//   1. forward: the instance runs from its initial state to tMax or its founder, exactly as the batch kernel steps it
+//      (the same team_step, so the same bits), keeping the state every K steps (a checkpoint: t, pose, rates and every
+//      node's volume, level and centroid, FP64) and the objective's readouts at the sample times;
+//   2. reverse: segment by segment, last first, the team restores the segment's checkpoint, recomputes its K steps with
+//      the tape hooks on (every node pass of the level solve, the solved levels, pose and buoyancy go to the team's
+//      tape in global memory), then runs the reverse of each step, last first (adjoint_step.cuh), adding the
+//      objective's adjoint at the sample states.
+// Memory per team: the checkpoints of one run and the tape of one segment; the adjoint of the state lives in shared
+// memory. Recomputing between checkpoints costs one more forward pass; the reverse sweep costs about one more.
+//
+// The objective: J = sum_k (trim(s_k) - trim*_k)^2 + (heave(s_k) - heave*_k)^2, trim in degrees and heave the mean of
+// the forward and aft drafts, where s_k is the state at which a readout curve recorded every sample time would take its
+// record (the first step start with t >= t_k; the final state for a run that stopped before t_k).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+
+#include "adjoint_kernel.h"
+#include "adjoint_step.cuh"
+#include "warp_step.cuh"
+
+namespace ssb {
+
+namespace {
+
+using adj::AdjPose;
+using adj::PoseD;
+
+template <int W>
+struct AdjTeam {
+  int rank, size, warp, nwarps, lane, width, bar;
+  __device__ __forceinline__ void sync() const {
+    if constexpr (W == 1) __syncwarp();
+    else asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(W * 32) : "memory");
+  }
+  __device__ __forceinline__ void add_int(int* p, int v) const { atomicAdd(p, v); }
+  // team-wide sums of K values (K <= 16), every thread receives them
+  __device__ __forceinline__ void reduce(double* v, int K, double* red) const {
+    for (int k = 0; k < K; ++k) {
+      double x = v[k];
+      for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+      if (lane == 0) red[warp * 16 + k] = x;
+    }
+    sync();
+    for (int k = 0; k < K; ++k) {
+      double s = 0;
+      for (int w = 0; w < nwarps; ++w) s += red[w * 16 + k];
+      v[k] = s;
+    }
+    sync();
+  }
+};
+
+// The tape hooks of the forward step (NoTape's counterpart): one lane of a level lane group writes each node pass, the
+// team writes the solved state, the pose and the buoyancy result.
+struct GpuTape {
+  adj::Tape t;
+  __device__ __forceinline__ void pass(int n, int k, double h, const PassR& p, const LevelLanes& L) const {
+    if (L.sub != 0) return;
+    if (k < adj::kMaxPasses) {
+      double* r = t.pass(n, k);
+      r[0] = h; r[1] = p.vol; r[2] = p.dv; r[3] = p.mx; r[4] = p.my; r[5] = p.mz; r[6] = p.zmin; r[7] = p.zmax;
+    }
+    t.i[t.L.npass + n] = k + 1;
+  }
+  template <int W>
+  __device__ __forceinline__ void solved(const DevModel& M, const Slot& S, const Team<W>& T) const {
+    const adj::TapeLayout& L = t.L;
+    for (int n = T.rank; n < M.nn; n += 32 * W) {
+      t.d[L.volS + n] = S.vol[n]; t.d[L.levelS + n] = S.level[n]; t.d[L.areaS + n] = S.area[n];
+      t.d[L.cxS + n] = S.cx[n]; t.d[L.cyS + n] = S.cy[n]; t.d[L.czS + n] = S.cz[n]; t.d[L.zmaxS + n] = S.zmax[n];
+    }
+    for (int g = T.rank; g < M.ng; g += 32 * W) t.i[L.merged + g] = S.merged[g];
+    if (T.leader()) {
+      const Pose& F = *S.pose;
+      const double p[14] = {F.R00, F.R01, F.R02, F.R10, F.R11, F.R12, F.R20, F.R21, F.R22, F.tx, F.ty, F.tz, F.cth, F.iR};
+      for (int k = 0; k < 14; ++k) t.d[L.pose + k] = p[k];
+      const Buoy& b = *S.buoy;
+      t.d[L.buoy] = b.V; t.d[L.buoy + 1] = b.x; t.d[L.buoy + 2] = b.y; t.d[L.buoy + 3] = b.z;
+    }
+  }
+};
+
+// Instance fields for team_step: the connection fields of the instance; events go nowhere (the adjoint runs keep no
+// event log: the founder flag, which ends a run, is kept in registers by team_step itself).
+struct AdjInst {
+  const std::uint8_t* en_;
+  const double *area_, *tOn_;
+  double* sink;  // per team: evCap + nmon + nmark doubles that absorb the event bookkeeping
+  std::int32_t* isink;
+  int nmon;
+  __device__ __forceinline__ const std::uint8_t* en() const { return en_; }
+  __device__ __forceinline__ const double* area() const { return area_; }
+  __device__ __forceinline__ const double* tOn() const { return tOn_; }
+  __device__ __forceinline__ double* evT() const { return sink; }
+  __device__ __forceinline__ std::int32_t* evId() const { return isink; }
+  __device__ __forceinline__ std::int32_t* evKind() const { return isink; }
+  __device__ __forceinline__ double* overT() const { return sink; }
+  __device__ __forceinline__ double* markT() const { return sink + nmon; }
+};
+
+// Per-team shared memory: the forward slot, then the reverse's arrays.
+struct AdjSmem {
+  adj::RevSlot rs;
+  adj::AdjState as;
+  double* grad;      // [nc]
+  double* sampleS;   // [nsamples] state index of each sample (as doubles)
+};
+
+__device__ __forceinline__ AdjSmem carve_adjoint(unsigned char* base, const AdjLayout& A) {
+  AdjSmem m;
+  auto d = [&](std::uint32_t off) { return reinterpret_cast<double*>(base + off); };
+  m.rs.hEff = d(A.hEff); m.rs.aEff = d(A.aEff); m.rs.dV = d(A.dV); m.rs.volPost = d(A.volPost);
+  m.rs.deg = reinterpret_cast<int*>(base + A.deg);
+  m.rs.clip = reinterpret_cast<std::int32_t*>(base + A.clip);
+  m.rs.aVolPost = d(A.aVolPost); m.rs.aCxs = d(A.aCxs); m.rs.aCys = d(A.aCys); m.rs.aCzs = d(A.aCzs); m.rs.aVs = d(A.aVs);
+  m.rs.aAcc = d(A.aAcc); m.rs.aZmx = d(A.aZmx); m.rs.aLs = d(A.aLs); m.rs.aAs = d(A.aAs);
+  m.rs.faHA = d(A.faHA); m.rs.faHB = d(A.faHB); m.rs.faAA = d(A.faAA); m.rs.faAB = d(A.faAB);
+  m.rs.red = d(A.red);
+  m.as.aVol = d(A.aVol); m.as.aLevel = d(A.aLevel); m.as.aCx = d(A.aCx); m.as.aCy = d(A.aCy); m.as.aCz = d(A.aCz);
+  m.grad = d(A.grad);
+  m.sampleS = d(A.sampleS);
+  return m;
+}
+
+// A checkpoint: t, zO, pitch, roll, vz, wth, wph, then vol, level, cx, cy, cz per node.
+template <int W>
+__device__ __forceinline__ void save_state(double* c, const SimRegs& R, const Slot& S, int nn, const Team<W>& T) {
+  if (T.leader()) { c[0] = R.t; c[1] = R.zO; c[2] = R.pitch; c[3] = R.roll; c[4] = R.vz; c[5] = R.wth; c[6] = R.wph; }
+  for (int n = T.rank; n < nn; n += 32 * W) {
+    c[7 + n] = S.vol[n]; c[7 + nn + n] = S.level[n]; c[7 + 2 * nn + n] = S.cx[n]; c[7 + 3 * nn + n] = S.cy[n]; c[7 + 4 * nn + n] = S.cz[n];
+  }
+}
+
+// Loads a state into the team's registers and slot, with the step's scratch cleared (as the batch kernel does when it
+// claims an instance).
+template <int W>
+__device__ __forceinline__ void load_state(const double* c, SimRegs& R, Slot& S, const DevModel& M, const Team<W>& T) {
+  R.t = c[0]; R.zO = c[1]; R.pitch = c[2]; R.roll = c[3]; R.vz = c[4]; R.wth = c[5]; R.wph = c[6];
+  R.calm = 0; R.inflow = 0; R.Vb = 0; R.hullTop = 0; R.mw = 0; R.bx = 0; R.by = 0; R.bz = 0;
+  R.foundered = 0; R.founderT = -1;
+  R.evCount = M.evCap;  // no event is recorded
+  const int nn = M.nn;
+  for (int n = T.rank; n < nn; n += 32 * W) {
+    S.vol[n] = c[7 + n]; S.level[n] = c[7 + nn + n]; S.cx[n] = c[7 + 2 * nn + n]; S.cy[n] = c[7 + 3 * nn + n]; S.cz[n] = c[7 + 4 * nn + n];
+    S.area[n] = 0; S.zmax[n] = 0; S.hEff[n] = 0; S.aEff[n] = 0; S.acc[n] = 0; S.deg[n] = 0;
+  }
+  for (int g = T.rank; g < M.ng; g += 32 * W) S.merged[g] = 0;
+  for (int c2 = T.rank; c2 < M.nc; c2 += 32 * W) { S.dV[c2] = 0; S.q[c2] = 0; }
+  T.sync();
+}
+
+// The objective's adjoint at the state with scalars (zO, pitch, roll): every thread adds the same values.
+__device__ __forceinline__ void add_sample_adjoint(const DevModel& M, double zO, double th, double ph, double aTrim, double aHeave, double* aSc) {
+  const PoseD F = adj::pose_of(M, zO, th, ph);
+  AdjPose aP;
+  adj::zero(aP);
+  adj::trim_heave_reverse(M, aTrim, aHeave, aP, aSc[1]);
+  adj::pose_reverse(M, F, aP, aSc[0], aSc[1], aSc[2]);
+}
+
+template <int W>
+__global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, SlotLayout SL, AdjLayout AL) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int team = blockIdx.x;
+  Team<W> T;
+  T.warp = threadIdx.x >> 5;
+  T.lane = threadIdx.x & 31;
+  T.rank = threadIdx.x;
+  T.bar = 1;
+  AdjTeam<W> AT{T.rank, 32 * W, T.warp, W, T.lane, 32, 1};
+  Slot S = carve_slot(smem, SL);
+  AdjSmem A = carve_adjoint(smem + SL.bytes, AL);
+  const adj::TapeLayout TL = adj::tape_layout(M.nn, M.ng);
+  const std::size_t recSize = 7 + 5 * static_cast<std::size_t>(M.nn);
+  double* const ckpt = B.ckpt + static_cast<std::size_t>(team) * B.maxCkpt * recSize;
+  unsigned char* const tapes = B.tape + static_cast<std::size_t>(team) * B.K * TL.bytes;
+  double* const sink = B.sink + static_cast<std::size_t>(team) * (M.evCap + M.nmon + M.nmark + 1);
+  std::int32_t* const isink = B.isink + static_cast<std::size_t>(team) * (M.evCap + 1);
+  const int NS = B.nsamples;
+  for (;;) {
+    if (T.leader()) S.misc[0] = atomicAdd(B.queue, 1);
+    T.sync();
+    const int inst = S.misc[0];
+    T.sync();
+    if (inst >= B.count) return;
+    const std::size_t ic = static_cast<std::size_t>(inst) * M.nc;
+    const AdjInst I{B.en + ic, B.area + ic, B.tOn + ic, sink, isink, M.nmon};
+    // the event bookkeeping sinks: overflow and mark times set (nothing fires), so events never write
+    for (int k = T.rank; k < M.nmon + M.nmark + 1; k += 32 * W) sink[k] = 1.0;
+    SimRegs R;
+    {
+      // the instance's initial state
+      const std::size_t in = static_cast<std::size_t>(inst) * M.nn;
+      double* c = ckpt;  // checkpoint 0 is the initial state
+      if (T.leader())
+        for (int k = 0; k < 7; ++k) c[k] = B.st0[static_cast<std::size_t>(inst) * 7 + k];
+      for (int n = T.rank; n < M.nn; n += 32 * W) {
+        c[7 + n] = B.vol0[in + n]; c[7 + M.nn + n] = B.level0[in + n];
+        c[7 + 2 * M.nn + n] = B.cx0[in + n]; c[7 + 3 * M.nn + n] = B.cy0[in + n]; c[7 + 4 * M.nn + n] = B.cz0[in + n];
+      }
+      __threadfence_block();
+      T.sync();
+      load_state(c, R, S, M, T);
+    }
+    // ---- 1. forward with checkpoints and the objective's samples
+    Pose& F = *S.pose;
+    F = make_pose(M, R.zO, R.pitch, R.roll);
+    const double* trimT = B.trimT + static_cast<std::size_t>(inst) * NS;
+    const double* heaveT = B.heaveT + static_cast<std::size_t>(inst) * NS;
+    double J = 0;
+    int k = 0;
+    long long s = 0;
+    for (;; ++s) {
+      if (s % B.K == 0 && s > 0) {
+        save_state(ckpt + static_cast<std::size_t>(s / B.K) * recSize, R, S, M.nn, T);
+        T.sync();
+      }
+      if (R.foundered || R.t >= B.tMax || s >= B.maxSteps) break;
+      while (k < NS && R.t >= B.sampleT[k]) {
+        double tr, hv;
+        adj::trim_heave(M, PoseD{F.R00, F.R01, F.R02, F.R10, F.R11, F.R12, F.R20, F.R21, F.R22, F.tx, F.ty, F.tz, F.cth, F.iR}, R.pitch, tr, hv);
+        J += (tr - trimT[k]) * (tr - trimT[k]) + (hv - heaveT[k]) * (hv - heaveT[k]);
+        if (T.leader()) {
+          B.trim[static_cast<std::size_t>(inst) * NS + k] = tr; B.heave[static_cast<std::size_t>(inst) * NS + k] = hv;
+          A.sampleS[k] = static_cast<double>(s);
+        }
+        ++k;
+      }
+      team_step<false, W>(M, F, R, S, I, T);
+      F = make_pose(M, R.zO, R.pitch, R.roll);
+    }
+    const long long S_end = s;
+    const double zE = R.zO, thE = R.pitch, phE = R.roll;
+    for (; k < NS; ++k) {
+      double tr, hv;
+      adj::trim_heave(M, PoseD{F.R00, F.R01, F.R02, F.R10, F.R11, F.R12, F.R20, F.R21, F.R22, F.tx, F.ty, F.tz, F.cth, F.iR}, R.pitch, tr, hv);
+      J += (tr - trimT[k]) * (tr - trimT[k]) + (hv - heaveT[k]) * (hv - heaveT[k]);
+      if (T.leader()) {
+        B.trim[static_cast<std::size_t>(inst) * NS + k] = tr; B.heave[static_cast<std::size_t>(inst) * NS + k] = hv;
+        A.sampleS[k] = static_cast<double>(S_end);
+      }
+    }
+    __threadfence_block();
+    T.sync();
+    // ---- 2. reverse
+    double aSc[6] = {0, 0, 0, 0, 0, 0};
+    for (int n = T.rank; n < M.nn; n += 32 * W) { A.as.aVol[n] = 0; A.as.aLevel[n] = 0; A.as.aCx[n] = 0; A.as.aCy[n] = 0; A.as.aCz[n] = 0; }
+    for (int c = T.rank; c < M.nc; c += 32 * W) A.grad[c] = 0;
+    T.sync();
+    // the samples at the final state (the objective's values of the trim and heave, recomputed from the outputs)
+    for (int q = 0; q < NS; ++q)
+      if (static_cast<long long>(A.sampleS[q]) == S_end) {
+        const double tr = B.trim[static_cast<std::size_t>(inst) * NS + q], hv = B.heave[static_cast<std::size_t>(inst) * NS + q];
+        add_sample_adjoint(M, zE, thE, phE, 2 * (tr - trimT[q]), 2 * (hv - heaveT[q]), aSc);
+      }
+    int err = 0;
+    const long long nseg = (S_end + B.K - 1) / B.K;
+    for (long long g = nseg - 1; g >= 0; --g) {
+      const long long s0 = g * B.K, s1 = (s0 + B.K < S_end) ? s0 + B.K : S_end;
+      load_state(ckpt + static_cast<std::size_t>(g) * recSize, R, S, M, T);
+      F = make_pose(M, R.zO, R.pitch, R.roll);
+      for (long long st = s0; st < s1; ++st) {
+        const adj::Tape tp = adj::tape_at(tapes + static_cast<std::size_t>(st - s0) * TL.bytes, TL);
+        if (T.leader()) { tp.d[TL.scal] = R.t; tp.d[TL.scal + 1] = R.zO; tp.d[TL.scal + 2] = R.pitch; tp.d[TL.scal + 3] = R.roll;
+                          tp.d[TL.scal + 4] = R.vz; tp.d[TL.scal + 5] = R.wth; tp.d[TL.scal + 6] = R.wph; }
+        for (int n = T.rank; n < M.nn; n += 32 * W) {
+          tp.d[TL.volIn + n] = S.vol[n]; tp.d[TL.levelIn + n] = S.level[n];
+          tp.d[TL.cxIn + n] = S.cx[n]; tp.d[TL.cyIn + n] = S.cy[n]; tp.d[TL.czIn + n] = S.cz[n];
+          tp.i[TL.npass + n] = 0;
+        }
+        T.sync();
+        team_step<false, W>(M, F, R, S, I, T, GpuTape{tp});
+        F = make_pose(M, R.zO, R.pitch, R.roll);
+      }
+      __threadfence_block();
+      T.sync();
+      for (long long st = s1 - 1; st >= s0; --st) {
+        const adj::Tape tp = adj::tape_at(tapes + static_cast<std::size_t>(st - s0) * TL.bytes, TL);
+        adj::reverse_step(AT, M, tp, I.en(), I.area(), I.tOn(), A.rs, A.as, aSc, A.grad, &err);
+        for (int q = 0; q < NS; ++q)
+          if (static_cast<long long>(A.sampleS[q]) == st) {
+            const double tr = B.trim[static_cast<std::size_t>(inst) * NS + q], hv = B.heave[static_cast<std::size_t>(inst) * NS + q];
+            add_sample_adjoint(M, tp.d[TL.scal + 1], tp.d[TL.scal + 2], tp.d[TL.scal + 3], 2 * (tr - trimT[q]), 2 * (hv - heaveT[q]), aSc);
+          }
+      }
+    }
+    T.sync();
+    for (int c = T.rank; c < M.nc; c += 32 * W) B.grad[ic + c] = A.grad[c];
+    if (err) atomicOr(B.error + inst, err);
+    if (T.leader()) { B.J[inst] = J; B.steps[inst] = S_end; }
+    T.sync();
+  }
+}
+
+}  // namespace
+
+AdjLayout adjoint_layout(int nn, int nc, int nsamples, int W) {
+  AdjLayout A{};
+  std::uint32_t off = 0;
+  auto take16 = [&](std::size_t bytes) {
+    const std::uint32_t at = off;
+    off = static_cast<std::uint32_t>((off + bytes + 15) & ~static_cast<std::size_t>(15));
+    return at;
+  };
+  const std::size_t N = sizeof(double) * static_cast<std::size_t>(std::max(nn, 1));
+  const std::size_t C = sizeof(double) * static_cast<std::size_t>(std::max(nc, 1));
+  A.hEff = take16(N); A.aEff = take16(N); A.dV = take16(C); A.volPost = take16(N);
+  A.deg = take16(sizeof(int) * static_cast<std::size_t>(std::max(nn, 1)));
+  A.clip = take16(sizeof(std::int32_t) * static_cast<std::size_t>(std::max(nn, 1)));
+  A.aVolPost = take16(N); A.aCxs = take16(N); A.aCys = take16(N); A.aCzs = take16(N); A.aVs = take16(N); A.aAcc = take16(N);
+  A.aZmx = take16(N); A.aLs = take16(N); A.aAs = take16(N);
+  A.faHA = take16(C); A.faHB = take16(C); A.faAA = take16(C); A.faAB = take16(C);
+  A.red = take16(sizeof(double) * 16 * static_cast<std::size_t>(W));
+  A.aVol = take16(N); A.aLevel = take16(N); A.aCx = take16(N); A.aCy = take16(N); A.aCz = take16(N);
+  A.grad = take16(C);
+  A.sampleS = take16(sizeof(double) * static_cast<std::size_t>(std::max(nsamples, 1)));
+  A.bytes = off;
+  return A;
+}
+
+std::size_t adjoint_tape_bytes(int nn, int ng) { return adj::tape_layout(nn, ng).bytes; }
+
+cudaError_t configure_adjoint_kernel(int W, std::size_t smem) {
+  const int b = static_cast<int>(smem);
+  switch (W) {
+    case 4: return cudaFuncSetAttribute(adjoint_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    case 8: return cudaFuncSetAttribute(adjoint_batch<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t adjoint_occupancy(int W, std::size_t smem, int* blocksPerSM) {
+  switch (W) {
+    case 4: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSM, adjoint_batch<4>, 4 * 32, smem);
+    case 8: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSM, adjoint_batch<8>, 8 * 32, smem);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_adjoint_kernel(int W, const DevModel& M, const AdjRun& B, const SlotLayout& SL, const AdjLayout& AL, int teams,
+                                  cudaStream_t stream) {
+  const std::size_t smem = static_cast<std::size_t>(SL.bytes) + AL.bytes;
+  switch (W) {
+    case 4: adjoint_batch<4><<<teams, 4 * 32, smem, stream>>>(M, B, SL, AL); break;
+    case 8: adjoint_batch<8><<<teams, 8 * 32, smem, stream>>>(M, B, SL, AL); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace ssb

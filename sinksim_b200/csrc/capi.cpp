@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 
+#include "adjoint.h"
 #include "batch.h"
 #include "model.h"
 #include "sweep.h"
@@ -17,6 +18,11 @@ void portable_math_host(int op, const double* x, const double* y, double* out, s
 cudaError_t portable_math_device(int op, const double* x, const double* y, double* out, std::int64_t n);
 double measure_add_mul_peak(bool fp64, int device);
 }  // namespace ssb
+
+struct ssb_adjoint {
+  std::unique_ptr<ssb::AdjointBatch> adj;
+  std::int32_t nsamples = 0;
+};
 
 struct ssb_batch {
   std::shared_ptr<ssb::Batch> batch;
@@ -539,3 +545,85 @@ uint64_t ssb_fnv1a64(uint64_t state, const void* data, size_t n) {
 }
 
 }  // extern "C"
+
+int ssb_adjoint_create(const char* ship_path, const char* sim_path, int32_t count, double t_max, int32_t checkpoint_every, int32_t team_warps,
+                       int32_t device, ssb_adjoint** out) {
+  return guard([&] {
+    need(ship_path, "ship_path"); need(sim_path, "sim_path"); need(out, "out");
+    *out = nullptr;
+    ssb::AdjointOptions o;
+    o.count = count;
+    o.tMax = t_max;
+    o.checkpointEvery = checkpoint_every ? checkpoint_every : 256;
+    o.teamWarps = team_warps;
+    o.device = device;
+    if (count < 1) throw std::invalid_argument("count must be at least 1");
+    need_device();
+    auto ship = ssb::load_ship(ship_path);
+    const ssb::CompiledSim sim = ssb::load_sim(sim_path);
+    ssb::check_pairing(*ship, sim);
+    auto h = std::make_unique<ssb_adjoint>();
+    h->adj = std::make_unique<ssb::AdjointBatch>(ship, sim, o);
+    *out = h.release();
+  });
+}
+
+void ssb_adjoint_destroy(ssb_adjoint* a) { delete a; }
+
+int ssb_adjoint_set_connection_enabled(ssb_adjoint* a, int32_t instance, int32_t connection, int32_t enabled) {
+  return guard([&] { need(a, "adjoint"); a->adj->set_connection_enabled(instance, connection, enabled != 0); });
+}
+
+int ssb_adjoint_set_connection_areas(ssb_adjoint* a, int32_t first, int32_t count, int32_t n_connections, const int32_t* connections,
+                                     const double* areas) {
+  return guard([&] {
+    need(a, "adjoint");
+    if (count > 0 && n_connections > 0) { need(connections, "connections"); need(areas, "areas"); }
+    a->adj->set_connection_areas(first, count, n_connections, connections, areas);
+  });
+}
+
+int ssb_adjoint_set_objective(ssb_adjoint* a, int32_t n, const double* times, const double* trim, const double* heave) {
+  return guard([&] {
+    need(a, "adjoint"); need(times, "times"); need(trim, "trim"); need(heave, "heave");
+    a->adj->set_objective(n, times, trim, heave);
+    a->nsamples = n;
+  });
+}
+
+int ssb_adjoint_run(ssb_adjoint* a, double* J, double* grad, int64_t* steps, int32_t* error, float* device_ms) {
+  return guard([&] {
+    need(a, "adjoint");
+    const float ms = a->adj->run();
+    if (device_ms) *device_ms = ms;
+    const int32_t n = a->adj->count(), nc = a->adj->connections();
+    for (int32_t i = 0; i < n; ++i) {
+      if (J) J[i] = a->adj->objective(i);
+      if (grad) std::memcpy(grad + static_cast<std::size_t>(i) * nc, a->adj->gradient(i), sizeof(double) * nc);
+      if (steps) steps[i] = a->adj->steps(i);
+      if (error) error[i] = a->adj->error(i);
+    }
+  });
+}
+
+int ssb_adjoint_samples(const ssb_adjoint* a, double* trim, double* heave) {
+  return guard([&] {
+    need(a, "adjoint");
+    const int32_t n = a->adj->count(), k = a->nsamples;
+    for (int32_t i = 0; i < n; ++i) {
+      if (trim) std::memcpy(trim + static_cast<std::size_t>(i) * k, a->adj->samples_trim(i), sizeof(double) * k);
+      if (heave) std::memcpy(heave + static_cast<std::size_t>(i) * k, a->adj->samples_heave(i), sizeof(double) * k);
+    }
+  });
+}
+
+int ssb_adjoint_info(const ssb_adjoint* a, int32_t* connections, int32_t* team_warps, int32_t* teams, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {
+  return guard([&] {
+    need(a, "adjoint");
+    if (connections) *connections = a->adj->connections();
+    if (team_warps) *team_warps = a->adj->team_warps();
+    if (teams) *teams = a->adj->teams();
+    if (h2d_bytes) *h2d_bytes = a->adj->upload_bytes();
+    if (d2h_bytes) *d2h_bytes = a->adj->download_bytes();
+  });
+}

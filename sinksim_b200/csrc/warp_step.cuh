@@ -22,32 +22,12 @@
 
 #include "device_model.h"
 #include "portable_math.cuh"
+#include "scheme.h"
 
 namespace ssb {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kLanes = 32;
-
-// Scheme v1 constants (engine/include/sinksim/kernel/scheme.hpp:11-28).
-constexpr double kEmptyVolume = 1e-6;
-constexpr double kFullFraction = 1.0 - 1e-7;
-constexpr double kLimiterShare = 0.5;
-constexpr double kOrificeHeadFloor = 0.01;
-constexpr double kWeirCoefficient = 2.0 / 3.0;
-constexpr double kWeirExponent = 1.5;
-constexpr double kVillemonteExponent = 0.385;
-constexpr int kNewtonFast = 6;
-constexpr double kSlopeMin = 1e-9;
-constexpr double kCentroidMinVolume = 1e-9;
-constexpr double kNoHead = -1e9;
-constexpr double kNoHeadTest = -1e8;
-constexpr double kPitchClamp = 1.35;
-constexpr double kRollClamp = 1.4;
-constexpr double kPi = 3.141592653589793;
-
-// JavaScript Math.max / Math.min: the first argument wins ties (kernel/math.hpp:29-30).
-__device__ __forceinline__ double jmax(double a, double b) { return (b > a) ? b : a; }
-__device__ __forceinline__ double jmin(double a, double b) { return (b < a) ? b : a; }
 
 __device__ __forceinline__ Pose make_pose(const DevModel& M, double zO, double th, double ph) {
   const double cth = pm::cos(th), sth = pm::sin(th), cph = pm::cos(ph), sph = pm::sin(ph);
@@ -389,17 +369,27 @@ __device__ __forceinline__ void set_centroid(Slot& S, int n, const PassR& p) {
 
 enum SolveStage { kStageFirst, kStageFull, kStageNewton };
 
+// Where a step's forward computation records what its reverse (the adjoint, adjoint_kernel.cu) needs: every node pass of
+// the level solve (node, pass number within the node's solve, level, result) and the solved levels. The batch kernels
+// pass NoTape, whose hooks are empty and compile away.
+struct NoTape {
+  __device__ __forceinline__ void pass(int, int, double, const PassR&, const LevelLanes&) const {}
+  template <int W>
+  __device__ __forceinline__ void solved(const DevModel&, const Slot&, const Team<W>&) const {}
+};
+
 // One node (levels.hpp:13-49).
-template <bool MIXED>
-__device__ __forceinline__ void solve_single(const DevModel& M, const Pose& F, Slot& S, int n, const LevelLanes& L) {
+template <bool MIXED, class Tape>
+__device__ __forceinline__ void solve_single(const DevModel& M, const Pose& F, Slot& S, int n, const LevelLanes& L, const Tape& tape) {
   const double V = S.vol[n], Vmax = __ldg(M.vmax + n);
   const double tol = jmax(1e-3 * Vmax, 0.5);
   double h = S.level[n];
   double hi = 0, a = 0, b = 0;
-  int stage = kStageFirst, it = 0;
+  int stage = kStageFirst, it = 0, slot = 0;
   PassR p;
   for (;;) {
     p = node_pass<MIXED>(M, F, n, h, L);
+    tape.pass(n, slot++, h, p, L);
     if (stage == kStageFirst) {
       const double lo = p.zmin;
       hi = p.zmax;
@@ -431,8 +421,9 @@ __device__ __forceinline__ void solve_single(const DevModel& M, const Pose& F, S
 }
 
 // A merged group of N nodes at one common level (levels.hpp:54-162); P holds the members' passes.
-template <bool MIXED>
-__device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Slot& S, PassR* P, const int* m, int N, const LevelLanes& L) {
+template <bool MIXED, class Tape>
+__device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Slot& S, PassR* P, const int* m, int N, const LevelLanes& L,
+                                            const Tape& tape) {
   double V = 0, Vmax = 0;
   for (int k = 0; k < N; ++k) { V += S.vol[__ldg(m + k)]; Vmax += __ldg(M.vmax + __ldg(m + k)); }
   bool allWet = true;
@@ -451,9 +442,13 @@ __device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Sl
   }
   const double tol = jmax(1e-3 * Vmax, 0.5);
   double hi = 0, a = 0, b = 0, dh = 0;
-  int stage = kStageFirst, it = 0;
+  int stage = kStageFirst, it = 0, slot = 0;
   for (;;) {
-    for (int k = 0; k < N; ++k) P[k] = node_pass<MIXED>(M, F, __ldg(m + k), h, L);
+    for (int k = 0; k < N; ++k) {
+      P[k] = node_pass<MIXED>(M, F, __ldg(m + k), h, L);
+      tape.pass(__ldg(m + k), slot, h, P[k], L);
+    }
+    ++slot;
     if (stage == kStageFirst) {
       for (int k = 0; k < N; ++k) S.zmax[__ldg(m + k)] = P[k].zmax;
       double lo = P[0].zmin;
@@ -549,8 +544,8 @@ __device__ __forceinline__ void solve_group(const DevModel& M, const Pose& F, Sl
 // Groups are independent (a group's solve reads and writes only its members), so the team's level lane groups take
 // them in turn: lane group u of the team (32 / kLevelLanes<MIXED> per warp) solves groups u, u + 32 W / kLevelLanes, ...
 // (the reference's block gave them to its eight warps, device_step.cuh:270-281).
-template <bool MIXED, int W>
-__device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, Slot& S, const Team<W>& T) {
+template <bool MIXED, int W, class Tape>
+__device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, Slot& S, const Team<W>& T, const Tape& tape) {
   constexpr int LANES = kLevelLanes<MIXED>, PER_WARP = 32 / LANES;
   LevelLanes L;
   L.lane = T.lane;
@@ -578,8 +573,8 @@ __device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, S
       }
     }
     S.merged[g] = merged ? 1 : 0;
-    if (merged) solve_group<MIXED>(M, F, S, P, m, N, L);
-    else for (int k = 0; k < N; ++k) solve_single<MIXED>(M, F, S, __ldg(m + k), L);
+    if (merged) solve_group<MIXED>(M, F, S, P, m, N, L, tape);
+    else for (int k = 0; k < N; ++k) solve_single<MIXED>(M, F, S, __ldg(m + k), L, tape);
   }
   __syncwarp();  // the lane groups leave the loop after different numbers of groups
 }
@@ -716,15 +711,17 @@ __device__ __forceinline__ void push_event(const DevModel& M, SimRegs& R, const 
 // per-connection work is spread over all 32 W threads of the team; scalars are computed redundantly and identically
 // by every thread, so every decision is uniform across the team.
 
-template <bool MIXED, int W, class IP>
-__device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimRegs& R, Slot& S, const IP& I, const Team<W>& T) {
+template <bool MIXED, int W, class IP, class Tape = NoTape>
+__device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimRegs& R, Slot& S, const IP& I, const Team<W>& T,
+                                          const Tape& tape = Tape{}) {
   constexpr int kStride = 32 * W;
   const int lane = T.lane, rank = T.rank;
   const double tNow = R.t;
   park(S.parked, R);  // until the volume update; no thread reads it before the barrier that ends that phase
   *S.buoy = buoyancy<MIXED, W>(M, F, T, S.hydro);  // every thread stores the same values
-  solve_levels<MIXED, W>(M, F, S, T);
+  solve_levels<MIXED, W>(M, F, S, T, tape);
   T.sync();
+  tape.solved(M, S, T);
 
   // effective heads and areas, then degrees (flows.hpp:15-35)
   for (int n = rank; n < M.nn; n += kStride) {

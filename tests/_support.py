@@ -117,6 +117,24 @@ def oracle_lib():
     return _oracle_lib
 
 
+def _structs(ship, sim):
+    """The oracle's C structs over a compiled model's arrays (the oracles copy them when they are created)."""
+    S = _Ship(len(ship["x"]), len(ship["segCol"]), len(ship["mu"]),
+              *(_p(ship[k], C.c_double) for k in ("x", "y", "dxdy", "zlo", "zhi")), _p(ship["segCol"], C.c_int32),
+              *(_p(ship[k], C.c_double) for k in ("segA", "segE", "mu", "vmax", "amin", "aov")),
+              _p(ship["segStart"], C.c_int32), _p(ship["segCount"], C.c_int32))
+    m = sim
+    M = _Sim(m["rho"], m["g"], m["dt"], len(m["gCount"]), _p(m["gStart"], C.c_int32), _p(m["gCount"], C.c_int32),
+             _p(m["gNodes"], C.c_int32), _p(m["gMode"], C.c_uint8), _p(m["gpx"], C.c_double), _p(m["gpy"], C.c_double),
+             _p(m["gpz"], C.c_double), m["gMargin"], len(m["ca"]), _p(m["ca"], C.c_int32), _p(m["cb"], C.c_int32),
+             _p(m["law"], C.c_uint8), *(_p(m[k], C.c_double) for k in ("cx", "cy", "cz", "area", "coef")),
+             _p(m["en"], C.c_uint8), _p(m["tOn"], C.c_double), _p(m["skipGroup"], C.c_int32), _p(m["monitor"], C.c_int32),
+             m["nmon"], m["monThreshold"], len(m["mkx"]), *(_p(m[k], C.c_double) for k in ("mkx", "mky", "mkz")),
+             _p(m["mkWhen"], C.c_uint8), *m["founder"], (C.c_double * 16)(*m["body"]), m["xFP"], m["xAP"],
+             (C.c_double * 7)(*m["state0"]), *(_p(m[k], C.c_double) for k in ("vol0", "level0", "cx0", "cy0", "cz0")))
+    return S, M
+
+
 class Oracle:
     """The C restatement of the reference step (oracle/sinksim_oracle.c) on one compiled model."""
 
@@ -125,19 +143,7 @@ class Oracle:
         self.ship, self.sim = ship, sim
         self.nodes = len(ship["mu"])
         self.nconn = len(sim["ca"])
-        S = _Ship(len(ship["x"]), len(ship["segCol"]), self.nodes,
-                  *(_p(ship[k], C.c_double) for k in ("x", "y", "dxdy", "zlo", "zhi")), _p(ship["segCol"], C.c_int32),
-                  *(_p(ship[k], C.c_double) for k in ("segA", "segE", "mu", "vmax", "amin", "aov")),
-                  _p(ship["segStart"], C.c_int32), _p(ship["segCount"], C.c_int32))
-        m = sim
-        M = _Sim(m["rho"], m["g"], m["dt"], len(m["gCount"]), _p(m["gStart"], C.c_int32), _p(m["gCount"], C.c_int32),
-                 _p(m["gNodes"], C.c_int32), _p(m["gMode"], C.c_uint8), _p(m["gpx"], C.c_double), _p(m["gpy"], C.c_double),
-                 _p(m["gpz"], C.c_double), m["gMargin"], len(m["ca"]), _p(m["ca"], C.c_int32), _p(m["cb"], C.c_int32),
-                 _p(m["law"], C.c_uint8), *(_p(m[k], C.c_double) for k in ("cx", "cy", "cz", "area", "coef")),
-                 _p(m["en"], C.c_uint8), _p(m["tOn"], C.c_double), _p(m["skipGroup"], C.c_int32), _p(m["monitor"], C.c_int32),
-                 m["nmon"], m["monThreshold"], len(m["mkx"]), *(_p(m[k], C.c_double) for k in ("mkx", "mky", "mkz")),
-                 _p(m["mkWhen"], C.c_uint8), *m["founder"], (C.c_double * 16)(*m["body"]), m["xFP"], m["xAP"],
-                 (C.c_double * 7)(*m["state0"]), *(_p(m[k], C.c_double) for k in ("vol0", "level0", "cx0", "cy0", "cz0")))
+        S, M = _structs(ship, sim)
         self.h = self.lib.sso_create(C.byref(S), C.byref(M), 1 if mixed else 0)
 
     def __del__(self):
@@ -187,6 +193,128 @@ class Oracle:
         q = np.empty(self.nconn)
         self.lib.sso_flows(self.h, _p(q, C.c_double))
         return q
+
+
+# ----------------------------------------------------------------------------------------------- the tangent-linear step
+
+_tangent_lib = None
+TANGENT_PARAMS = 10
+
+
+def tangent_lib():
+    global _tangent_lib
+    if _tangent_lib is None:
+        lib = C.CDLL(os.path.join(REF_DIR, "libsinksim_tangent.so"))
+        lib.sst_create.restype = C.c_void_p
+        lib.sst_create.argtypes = [C.POINTER(_Ship), C.POINTER(_Sim)]
+        lib.sst_destroy.argtypes = [C.c_void_p]
+        lib.sst_set_connection.argtypes = [C.c_void_p, C.c_int32, C.c_int, C.c_double, C.c_double]
+        lib.sst_seed_area.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double]
+        lib.sst_step.argtypes = [C.c_void_p, C.c_int64]
+        lib.sst_get_record.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.sst_readouts.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.sst_foundered.argtypes = [C.c_void_p]
+        _tangent_lib = lib
+    return _tangent_lib
+
+
+class Tangent:
+    """The tangent-linear restatement (oracle/sinksim_tangent.cpp): the portable step over dual numbers carrying
+    derivatives with respect to up to 10 parameters that enter through connection areas."""
+
+    def __init__(self, ship, sim):
+        tl = tangent_lib()
+        self.nodes = len(ship["mu"])
+        self.nconn = len(sim["ca"])
+        S, M = _structs(ship, sim)
+        self.tl = tl
+        self.t = tl.sst_create(C.byref(S), C.byref(M))
+
+    def __del__(self):
+        if getattr(self, "t", None):
+            self.tl.sst_destroy(self.t)
+            self.t = None
+
+    def set_connection(self, c, enabled=-1, area=float("nan"), tOn=float("nan")):
+        self.tl.sst_set_connection(self.t, c, enabled, area, tOn)
+
+    def seed_area(self, c, p, g):
+        self.tl.sst_seed_area(self.t, c, p, g)
+
+    def step(self, n=1):
+        self.tl.sst_step(self.t, n)
+
+    def record(self, tangents=False):
+        r = np.empty(10 + 5 * self.nodes)
+        d = np.empty((TANGENT_PARAMS, r.size))
+        self.tl.sst_get_record(self.t, _p(r, C.c_double), _p(d, C.c_double))
+        return (r, d) if tangents else r
+
+    def readouts(self, tangents=False):
+        r = np.empty(7)
+        d = np.empty((TANGENT_PARAMS, 7))
+        self.tl.sst_readouts(self.t, _p(r, C.c_double), _p(d, C.c_double))
+        return (r, d) if tangents else r
+
+    def foundered(self):
+        return bool(self.tl.sst_foundered(self.t))
+
+
+# ----------------------------------------------------------------------------------------------- the adjoint on the host
+
+_adjoint_host_lib = None
+
+
+def adjoint_host_gradient(ship, sim, en, area, t_on, steps, sample_steps, trim_target, heave_target):
+    """The product's reverse step run on the CPU (oracle/adjoint_host.cpp) over the C restatement's tapes: the
+    trajectory objective sum_k (trim - trim_k)^2 + (heave - heave_k)^2 at the states after sample_steps[k] steps and its
+    gradient with respect to every connection area. Returns (J, grad, error bits)."""
+    global _adjoint_host_lib
+    if _adjoint_host_lib is None:
+        lib = C.CDLL(os.path.join(REF_DIR, "libsinksim_adjoint_host.so"))
+        lib.ssa_gradient.restype = C.c_int
+        lib.ssa_gradient.argtypes = [C.POINTER(_Ship), C.POINTER(_Sim), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]
+        _adjoint_host_lib = lib
+    S, M = _structs(ship, sim)
+    en = np.ascontiguousarray(en, dtype=np.uint8)
+    area = f64(area)
+    t_on = f64(t_on)
+    ss = np.ascontiguousarray(sample_steps, dtype=np.int64)
+    tt = f64(trim_target)
+    ht = f64(heave_target)
+    grad = np.zeros(len(sim["ca"]))
+    J = C.c_double()
+    err = _adjoint_host_lib.ssa_gradient(C.byref(S), C.byref(M), en.ctypes.data, area.ctypes.data, t_on.ctypes.data, int(steps), ss.size,
+                                         ss.ctypes.data, tt.ctypes.data, ht.ctypes.data, C.byref(J), grad.ctypes.data)
+    return J.value, grad, err
+
+
+def tangent_gradient(ship, sim, en, area, t_on, conns, steps, sample_steps, trim_target, heave_target):
+    """d J / d area[c] for the connections `conns` (at most 10) by the tangent-linear restatement, and J."""
+    t = Tangent(ship, sim)
+    for c in range(len(sim["ca"])):
+        t.set_connection(c, enabled=int(en[c]), area=float(area[c]), tOn=float(t_on[c]))
+    for p, c in enumerate(conns):
+        t.seed_area(int(c), p, 1.0)
+    order = np.argsort(sample_steps, kind="stable")
+    done, J = 0, 0.0
+    g = np.zeros(TANGENT_PARAMS)
+    vals = {}
+    for k in order:
+        s = min(int(sample_steps[k]), steps)
+        if s > done:
+            t.step(s - done)
+            done = s
+        r, d = t.readouts(tangents=True)
+        vals[k] = (r, d)
+    for k in range(len(sample_steps)):
+        r, d = vals[k]
+        trim, heave = r[1], 0.5 * (r[5] + r[6])
+        dtrim, dheave = d[:, 1], 0.5 * (d[:, 5] + d[:, 6])
+        J += (trim - trim_target[k]) ** 2 + (heave - heave_target[k]) ** 2
+        g += 2 * (trim - trim_target[k]) * dtrim + 2 * (heave - heave_target[k]) * dheave
+    return J, g[:len(conns)]
 
 
 # ----------------------------------------------------------------------------------------------- the reference engine
