@@ -1,357 +1,354 @@
-// Loading compiled ships and sims. The member names, the checks and the hash order follow the reference's loader
-// (engine/src/compiled.cpp:108-279) so that the same files load with the same verdicts: every numeric array is
-// re-hashed after parsing and a mismatch is an error, because it means a value did not survive the JSON round trip.
+// Loading compiled ships and sims ("sinksim.compiled-ship" / "sinksim.compiled-sim", the reference's docs/FORMATS.md).
+//
+// A compiled file is a set of named arrays ("columns.x", "connections.area", ...) plus a few scalars. Each loader here
+// is a declaration: a table of the arrays it reads, in the order the format hashes them, each with its element type,
+// the length it must have and, for integers, the range it must fall in. One generic reader walks the table: it reads
+// and checks every array, then re-hashes each one (FNV-1a over its little-endian bytes, -0 as 0) and the chain of all
+// of them, and refuses the file when any hash differs from the one the file states: a value that did not survive the
+// JSON round trip, or a hand-edited file. The hash order and the verdicts are the format's (the reference's loader,
+// engine/src/compiled.cpp:82-279, reads the same files with the same outcome); the table-driven reader is this
+// project's own.
 #include "model.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <numeric>
 #include <stdexcept>
 
 #include "json.h"
 
 namespace ssb {
 
-void Fnv1a64::f64(const double* v, std::size_t n) {
+// ----------------------------------------------------------------------------- FNV-1a
+
+namespace {
+template <class Word>
+void feed_words(Fnv1a64& h, const Word* v, std::size_t n) {
+  unsigned char b[sizeof(Word)];
   for (std::size_t i = 0; i < n; ++i) {
-    double d = v[i];
-    if (d == 0) d = 0.0;
-    std::uint64_t bits;
-    std::memcpy(&bits, &d, 8);
-    unsigned char b[8];
-    for (int k = 0; k < 8; ++k) b[k] = static_cast<unsigned char>((bits >> (8 * k)) & 0xffu);
-    update(b, 8);
+    Word w = v[i];
+    for (std::size_t k = 0; k < sizeof(Word); ++k) { b[k] = static_cast<unsigned char>(w & 0xffu); w >>= 8; }
+    h.update(b, sizeof(Word));
   }
+}
+}  // namespace
+
+void Fnv1a64::f64(const double* v, std::size_t n) {
+  std::vector<std::uint64_t> w(n);
+  for (std::size_t i = 0; i < n; ++i) {
+    const double d = v[i] == 0 ? 0.0 : v[i];  // -0 and +0 hash alike
+    std::memcpy(&w[i], &d, 8);
+  }
+  feed_words(*this, w.data(), n);
 }
 
 void Fnv1a64::i32(const std::int32_t* v, std::size_t n) {
-  for (std::size_t i = 0; i < n; ++i) {
-    std::uint32_t bits;
-    std::memcpy(&bits, &v[i], 4);
-    unsigned char b[4];
-    for (int k = 0; k < 4; ++k) b[k] = static_cast<unsigned char>((bits >> (8 * k)) & 0xffu);
-    update(b, 4);
-  }
+  std::vector<std::uint32_t> w(n);
+  std::memcpy(w.data(), v, n * 4);
+  feed_words(*this, w.data(), n);
 }
 
 std::string Fnv1a64::hex() const {
-  static const char* digits = "0123456789abcdef";
-  std::string s(16, '0');
-  for (int i = 15; i >= 0; --i) s[static_cast<std::size_t>(i)] = digits[(h_ >> (4 * (15 - i))) & 0xfu];
-  return s;
+  char buf[17];
+  for (int i = 0; i < 16; ++i) buf[i] = "0123456789abcdef"[(h_ >> (60 - 4 * i)) & 0xfu];
+  buf[16] = 0;
+  return buf;
 }
 
 std::int32_t CompiledSim::maxGroupSize() const {
-  std::int32_t m = 1;
-  for (const std::int32_t c : gNodeCount) if (c > m) m = c;
-  return m;
+  return gNodeCount.empty() ? 1 : std::max<std::int32_t>(1, *std::max_element(gNodeCount.begin(), gNodeCount.end()));
 }
 
 std::int32_t CompiledSim::kindIndex(const std::string& name) const {
-  for (std::size_t i = 0; i < kindNames.size(); ++i)
-    if (kindNames[i] == name) return static_cast<std::int32_t>(i);
-  return -1;
+  const auto it = std::find(kindNames.begin(), kindNames.end(), name);
+  return it == kindNames.end() ? -1 : static_cast<std::int32_t>(it - kindNames.begin());
 }
+
+// ----------------------------------------------------------------------------- the table-driven reader
 
 namespace {
 
 using json::Value;
 
-[[noreturn]] void bad(const std::string& file, const std::string& what) { throw std::runtime_error(file + ": " + what); }
-
-const Value& at(const Value& obj, const char* key, const std::string& file) { return json::member(obj, key, file); }
-
-std::vector<double> numbers(const Value& v, const std::string& file, const std::string& what) {
-  if (!v.is_array()) bad(file, what + " must be an array");
-  std::vector<double> out;
-  out.reserve(v.size());
-  std::size_t i = 0;
-  for (const Value& x : v.items()) {
-    if (!x.is_number()) bad(file, what + "[" + std::to_string(i) + "] is not a number");
-    out.push_back(x.as_double());
-    ++i;
+// A compiled document: the parsed JSON, its file name for the messages, and lookups by dotted path.
+class Document {
+ public:
+  Document(const std::string& file, const char* format) : file_(file), doc_(json::read_file(file)) {
+    if (json::string_or(doc_, "format", "") != format) fail(std::string("not a ") + format + " file");
+    const long long v = json::integer(doc_, "formatVersion", file_);
+    if (v != 1) fail("formatVersion " + std::to_string(v) + " cannot be read (this engine reads version 1)");
   }
-  return out;
-}
-
-std::vector<std::int32_t> indices(const Value& v, const std::string& file, const std::string& what, std::int64_t lo, std::int64_t hi) {
-  const std::vector<double> d = numbers(v, file, what);
-  std::vector<std::int32_t> out;
-  out.reserve(d.size());
-  for (std::size_t i = 0; i < d.size(); ++i) {
-    if (d[i] != std::floor(d[i]) || d[i] < static_cast<double>(lo) || d[i] > static_cast<double>(hi))
-      bad(file, what + "[" + std::to_string(i) + "] = " + json::format_number(d[i]) + " is not an integer in [" + std::to_string(lo) + ", " +
-                    std::to_string(hi) + "]");
-    out.push_back(static_cast<std::int32_t>(d[i]));
+  [[noreturn]] void fail(const std::string& why) const { throw std::runtime_error(file_ + ": " + why); }
+  const Value& at(const std::string& path) const {
+    const Value* v = find(path);
+    if (!v) fail("missing " + path);
+    return *v;
   }
-  return out;
-}
-
-std::vector<std::uint8_t> bytes(const Value& v, const std::string& file, const std::string& what) {
-  const std::vector<std::int32_t> d = indices(v, file, what, 0, 255);
-  return std::vector<std::uint8_t>(d.begin(), d.end());
-}
-
-std::vector<std::string> strings(const Value& v, const std::string& file, const std::string& what) {
-  if (!v.is_array()) bad(file, what + " must be an array");
-  std::vector<std::string> out;
-  for (const Value& s : v.items()) {
-    if (!s.is_string()) bad(file, what + " must contain strings");
-    out.push_back(s.as_string());
+  const Value* find(const std::string& path) const {
+    const Value* v = &doc_;
+    std::size_t from = 0;
+    while (v) {
+      const std::size_t dot = path.find('.', from);
+      v = v->find(path.substr(from, dot == std::string::npos ? std::string::npos : dot - from));
+      if (dot == std::string::npos) break;
+      from = dot + 1;
+    }
+    return v;
   }
-  return out;
-}
+  double scalar(const std::string& path) const {
+    const Value& v = at(path);
+    if (!v.is_number()) fail(path + " is not a number");
+    return v.as_double();
+  }
+  std::size_t count(const std::string& path) const {
+    const double d = scalar(path);
+    if (!(d >= 0) || d != std::floor(d)) fail(path + " is not a count");
+    return static_cast<std::size_t>(d);
+  }
+  std::string text(const std::string& path) const {
+    const Value& v = at(path);
+    if (!v.is_string()) fail(path + " is not a string");
+    return v.as_string();
+  }
+  std::string text_or(const std::string& path, const std::string& fallback) const {
+    const Value* v = find(path);
+    return v && v->is_string() ? v->as_string() : fallback;
+  }
+  // length of the array at path (the arrays whose length defines a count)
+  std::size_t length(const std::string& path) const {
+    const Value& v = at(path);
+    if (!v.is_array()) fail(path + " is not an array");
+    return v.size();
+  }
+  const std::string& file() const { return file_; }
 
-void same_size(const std::string& file, const std::string& what, std::size_t got, std::size_t want) {
-  if (got != want) bad(file, what + " has " + std::to_string(got) + " entries, expected " + std::to_string(want));
-}
-
-struct Hashed {
-  const char* name;
-  char kind;  // 'f' f64, 'i' i32, 'b' u8
-  const void* data;
-  std::size_t n;
+ private:
+  std::string file_;
+  Value doc_;
 };
 
-void feed(Fnv1a64& h, const Hashed& a) {
-  if (a.kind == 'f') h.f64(static_cast<const double*>(a.data), a.n);
-  else if (a.kind == 'i') h.i32(static_cast<const std::int32_t*>(a.data), a.n);
-  else h.u8(static_cast<const std::uint8_t*>(a.data), a.n);
+constexpr std::size_t kAnyLength = static_cast<std::size_t>(-1);
+
+// One array of a compiled file: its path, where it goes, the length it must have, the integer range (for Int and
+// Byte) and whether the format hashes it.
+struct ArraySpec {
+  enum Kind { Real, Int, Byte, Text } kind;
+  const char* path;
+  void* out;  // std::vector<double> / <std::int32_t> / <std::uint8_t> / <std::string>
+  std::size_t length;
+  long long lo, hi;
+  bool hashed;
+};
+
+ArraySpec reals(const char* path, std::vector<double>& out, std::size_t length) { return {ArraySpec::Real, path, &out, length, 0, 0, true}; }
+ArraySpec ints(const char* path, std::vector<std::int32_t>& out, std::size_t length, long long lo, long long hi) {
+  return {ArraySpec::Int, path, &out, length, lo, hi, true};
+}
+ArraySpec bytes(const char* path, std::vector<std::uint8_t>& out, std::size_t length) { return {ArraySpec::Byte, path, &out, length, 0, 255, true}; }
+ArraySpec texts(const char* path, std::vector<std::string>& out, std::size_t length) { return {ArraySpec::Text, path, &out, length, 0, 0, false}; }
+
+void read_one(const Document& d, const ArraySpec& s) {
+  const Value& a = d.at(s.path);
+  if (!a.is_array()) d.fail(std::string(s.path) + " is not an array");
+  if (s.length != kAnyLength && a.size() != s.length)
+    d.fail(std::string(s.path) + ": " + std::to_string(a.size()) + " values where the file declares " + std::to_string(s.length));
+  const std::vector<Value>& items = a.items();
+  if (s.kind == ArraySpec::Text) {
+    auto& out = *static_cast<std::vector<std::string>*>(s.out);
+    out.clear();
+    for (const Value& v : items) {
+      if (!v.is_string()) d.fail(std::string(s.path) + " holds a value that is not a string");
+      out.push_back(v.as_string());
+    }
+    return;
+  }
+  std::vector<double> vals(items.size());
+  for (std::size_t i = 0; i < items.size(); ++i) {
+    if (!items[i].is_number()) d.fail(std::string(s.path) + "[" + std::to_string(i) + "] is not a number");
+    vals[i] = items[i].as_double();
+  }
+  if (s.kind == ArraySpec::Real) {
+    *static_cast<std::vector<double>*>(s.out) = std::move(vals);
+    return;
+  }
+  for (std::size_t i = 0; i < vals.size(); ++i)
+    if (vals[i] != std::floor(vals[i]) || vals[i] < static_cast<double>(s.lo) || vals[i] > static_cast<double>(s.hi))
+      d.fail(std::string(s.path) + "[" + std::to_string(i) + "] = " + json::format_number(vals[i]) + " is outside the integers " +
+             std::to_string(s.lo) + " .. " + std::to_string(s.hi));
+  if (s.kind == ArraySpec::Int) {
+    auto& out = *static_cast<std::vector<std::int32_t>*>(s.out);
+    out.assign(vals.size(), 0);
+    std::transform(vals.begin(), vals.end(), out.begin(), [](double x) { return static_cast<std::int32_t>(x); });
+  } else {
+    auto& out = *static_cast<std::vector<std::uint8_t>*>(s.out);
+    out.assign(vals.size(), 0);
+    std::transform(vals.begin(), vals.end(), out.begin(), [](double x) { return static_cast<std::uint8_t>(x); });
+  }
 }
 
-std::string verify_hashes(const Value& doc, const std::string& file, const std::vector<Hashed>& arrays) {
-  const Value& H = at(doc, "hash", file);
-  Fnv1a64 chain;
-  for (const Hashed& a : arrays) {
-    Fnv1a64 one;
-    feed(one, a);
-    feed(chain, a);
-    const std::string want = json::string(H, a.name, file + " hash");
-    if (one.hex() != want) bad(file, std::string("hash mismatch on ") + a.name + " (" + one.hex() + " vs " + want + "): the JSON round trip was not exact");
+void hash_into(Fnv1a64& h, const ArraySpec& s) {
+  switch (s.kind) {
+    case ArraySpec::Real: { const auto& v = *static_cast<const std::vector<double>*>(s.out); h.f64(v.data(), v.size()); break; }
+    case ArraySpec::Int: { const auto& v = *static_cast<const std::vector<std::int32_t>*>(s.out); h.i32(v.data(), v.size()); break; }
+    case ArraySpec::Byte: { const auto& v = *static_cast<const std::vector<std::uint8_t>*>(s.out); h.u8(v.data(), v.size()); break; }
+    case ArraySpec::Text: break;
   }
-  const std::string want = json::string(H, "all", file + " hash");
-  if (chain.hex() != want) bad(file, "chained hash mismatch (" + chain.hex() + " vs " + want + ")");
+}
+
+// Reads every array of the table, then checks the file's per-array hashes and the chained hash over the hashed arrays
+// in table order; returns the chained hash.
+std::string read_arrays(const Document& d, const std::vector<ArraySpec>& table) {
+  for (const ArraySpec& s : table) read_one(d, s);
+  Fnv1a64 chain;
+  for (const ArraySpec& s : table) {
+    if (!s.hashed) continue;
+    Fnv1a64 own;
+    hash_into(own, s);
+    hash_into(chain, s);
+    const std::string stated = d.text(std::string("hash.") + s.path);
+    if (own.hex() != stated)
+      d.fail(std::string("hash mismatch on ") + s.path + ": the values hash to " + own.hex() + ", the file states " + stated);
+  }
+  const std::string stated = d.text("hash.all");
+  if (chain.hex() != stated) d.fail("hash mismatch on the chain of all arrays: " + chain.hex() + ", the file states " + stated);
   return chain.hex();
 }
 
-void check_format(const Value& doc, const std::string& file, const char* format, int version) {
-  if (json::string_or(doc, "format", "") != format) bad(file, std::string("format is not ") + format);
-  const long long v = json::integer(doc, "formatVersion", file);
-  if (v != version) bad(file, "formatVersion " + std::to_string(v) + " is not supported (engine reads " + std::to_string(version) + ")");
-}
-
-double real(const Value& obj, const char* key, const std::string& file) { return json::number(obj, key, file); }
-
 }  // namespace
 
+// ----------------------------------------------------------------------------- the two formats
+
 std::shared_ptr<CompiledShip> load_ship(const std::string& file) {
-  const Value doc = json::read_file(file);
-  check_format(doc, file, "sinksim.compiled-ship", 1);
+  const Document d(file, "sinksim.compiled-ship");
   auto S = std::make_shared<CompiledShip>();
-  S->id = json::string(doc, "id", file);
-  if (const Value* meta = doc.find("meta")) S->title = json::string_or(*meta, "title", "");
-  const Value& C = at(doc, "columns", file);
-  const auto nc = static_cast<std::size_t>(json::integer(C, "n", file));
-  S->x = numbers(at(C, "x", file), file, "columns.x"); same_size(file, "columns.x", S->x.size(), nc);
-  S->y = numbers(at(C, "y", file), file, "columns.y"); same_size(file, "columns.y", S->y.size(), nc);
-  S->dxdy = numbers(at(C, "dxdy", file), file, "columns.dxdy"); same_size(file, "columns.dxdy", S->dxdy.size(), nc);
-  S->zlo = numbers(at(C, "zlo", file), file, "columns.zlo"); same_size(file, "columns.zlo", S->zlo.size(), nc);
-  S->zhi = numbers(at(C, "zhi", file), file, "columns.zhi"); same_size(file, "columns.zhi", S->zhi.size(), nc);
-  S->zone = indices(at(C, "zone", file), file, "columns.zone", 0, 1 << 30); same_size(file, "columns.zone", S->zone.size(), nc);
-  S->side = indices(at(C, "side", file), file, "columns.side", 0, 1); same_size(file, "columns.side", S->side.size(), nc);
-
-  const Value& N = at(doc, "nodes", file);
-  const auto nn = static_cast<std::size_t>(json::integer(N, "n", file));
-  S->nodeLabel = strings(at(N, "label", file), file, "nodes.label"); same_size(file, "nodes.label", S->nodeLabel.size(), nn);
-  S->mu = numbers(at(N, "mu", file), file, "nodes.mu"); same_size(file, "nodes.mu", S->mu.size(), nn);
-  S->vmax = numbers(at(N, "vmax", file), file, "nodes.vmax"); same_size(file, "nodes.vmax", S->vmax.size(), nn);
-  S->amin = numbers(at(N, "amin", file), file, "nodes.amin"); same_size(file, "nodes.amin", S->amin.size(), nn);
-  S->aov = numbers(at(N, "aov", file), file, "nodes.aov"); same_size(file, "nodes.aov", S->aov.size(), nn);
-
-  const Value& G = at(doc, "segments", file);
-  const auto ns = static_cast<std::size_t>(json::integer(G, "n", file));
-  S->segStart = indices(at(N, "segStart", file), file, "nodes.segStart", 0, static_cast<std::int64_t>(ns)); same_size(file, "nodes.segStart", S->segStart.size(), nn);
-  S->segCount = indices(at(N, "segCount", file), file, "nodes.segCount", 0, static_cast<std::int64_t>(ns)); same_size(file, "nodes.segCount", S->segCount.size(), nn);
-  S->segCol = indices(at(G, "col", file), file, "segments.col", 0, static_cast<std::int64_t>(nc) - 1); same_size(file, "segments.col", S->segCol.size(), ns);
-  S->segA = numbers(at(G, "a", file), file, "segments.a"); same_size(file, "segments.a", S->segA.size(), ns);
-  S->segE = numbers(at(G, "e", file), file, "segments.e"); same_size(file, "segments.e", S->segE.size(), ns);
+  S->id = d.text("id");
+  S->title = d.text_or("meta.title", "");
+  const std::size_t nc = d.count("columns.n"), nn = d.count("nodes.n"), ns = d.count("segments.n");
+  const auto ns_ll = static_cast<long long>(ns), nc_ll = static_cast<long long>(nc);
+  // the hash order of the format: columns, nodes, segments
+  S->hashAll = read_arrays(d, {
+      reals("columns.x", S->x, nc), reals("columns.y", S->y, nc), reals("columns.dxdy", S->dxdy, nc),
+      reals("columns.zlo", S->zlo, nc), reals("columns.zhi", S->zhi, nc),
+      ints("columns.zone", S->zone, nc, 0, 1 << 30), ints("columns.side", S->side, nc, 0, 1),
+      reals("nodes.mu", S->mu, nn), reals("nodes.vmax", S->vmax, nn), reals("nodes.amin", S->amin, nn), reals("nodes.aov", S->aov, nn),
+      ints("nodes.segStart", S->segStart, nn, 0, ns_ll), ints("nodes.segCount", S->segCount, nn, 0, ns_ll),
+      ints("segments.col", S->segCol, ns, 0, nc_ll - 1), reals("segments.a", S->segA, ns), reals("segments.e", S->segE, ns),
+      texts("nodes.label", S->nodeLabel, nn),
+  });
   for (std::size_t n = 0; n < nn; ++n)
     if (static_cast<std::size_t>(S->segStart[n]) + static_cast<std::size_t>(S->segCount[n]) > ns)
-      bad(file, "node " + std::to_string(n) + " segment range exceeds the segment table");
-
-  S->hashAll = verify_hashes(doc, file, {
-    {"columns.x", 'f', S->x.data(), nc}, {"columns.y", 'f', S->y.data(), nc}, {"columns.dxdy", 'f', S->dxdy.data(), nc},
-    {"columns.zlo", 'f', S->zlo.data(), nc}, {"columns.zhi", 'f', S->zhi.data(), nc},
-    {"columns.zone", 'i', S->zone.data(), nc}, {"columns.side", 'i', S->side.data(), nc},
-    {"nodes.mu", 'f', S->mu.data(), nn}, {"nodes.vmax", 'f', S->vmax.data(), nn}, {"nodes.amin", 'f', S->amin.data(), nn},
-    {"nodes.aov", 'f', S->aov.data(), nn}, {"nodes.segStart", 'i', S->segStart.data(), nn}, {"nodes.segCount", 'i', S->segCount.data(), nn},
-    {"segments.col", 'i', S->segCol.data(), ns}, {"segments.a", 'f', S->segA.data(), ns}, {"segments.e", 'f', S->segE.data(), ns},
-  });
+      d.fail("the segments of node " + std::to_string(n) + " run past the segment table");
   return S;
 }
 
 CompiledSim load_sim(const std::string& file) {
-  const Value doc = json::read_file(file);
-  check_format(doc, file, "sinksim.compiled-sim", 1);
+  const Document d(file, "sinksim.compiled-sim");
   CompiledSim M;
-  M.id = json::string(doc, "id", file);
-  M.shipId = json::string(doc, "ship", file);
-  M.shipHash = json::string(doc, "shipHash", file);
-  if (const Value* meta = doc.find("meta")) M.title = json::string_or(*meta, "title", "");
-  const Value& K = at(doc, "constants", file);
-  M.rho = real(K, "rho", file);
-  M.g = real(K, "g", file);
-  M.dt = real(at(doc, "scheme", file), "dt", file);
+  M.id = d.text("id");
+  M.shipId = d.text("ship");
+  M.shipHash = d.text("shipHash");
+  M.title = d.text_or("meta.title", "");
+  M.rho = d.scalar("constants.rho");
+  M.g = d.scalar("constants.g");
+  M.dt = d.scalar("scheme.dt");
+  M.t0 = d.scalar("state0.t"); M.zO0 = d.scalar("state0.zO"); M.pitch0 = d.scalar("state0.pitch"); M.roll0 = d.scalar("state0.roll");
+  M.vz0 = d.scalar("state0.vz"); M.wth0 = d.scalar("state0.wth"); M.wph0 = d.scalar("state0.wph");
+  M.gMargin = d.scalar("groups.margin");
+  M.monitorThreshold = d.scalar("monitors.threshold");
+  M.hullTopBelow = d.scalar("founder.hullTopBelow"); M.pitchAbsAbove = d.scalar("founder.pitchAbsAbove");
+  M.buoyancyBelow = d.scalar("founder.buoyancyBelow"); M.minT = d.scalar("founder.minT");
+  M.xFP = d.scalar("readout.xFP"); M.xAP = d.scalar("readout.xAP");
+  // the body: ms, KG, g0 (three values), then XO .. qph
+  M.body[0] = d.scalar("body.ms");
+  M.body[1] = d.scalar("body.KG");
+  std::vector<double> g0;
+  read_one(d, reals("body.g0", g0, 3));
+  std::copy(g0.begin(), g0.end(), M.body + 2);
+  const char* tail[] = {"XO", "YO", "mh0", "Ith0", "Iph0", "cDz", "cDth", "cDph", "qz", "qth", "qph"};
+  for (int k = 0; k < 11; ++k) M.body[5 + k] = d.scalar(std::string("body.") + tail[k]);
 
-  const Value& st = at(doc, "state0", file);
-  M.t0 = real(st, "t", file); M.zO0 = real(st, "zO", file); M.pitch0 = real(st, "pitch", file); M.roll0 = real(st, "roll", file);
-  M.vz0 = real(st, "vz", file); M.wth0 = real(st, "wth", file); M.wph0 = real(st, "wph", file);
-  M.vol0 = numbers(at(st, "vol", file), file, "state0.vol");
-  const auto nn = M.vol0.size();
-  M.level0 = numbers(at(st, "level", file), file, "state0.level"); same_size(file, "state0.level", M.level0.size(), nn);
-  M.cx0 = numbers(at(st, "cx", file), file, "state0.cx"); same_size(file, "state0.cx", M.cx0.size(), nn);
-  M.cy0 = numbers(at(st, "cy", file), file, "state0.cy"); same_size(file, "state0.cy", M.cy0.size(), nn);
-  M.cz0 = numbers(at(st, "cz", file), file, "state0.cz"); same_size(file, "state0.cz", M.cz0.size(), nn);
-
-  const Value& G = at(doc, "groups", file);
-  const auto ng = static_cast<std::size_t>(json::integer(G, "n", file));
-  M.gNodeCount = indices(at(G, "nodeCount", file), file, "groups.nodeCount", 1, 1 << 20); same_size(file, "groups.nodeCount", M.gNodeCount.size(), ng);
-  M.gNodes = indices(at(G, "nodes", file), file, "groups.nodes", 0, static_cast<std::int64_t>(nn) - 1);
-  M.gNodeStart = indices(at(G, "nodeStart", file), file, "groups.nodeStart", 0, static_cast<std::int64_t>(M.gNodes.size())); same_size(file, "groups.nodeStart", M.gNodeStart.size(), ng);
-  M.gMode = bytes(at(G, "mode", file), file, "groups.mode"); same_size(file, "groups.mode", M.gMode.size(), ng);
-  M.gpx = numbers(at(G, "px", file), file, "groups.px"); same_size(file, "groups.px", M.gpx.size(), ng);
-  M.gpy = numbers(at(G, "py", file), file, "groups.py"); same_size(file, "groups.py", M.gpy.size(), ng);
-  M.gpz = numbers(at(G, "pz", file), file, "groups.pz"); same_size(file, "groups.pz", M.gpz.size(), ng);
-  M.gMargin = real(G, "margin", file);
-  for (std::size_t g = 0; g < ng; ++g)
-    if (static_cast<std::size_t>(M.gNodeStart[g]) + static_cast<std::size_t>(M.gNodeCount[g]) > M.gNodes.size())
-      bad(file, "group " + std::to_string(g) + " member range exceeds the member table");
-
-  const Value& C = at(doc, "connections", file);
-  const auto ncn = static_cast<std::size_t>(json::integer(C, "n", file));
-  M.ca = indices(at(C, "a", file), file, "connections.a", -1, static_cast<std::int64_t>(nn) - 1); same_size(file, "connections.a", M.ca.size(), ncn);
-  M.cb = indices(at(C, "b", file), file, "connections.b", 0, static_cast<std::int64_t>(nn) - 1); same_size(file, "connections.b", M.cb.size(), ncn);
-  M.cLaw = bytes(at(C, "type", file), file, "connections.type"); same_size(file, "connections.type", M.cLaw.size(), ncn);
-  M.cx = numbers(at(C, "x", file), file, "connections.x"); same_size(file, "connections.x", M.cx.size(), ncn);
-  M.cy = numbers(at(C, "y", file), file, "connections.y"); same_size(file, "connections.y", M.cy.size(), ncn);
-  M.cz = numbers(at(C, "z", file), file, "connections.z"); same_size(file, "connections.z", M.cz.size(), ncn);
-  M.cArea = numbers(at(C, "area", file), file, "connections.area"); same_size(file, "connections.area", M.cArea.size(), ncn);
-  M.cCoef = numbers(at(C, "coef", file), file, "connections.coef"); same_size(file, "connections.coef", M.cCoef.size(), ncn);
-  M.cKind = bytes(at(C, "kind", file), file, "connections.kind"); same_size(file, "connections.kind", M.cKind.size(), ncn);
-  M.cIdx = indices(at(C, "idx", file), file, "connections.idx", -1, 1 << 30); same_size(file, "connections.idx", M.cIdx.size(), ncn);
-  M.cEn = bytes(at(C, "en", file), file, "connections.en"); same_size(file, "connections.en", M.cEn.size(), ncn);
-  M.cTOn = numbers(at(C, "tOn", file), file, "connections.tOn"); same_size(file, "connections.tOn", M.cTOn.size(), ncn);
-  M.cSkipGroup = indices(at(C, "skipGroup", file), file, "connections.skipGroup", -1, static_cast<std::int64_t>(ng) - 1); same_size(file, "connections.skipGroup", M.cSkipGroup.size(), ncn);
-  M.cMonitor = indices(at(C, "monitor", file), file, "connections.monitor", -1, 1 << 30); same_size(file, "connections.monitor", M.cMonitor.size(), ncn);
-  if (const Value* kn = C.find("kindNames")) M.kindNames = strings(*kn, file, "connections.kindNames");
-
-  const Value& Mo = at(doc, "monitors", file);
-  M.monitorThreshold = real(Mo, "threshold", file);
-  M.monitorId = strings(at(Mo, "id", file), file, "monitors.id");
-  M.monitorLabel = strings(at(Mo, "label", file), file, "monitors.label");
-  same_size(file, "monitors.label", M.monitorLabel.size(), M.monitorId.size());
-  for (std::size_t c = 0; c < ncn; ++c)
-    if (M.cMonitor[c] >= static_cast<std::int32_t>(M.monitorId.size())) bad(file, "connection " + std::to_string(c) + " refers to a monitor that does not exist");
-
-  const Value& Mk = at(doc, "marks", file);
-  M.markId = strings(at(Mk, "id", file), file, "marks.id");
-  M.markLabel = strings(at(Mk, "label", file), file, "marks.label");
-  M.mkx = numbers(at(Mk, "x", file), file, "marks.x");
-  M.mky = numbers(at(Mk, "y", file), file, "marks.y");
-  M.mkz = numbers(at(Mk, "z", file), file, "marks.z");
-  M.mkWhen = bytes(at(Mk, "when", file), file, "marks.when");
-  same_size(file, "marks.label", M.markLabel.size(), M.markId.size());
-  same_size(file, "marks.x", M.mkx.size(), M.markId.size());
-  same_size(file, "marks.y", M.mky.size(), M.markId.size());
-  same_size(file, "marks.z", M.mkz.size(), M.markId.size());
-  same_size(file, "marks.when", M.mkWhen.size(), M.markId.size());
-
-  const Value& Fo = at(doc, "founder", file);
-  M.hullTopBelow = real(Fo, "hullTopBelow", file);
-  M.pitchAbsAbove = real(Fo, "pitchAbsAbove", file);
-  M.buoyancyBelow = real(Fo, "buoyancyBelow", file);
-  M.minT = real(Fo, "minT", file);
-
-  const Value& B = at(doc, "body", file);
-  const std::vector<double> g0 = numbers(at(B, "g0", file), file, "body.g0");
-  same_size(file, "body.g0", g0.size(), 3);
-  const char* keys[] = {"ms", "KG"};
-  M.body[0] = real(B, keys[0], file); M.body[1] = real(B, keys[1], file);
-  M.body[2] = g0[0]; M.body[3] = g0[1]; M.body[4] = g0[2];
-  const char* rest[] = {"XO", "YO", "mh0", "Ith0", "Iph0", "cDz", "cDth", "cDph", "qz", "qth", "qph"};
-  for (int k = 0; k < 11; ++k) M.body[5 + k] = real(B, rest[k], file);
-
-  const Value& R = at(doc, "readout", file);
-  M.xFP = real(R, "xFP", file);
-  M.xAP = real(R, "xAP", file);
-
-  M.hashAll = verify_hashes(doc, file, {
-    {"groups.nodeStart", 'i', M.gNodeStart.data(), ng}, {"groups.nodeCount", 'i', M.gNodeCount.data(), ng}, {"groups.nodes", 'i', M.gNodes.data(), M.gNodes.size()},
-    {"groups.mode", 'b', M.gMode.data(), ng}, {"groups.px", 'f', M.gpx.data(), ng}, {"groups.py", 'f', M.gpy.data(), ng}, {"groups.pz", 'f', M.gpz.data(), ng},
-    {"connections.a", 'i', M.ca.data(), ncn}, {"connections.b", 'i', M.cb.data(), ncn}, {"connections.type", 'b', M.cLaw.data(), ncn},
-    {"connections.x", 'f', M.cx.data(), ncn}, {"connections.y", 'f', M.cy.data(), ncn}, {"connections.z", 'f', M.cz.data(), ncn},
-    {"connections.area", 'f', M.cArea.data(), ncn}, {"connections.coef", 'f', M.cCoef.data(), ncn}, {"connections.kind", 'b', M.cKind.data(), ncn},
-    {"connections.idx", 'i', M.cIdx.data(), ncn}, {"connections.en", 'b', M.cEn.data(), ncn}, {"connections.tOn", 'f', M.cTOn.data(), ncn},
-    {"connections.skipGroup", 'i', M.cSkipGroup.data(), ncn}, {"connections.monitor", 'i', M.cMonitor.data(), ncn},
-    {"marks.x", 'f', M.mkx.data(), M.mkx.size()}, {"marks.y", 'f', M.mky.data(), M.mky.size()}, {"marks.z", 'f', M.mkz.data(), M.mkz.size()},
-    {"marks.when", 'b', M.mkWhen.data(), M.mkWhen.size()},
-    {"state0.vol", 'f', M.vol0.data(), nn}, {"state0.level", 'f', M.level0.data(), nn},
-    {"state0.cx", 'f', M.cx0.data(), nn}, {"state0.cy", 'f', M.cy0.data(), nn}, {"state0.cz", 'f', M.cz0.data(), nn},
+  // counts: nodes from the initial volumes, the rest declared or from their id lists
+  const std::size_t nn = d.length("state0.vol"), ng = d.count("groups.n"), nk = d.count("connections.n");
+  const std::size_t members = d.length("groups.nodes"), nmon = d.length("monitors.id"), nmark = d.length("marks.id");
+  const auto nn_ll = static_cast<long long>(nn), ng_ll = static_cast<long long>(ng);
+  // the hash order of the format: groups, connections, marks, initial state
+  M.hashAll = read_arrays(d, {
+      ints("groups.nodeStart", M.gNodeStart, ng, 0, static_cast<long long>(members)), ints("groups.nodeCount", M.gNodeCount, ng, 1, 1 << 20),
+      ints("groups.nodes", M.gNodes, kAnyLength, 0, nn_ll - 1), bytes("groups.mode", M.gMode, ng),
+      reals("groups.px", M.gpx, ng), reals("groups.py", M.gpy, ng), reals("groups.pz", M.gpz, ng),
+      ints("connections.a", M.ca, nk, -1, nn_ll - 1), ints("connections.b", M.cb, nk, 0, nn_ll - 1), bytes("connections.type", M.cLaw, nk),
+      reals("connections.x", M.cx, nk), reals("connections.y", M.cy, nk), reals("connections.z", M.cz, nk),
+      reals("connections.area", M.cArea, nk), reals("connections.coef", M.cCoef, nk), bytes("connections.kind", M.cKind, nk),
+      ints("connections.idx", M.cIdx, nk, -1, 1 << 30), bytes("connections.en", M.cEn, nk), reals("connections.tOn", M.cTOn, nk),
+      ints("connections.skipGroup", M.cSkipGroup, nk, -1, ng_ll - 1), ints("connections.monitor", M.cMonitor, nk, -1, static_cast<long long>(nmon) - 1),
+      reals("marks.x", M.mkx, nmark), reals("marks.y", M.mky, nmark), reals("marks.z", M.mkz, nmark), bytes("marks.when", M.mkWhen, nmark),
+      reals("state0.vol", M.vol0, nn), reals("state0.level", M.level0, nn), reals("state0.cx", M.cx0, nn), reals("state0.cy", M.cy0, nn),
+      reals("state0.cz", M.cz0, nn),
+      texts("monitors.id", M.monitorId, nmon), texts("monitors.label", M.monitorLabel, nmon),
+      texts("marks.id", M.markId, nmark), texts("marks.label", M.markLabel, nmark),
   });
+  if (d.find("connections.kindNames")) read_one(d, texts("connections.kindNames", M.kindNames, kAnyLength));
+  for (std::size_t g = 0; g < ng; ++g)
+    if (static_cast<std::size_t>(M.gNodeStart[g]) + static_cast<std::size_t>(M.gNodeCount[g]) > members)
+      d.fail("the members of group " + std::to_string(g) + " run past the member table");
   return M;
 }
 
 void check_pairing(const CompiledShip& ship, const CompiledSim& sim) {
-  if (sim.shipId != ship.id) throw std::runtime_error("simulation " + sim.id + " was compiled for ship " + sim.shipId + ", not " + ship.id);
+  // the sim names the ship it was compiled for and the chained hash of that ship's arrays
+  // (engine/src/compiled.cpp:275-279 of the reference makes the same three checks)
+  if (sim.shipId != ship.id) throw std::runtime_error("simulation " + sim.id + " belongs to ship " + sim.shipId + ", not to " + ship.id);
   if (sim.shipHash != ship.hashAll)
-    throw std::runtime_error("simulation " + sim.id + " was compiled against a different build of ship " + ship.id + " (hash " + sim.shipHash + " vs " + ship.hashAll + ")");
+    throw std::runtime_error("simulation " + sim.id + " was compiled against another build of ship " + ship.id + " (its ship hash " + sim.shipHash +
+                             ", the ship's " + ship.hashAll + ")");
   if (sim.nodes() != ship.nodes())
-    throw std::runtime_error("simulation " + sim.id + " has " + std::to_string(sim.nodes()) + " nodes, ship " + ship.id + " has " + std::to_string(ship.nodes()));
+    throw std::runtime_error("simulation " + sim.id + " describes " + std::to_string(sim.nodes()) + " nodes, ship " + ship.id + " has " +
+                             std::to_string(ship.nodes()));
 }
 
+// ----------------------------------------------------------------------------- derived tables
+
 Incidence build_incidence(const CompiledSim& sim) {
-  const auto nn = static_cast<std::size_t>(sim.nodes());
-  const std::int32_t nc = sim.connections();
+  // Every connection touches its b node (+dV) and, unless it opens to the sea, its a node (-dV). Listing those
+  // touches in connection order and sorting them stably by node gives each node its connections in increasing
+  // order: the order in which a scatter over the connections would have added them (engine/src/model.cpp:26-56 of
+  // the reference builds the same lists).
+  struct Touch {
+    std::int32_t node, conn;
+    std::uint8_t side;
+  };
+  std::vector<Touch> touches;
   Incidence inc;
+  for (std::int32_t c = 0; c < sim.connections(); ++c) {
+    if (sim.ca[c] >= 0) touches.push_back({sim.ca[c], c, 0});
+    else inc.sea.push_back(c);
+    touches.push_back({sim.cb[c], c, 1});
+  }
+  std::stable_sort(touches.begin(), touches.end(), [](const Touch& x, const Touch& y) { return x.node < y.node; });
+  const auto nn = static_cast<std::size_t>(sim.nodes());
   inc.count.assign(nn, 0);
-  for (std::int32_t c = 0; c < nc; ++c) {
-    if (sim.ca[c] >= 0) inc.count[static_cast<std::size_t>(sim.ca[c])]++;
-    inc.count[static_cast<std::size_t>(sim.cb[c])]++;
+  for (const Touch& t : touches) {
+    inc.count[static_cast<std::size_t>(t.node)]++;
+    inc.conn.push_back(t.conn);
+    inc.side.push_back(t.side);
   }
   inc.start.assign(nn, 0);
-  std::int32_t total = 0;
-  for (std::size_t n = 0; n < nn; ++n) { inc.start[n] = total; total += inc.count[n]; }
-  inc.conn.assign(static_cast<std::size_t>(total), -1);
-  inc.side.assign(static_cast<std::size_t>(total), 0);
-  std::vector<std::int32_t> fill(nn, 0);
-  for (std::int32_t c = 0; c < nc; ++c) {
-    if (sim.ca[c] >= 0) {
-      const auto n = static_cast<std::size_t>(sim.ca[c]);
-      const auto k = static_cast<std::size_t>(inc.start[n] + fill[n]++);
-      inc.conn[k] = c; inc.side[k] = 0;
-    } else {
-      inc.sea.push_back(c);
-    }
-    const auto n = static_cast<std::size_t>(sim.cb[c]);
-    const auto k = static_cast<std::size_t>(inc.start[n] + fill[n]++);
-    inc.conn[k] = c; inc.side[k] = 1;
-  }
+  std::partial_sum(inc.count.begin(), inc.count.end() - (nn ? 1 : 0), inc.start.begin() + (nn ? 1 : 0));
   return inc;
 }
 
 MonitorLists build_monitor_lists(const CompiledSim& sim) {
-  const auto nm = static_cast<std::size_t>(sim.monitors());
+  // per monitor the connections that report to it, in increasing order (the monitor sums of the event pass)
   MonitorLists L;
-  L.count.assign(nm, 0);
-  for (const std::int32_t m : sim.cMonitor) if (m >= 0) L.count[static_cast<std::size_t>(m)]++;
-  L.start.assign(nm, 0);
-  std::int32_t total = 0;
-  for (std::size_t m = 0; m < nm; ++m) { L.start[m] = total; total += L.count[m]; }
-  L.conn.assign(static_cast<std::size_t>(total), 0);
-  std::vector<std::int32_t> fill(nm, 0);
-  for (std::int32_t c = 0; c < sim.connections(); ++c) {
-    const std::int32_t m = sim.cMonitor[static_cast<std::size_t>(c)];
-    if (m < 0) continue;
-    L.conn[static_cast<std::size_t>(L.start[m] + fill[m]++)] = c;
+  const auto nm = static_cast<std::size_t>(sim.monitors());
+  std::vector<std::vector<std::int32_t>> lists(nm);
+  for (std::int32_t c = 0; c < sim.connections(); ++c)
+    if (sim.cMonitor[static_cast<std::size_t>(c)] >= 0) lists[static_cast<std::size_t>(sim.cMonitor[static_cast<std::size_t>(c)])].push_back(c);
+  for (const auto& l : lists) {
+    L.start.push_back(static_cast<std::int32_t>(L.conn.size()));
+    L.count.push_back(static_cast<std::int32_t>(l.size()));
+    L.conn.insert(L.conn.end(), l.begin(), l.end());
   }
   return L;
 }

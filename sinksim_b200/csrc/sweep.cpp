@@ -1,3 +1,8 @@
+// Sweep files, their application to instances, batch-results files and traces: the formats "sinksim.sweep",
+// "sinksim.batch-results" and "sinksim.trace" of the reference (engine/include/sinksim/sweep.hpp:20-108,
+// engine/src/sweep.cpp, engine/src/trace.cpp:272-308). The member names, their order and the numbers' text are the
+// formats'; the code is organised around tables: the columns of a readout curve, the final readouts and the trace
+// columns are each declared once and drive the writer, the reader and the exact comparison alike.
 #include "sweep.h"
 
 #include <algorithm>
@@ -12,70 +17,122 @@ using json::Value;
 
 namespace {
 
-std::uint8_t kind_byte(const CompiledSim& sim, const std::string& name, const std::string& where) {
+// ----------------------------------------------------------------------------- the tables
+
+// The seven columns of a readout curve, in the file's order.
+struct CurveColumn {
+  const char* name;
+  double CurveRecord::*field;
+};
+constexpr CurveColumn kCurve[] = {{"t", &CurveRecord::t},         {"trim", &CurveRecord::trim},     {"list", &CurveRecord::list},
+                                  {"water", &CurveRecord::water}, {"inflow", &CurveRecord::inflow}, {"draftF", &CurveRecord::dF},
+                                  {"draftA", &CurveRecord::dA}};
+
+// The final readouts of an instance, in the file's order, with the short name the comparison reports.
+struct FinalField {
+  const char* name;
+  const char* shortName;
+  double InstanceResult::*field;
+};
+constexpr FinalField kFinal[] = {{"trimDeg", "trim", &InstanceResult::fTrim},    {"listDeg", "list", &InstanceResult::fList},
+                                 {"waterT", "water", &InstanceResult::fWater},   {"draftF", "draftF", &InstanceResult::fDraftF},
+                                 {"draftA", "draftA", &InstanceResult::fDraftA}, {"inflowTpm", "inflow", &InstanceResult::fInflow}};
+// the comparison checks every final field but the inflow (the reference's sweep::compare does the same)
+constexpr int kComparedFinal = 5;
+
+// The columns of a trace block, in the file's (and the hash chain's) order.
+struct TraceField {
+  const char* name;
+  std::vector<double> TraceColumns::*field;
+};
+constexpr TraceField kTrace[] = {{"t", &TraceColumns::t},         {"zO", &TraceColumns::zO},       {"pitch", &TraceColumns::pitch},
+                                 {"roll", &TraceColumns::roll},   {"vz", &TraceColumns::vz},       {"wth", &TraceColumns::wth},
+                                 {"wph", &TraceColumns::wph},     {"inflow", &TraceColumns::inflow}, {"Vb", &TraceColumns::Vb},
+                                 {"hullTop", &TraceColumns::hullTop}, {"vol", &TraceColumns::vol},   {"level", &TraceColumns::level},
+                                 {"cx", &TraceColumns::cx},       {"cy", &TraceColumns::cy},       {"cz", &TraceColumns::cz}};
+
+Value header(const char* format) {
+  Value doc = Value::object();
+  doc.set("format", Value::string(format));
+  doc.set("formatVersion", Value::integer(1));
+  return doc;
+}
+
+// A sweep must state its formatVersion; a results file may omit it.
+void expect_format(const Value& doc, const std::string& path, const char* format, bool versionRequired) {
+  if (json::string_or(doc, "format", "") != format) throw std::runtime_error(path + ": not a " + format + " file");
+  if ((versionRequired || doc.contains("formatVersion")) && json::integer(doc, "formatVersion", path) != 1)
+    throw std::runtime_error(path + ": " + format + " formatVersion " + std::to_string(json::integer(doc, "formatVersion", path)) +
+                             " cannot be read (version 1 can)");
+}
+
+// ----------------------------------------------------------------------------- sweeps
+
+std::uint8_t kind_of(const CompiledSim& sim, const std::string& name, const std::string& where) {
   const std::int32_t k = sim.kindIndex(name);
-  if (k < 0) throw std::runtime_error(where + ": unknown connection kind \"" + name + "\"");
+  if (k < 0) throw std::runtime_error(where + ": the sim has no connection kind \"" + name + "\"");
   return static_cast<std::uint8_t>(k);
 }
 
-std::string kind_name(const CompiledSim& sim, std::uint8_t kind) {
-  const auto i = static_cast<std::size_t>(kind);
-  return i < sim.kindNames.size() ? sim.kindNames[i] : std::to_string(kind);
+std::string kind_label(const CompiledSim& sim, std::uint8_t kind) {
+  return kind < sim.kindNames.size() ? sim.kindNames[kind] : std::to_string(kind);
+}
+
+// One entry of an instance's "connections" list: a selector (one connection, or a kind with an optional index
+// within the kind) and the fields it sets.
+ConnectionOverride read_override(const Value& o, const CompiledSim& sim, const std::string& where) {
+  if (!o.is_object()) throw std::runtime_error(where + ": a connection override must be an object");
+  ConnectionOverride ov;
+  if (o.contains("conn")) {
+    ov.conn = static_cast<std::int32_t>(json::integer(o, "conn", where));  // a connection that does not exist matches nothing
+  } else {
+    ov.kind = kind_of(sim, json::string(o, "kind", where), where);
+    if (o.contains("idx")) ov.idx = static_cast<std::int32_t>(json::integer(o, "idx", where));
+  }
+  if ((ov.hasEnabled = o.contains("enabled"))) ov.enabled = json::boolean(o, "enabled", where);
+  if ((ov.hasTOn = o.contains("tOn"))) ov.tOn = json::number(o, "tOn", where);
+  if ((ov.hasArea = o.contains("area"))) ov.area = json::number(o, "area", where);
+  return ov;
+}
+
+SweepInstance read_instance(const Value& j, std::size_t index, const CompiledSim& sim, const std::string& path) {
+  SweepInstance in;
+  in.id = json::string_or(j, "id", "instance" + std::to_string(index));
+  const std::string where = path + ", instance " + in.id;
+  if (const Value* s = j.find("scale")) {
+    if (!s->is_object()) throw std::runtime_error(where + ": scale must map connection kinds to factors");
+    for (const auto& [kind, factor] : s->members()) {
+      if (!factor.is_number()) throw std::runtime_error(where + ": the scale of " + kind + " is not a number");
+      in.kindScale.emplace_back(kind_of(sim, kind, where), factor.as_double());
+    }
+  }
+  if (const Value* list = j.find("connections")) {
+    if (!list->is_array()) throw std::runtime_error(where + ": connections must be a list of overrides");
+    for (const Value& o : list->items()) in.overrides.push_back(read_override(o, sim, where));
+  }
+  return in;
 }
 
 }  // namespace
 
 Sweep load_sweep(const std::string& path, const CompiledSim& sim) {
   const Value doc = json::read_file(path);
-  if (json::string_or(doc, "format", "") != "sinksim.sweep") throw std::runtime_error(path + ": format is not sinksim.sweep");
-  if (json::integer(doc, "formatVersion", path) != 1) throw std::runtime_error(path + ": unsupported sweep formatVersion");
+  expect_format(doc, path, "sinksim.sweep", true);
   Sweep sw;
   sw.ship = json::string_or(doc, "ship", "");
   sw.sim = json::string_or(doc, "sim", "");
-  sw.tMax = json::number_or(doc, "tMax", 5 * 3600);
-  sw.every = json::number_or(doc, "every", 30);
-  const Value* sws = doc.find("stopWhenStable");
-  sw.stopWhenStable = sws && sws->is_bool() && sws->as_bool();
+  sw.tMax = json::number_or(doc, "tMax", sw.tMax);
+  sw.every = json::number_or(doc, "every", sw.every);
+  const Value* stable = doc.find("stopWhenStable");
+  sw.stopWhenStable = stable && stable->is_bool() && stable->as_bool();
   const Value& list = json::member(doc, "instances", path);
-  if (!list.is_array()) throw std::runtime_error(path + ": instances must be an array");
-  std::size_t k = 0;
-  for (const Value& j : list.items()) {
-    SweepInstance in;
-    in.id = json::string_or(j, "id", "instance" + std::to_string(k));
-    const std::string where = path + " instance " + in.id;
-    if (const Value* s = j.find("scale")) {
-      if (!s->is_object()) throw std::runtime_error(where + ": scale must be an object of kind -> factor");
-      for (const auto& kv : s->members()) {
-        if (!kv.second.is_number()) throw std::runtime_error(where + ": scale factor for " + kv.first + " is not a number");
-        in.kindScale.emplace_back(kind_byte(sim, kv.first, where), kv.second.as_double());
-      }
-    }
-    if (const Value* l2 = j.find("connections")) {
-      if (!l2->is_array()) throw std::runtime_error(where + ": connections must be an array");
-      for (const Value& o : l2->items()) {
-        ConnectionOverride ov;
-        if (o.contains("conn")) {
-          ov.conn = static_cast<std::int32_t>(json::integer(o, "conn", where));
-        } else {
-          ov.kind = kind_byte(sim, json::string(o, "kind", where), where);
-          if (o.contains("idx")) ov.idx = static_cast<std::int32_t>(json::integer(o, "idx", where));
-        }
-        if (o.contains("enabled")) { ov.hasEnabled = true; ov.enabled = json::boolean(o, "enabled", where); }
-        if (o.contains("tOn")) { ov.hasTOn = true; ov.tOn = json::number(o, "tOn", where); }
-        if (o.contains("area")) { ov.hasArea = true; ov.area = json::number(o, "area", where); }
-        in.overrides.push_back(ov);
-      }
-    }
-    sw.instances.push_back(std::move(in));
-    ++k;
-  }
+  if (!list.is_array()) throw std::runtime_error(path + ": instances must be a list");
+  for (std::size_t i = 0; i < list.items().size(); ++i) sw.instances.push_back(read_instance(list.items()[i], i, sim, path));
   return sw;
 }
 
 void save_sweep(const Sweep& sw, const std::string& path, const CompiledSim& sim) {
-  Value doc = Value::object();
-  doc.set("format", Value::string("sinksim.sweep"));
-  doc.set("formatVersion", Value::integer(1));
+  Value doc = header("sinksim.sweep");
   doc.set("ship", Value::string(sw.ship));
   doc.set("sim", Value::string(sw.sim));
   doc.set("tMax", Value::number(sw.tMax));
@@ -87,52 +144,60 @@ void save_sweep(const Sweep& sw, const std::string& path, const CompiledSim& sim
     j.set("id", Value::string(in.id));
     if (!in.kindScale.empty()) {
       Value s = Value::object();
-      for (const auto& [kind, factor] : in.kindScale) s.set(kind_name(sim, kind), Value::number(factor));
-      j.set("scale", s);
+      for (const auto& [kind, factor] : in.kindScale) s.set(kind_label(sim, kind), Value::number(factor));
+      j.set("scale", std::move(s));
     }
     if (!in.overrides.empty()) {
-      Value l2 = Value::array();
+      Value ovs = Value::array();
       for (const ConnectionOverride& o : in.overrides) {
         Value x = Value::object();
-        if (o.conn >= 0) x.set("conn", Value::integer(o.conn));
-        else {
-          x.set("kind", Value::string(kind_name(sim, o.kind)));
+        if (o.conn >= 0) {
+          x.set("conn", Value::integer(o.conn));
+        } else {
+          x.set("kind", Value::string(kind_label(sim, o.kind)));
           if (o.idx >= 0) x.set("idx", Value::integer(o.idx));
         }
         if (o.hasEnabled) x.set("enabled", Value::boolean(o.enabled));
         if (o.hasTOn) x.set("tOn", Value::number(o.tOn));
         if (o.hasArea) x.set("area", Value::number(o.area));
-        l2.push(x);
+        ovs.push(std::move(x));
       }
-      j.set("connections", l2);
+      j.set("connections", std::move(ovs));
     }
-    list.push(j);
+    list.push(std::move(j));
   }
-  doc.set("instances", list);
+  doc.set("instances", std::move(list));
   json::write_file(path, doc, 2);
 }
 
 void apply_instance(const SweepInstance& in, const CompiledSim& base, std::uint8_t* en, double* area, double* tOn) {
+  // The connections a selector names: one connection, every connection of a kind, or the one(s) of a kind with the
+  // given index within the kind.
   const std::int32_t nc = base.connections();
+  auto selected = [&](const ConnectionOverride& o, std::int32_t c) {
+    if (o.conn >= 0) return c == o.conn;
+    const auto i = static_cast<std::size_t>(c);
+    return base.cKind[i] == o.kind && (o.idx < 0 || base.cIdx[i] == o.idx);
+  };
+  // kind scales first, each the single product compiled area x factor (sweep.hpp:49-57 of the reference), so that
+  // a scale set here and the same product computed anywhere else give the same bits
   for (const auto& [kind, factor] : in.kindScale)
     for (std::int32_t c = 0; c < nc; ++c)
       if (base.cKind[static_cast<std::size_t>(c)] == kind) area[c] = base.cArea[static_cast<std::size_t>(c)] * factor;
-  for (const ConnectionOverride& o : in.overrides) {
+  // then the overrides, in the order written (sweep.hpp:58-65), a later one winning over an earlier one
+  for (const ConnectionOverride& o : in.overrides)
     for (std::int32_t c = 0; c < nc; ++c) {
-      const auto i = static_cast<std::size_t>(c);
-      const bool match = o.conn >= 0 ? c == o.conn : (base.cKind[i] == o.kind && (o.idx < 0 || base.cIdx[i] == o.idx));
-      if (!match) continue;
+      if (!selected(o, c)) continue;
       if (o.hasEnabled) en[c] = o.enabled ? 1 : 0;
       if (o.hasArea) area[c] = o.area;
       if (o.hasTOn) tOn[c] = o.tOn;
     }
-  }
 }
 
+// ----------------------------------------------------------------------------- batch results
+
 void save_results(const Results& r, const std::string& path) {
-  Value doc = Value::object();
-  doc.set("format", Value::string("sinksim.batch-results"));
-  doc.set("formatVersion", Value::integer(1));
+  Value doc = header("sinksim.batch-results");
   doc.set("ship", Value::string(r.ship));
   doc.set("sim", Value::string(r.sim));
   doc.set("numerics", Value::string(r.numerics));
@@ -147,46 +212,34 @@ void save_results(const Results& r, const std::string& path) {
     j.set("founderT", Value::number(in.founderT));
     j.set("tEnd", Value::number(in.tEnd));
     j.set("steps", Value::integer(in.steps));
-    Value f = Value::object();
-    f.set("trimDeg", Value::number(in.fTrim));
-    f.set("listDeg", Value::number(in.fList));
-    f.set("waterT", Value::number(in.fWater));
-    f.set("draftF", Value::number(in.fDraftF));
-    f.set("draftA", Value::number(in.fDraftA));
-    f.set("inflowTpm", Value::number(in.fInflow));
-    j.set("final", f);
-    Value ev = Value::array();
+    Value fin = Value::object();
+    for (const FinalField& f : kFinal) fin.set(f.name, Value::number(in.*f.field));
+    j.set("final", std::move(fin));
+    Value events = Value::array();
     for (const EventRecord& e : in.events) {
       Value x = Value::object();
       x.set("t", Value::number(e.t));
       x.set("id", Value::string(e.id));
       x.set("label", Value::string(e.label));
-      ev.push(x);
+      events.push(std::move(x));
     }
-    j.set("events", ev);
-    std::vector<double> t, trim, lst, water, inflow, dF, dA;
-    for (const CurveRecord& k : in.curve) {
-      t.push_back(k.t); trim.push_back(k.trim); lst.push_back(k.list); water.push_back(k.water);
-      inflow.push_back(k.inflow); dF.push_back(k.dF); dA.push_back(k.dA);
+    j.set("events", std::move(events));
+    Value curve = Value::object();
+    for (const CurveColumn& col : kCurve) {
+      std::vector<double> v(in.curve.size());
+      std::transform(in.curve.begin(), in.curve.end(), v.begin(), [&](const CurveRecord& k) { return k.*col.field; });
+      curve.set(col.name, Value::numbers(v));
     }
-    Value c = Value::object();
-    c.set("t", Value::numbers(t));
-    c.set("trim", Value::numbers(trim));
-    c.set("list", Value::numbers(lst));
-    c.set("water", Value::numbers(water));
-    c.set("inflow", Value::numbers(inflow));
-    c.set("draftF", Value::numbers(dF));
-    c.set("draftA", Value::numbers(dA));
-    j.set("curve", c);
-    list.push(j);
+    j.set("curve", std::move(curve));
+    list.push(std::move(j));
   }
-  doc.set("instances", list);
+  doc.set("instances", std::move(list));
   json::write_file(path, doc, 2);
 }
 
 Results load_results(const std::string& path) {
   const Value doc = json::read_file(path);
-  if (json::string_or(doc, "format", "") != "sinksim.batch-results") throw std::runtime_error(path + ": format is not sinksim.batch-results");
+  expect_format(doc, path, "sinksim.batch-results", false);
   Results r;
   r.ship = json::string_or(doc, "ship", "");
   r.sim = json::string_or(doc, "sim", "");
@@ -197,76 +250,63 @@ Results load_results(const std::string& path) {
   for (const Value& j : json::member(doc, "instances", path).items()) {
     InstanceResult in;
     in.id = json::string_or(j, "id", "");
-    in.foundered = json::boolean(j, "foundered", path);
-    in.founderT = json::number(j, "founderT", path);
-    in.tEnd = json::number(j, "tEnd", path);
-    in.steps = json::integer(j, "steps", path);
-    const Value& f = json::member(j, "final", path);
-    in.fTrim = json::number(f, "trimDeg", path); in.fList = json::number(f, "listDeg", path); in.fWater = json::number(f, "waterT", path);
-    in.fDraftF = json::number(f, "draftF", path); in.fDraftA = json::number(f, "draftA", path); in.fInflow = json::number(f, "inflowTpm", path);
-    for (const Value& e : json::member(j, "events", path).items())
-      in.events.push_back(EventRecord{json::number(e, "t", path), json::string(e, "id", path), json::string_or(e, "label", "")});
-    const Value& c = json::member(j, "curve", path);
-    auto col = [&](const char* k) {
-      std::vector<double> v;
-      for (const Value& x : json::member(c, k, path).items()) v.push_back(x.as_double());
-      return v;
-    };
-    const auto t = col("t"), trim = col("trim"), lst = col("list"), water = col("water"), inflow = col("inflow"), dF = col("draftF"), dA = col("draftA");
-    for (std::size_t i = 0; i < t.size(); ++i) in.curve.push_back(CurveRecord{t[i], trim[i], lst[i], water[i], inflow[i], dF[i], dA[i]});
+    const std::string where = path + ", instance " + in.id;
+    in.foundered = json::boolean(j, "foundered", where);
+    in.founderT = json::number(j, "founderT", where);
+    in.tEnd = json::number(j, "tEnd", where);
+    in.steps = json::integer(j, "steps", where);
+    const Value& fin = json::member(j, "final", where);
+    for (const FinalField& f : kFinal) in.*f.field = json::number(fin, f.name, where);
+    for (const Value& e : json::member(j, "events", where).items())
+      in.events.push_back(EventRecord{json::number(e, "t", where), json::string(e, "id", where), json::string_or(e, "label", "")});
+    const Value& curve = json::member(j, "curve", where);
+    const std::size_t n = json::member(curve, "t", where).size();
+    in.curve.assign(n, CurveRecord{});
+    for (const CurveColumn& col : kCurve) {
+      const Value& v = json::member(curve, col.name, where);
+      if (v.size() != n) throw std::runtime_error(where + ": curve column " + col.name + " has " + std::to_string(v.size()) + " values, t has " + std::to_string(n));
+      for (std::size_t k = 0; k < n; ++k) in.curve[k].*col.field = v.items()[k].as_double();
+    }
     r.instances.push_back(std::move(in));
   }
   return r;
 }
 
 Diff compare_results(const Results& a, const Results& b) {
+  // Value for value, bit for bit: two NaNs agree, everything else must be equal. The first difference is reported by
+  // its place ("instance <id> curve[k] trim").
   Diff d;
-  auto note = [&](const std::string& where, double x, double y) {
+  auto same = [&](const std::string& where, double x, double y) {
     ++d.compared;
-    if (x != y && !(std::isnan(x) && std::isnan(y))) {
-      ++d.differing;
-      const double ad = std::fabs(x - y);
-      if (ad > d.maxAbs) d.maxAbs = ad;
-      if (d.first.empty()) d.first = where + ": " + json::format_number(x) + " vs " + json::format_number(y);
-    }
+    if (x == y || (std::isnan(x) && std::isnan(y))) return;
+    ++d.differing;
+    d.maxAbs = std::max(d.maxAbs, std::fabs(x - y));
+    if (d.first.empty()) d.first = where + ": " + json::format_number(x) + " vs " + json::format_number(y);
   };
   if (a.instances.size() != b.instances.size()) {
-    d.differing++;
+    d.differing = 1;
     d.first = "instance count " + std::to_string(a.instances.size()) + " vs " + std::to_string(b.instances.size());
     return d;
   }
   for (std::size_t i = 0; i < a.instances.size(); ++i) {
-    const InstanceResult& x = a.instances[i];
-    const InstanceResult& y = b.instances[i];
+    const InstanceResult &x = a.instances[i], &y = b.instances[i];
     const std::string w = "instance " + x.id;
-    note(w + " foundered", x.foundered, y.foundered);
-    note(w + " founderT", x.founderT, y.founderT);
-    note(w + " tEnd", x.tEnd, y.tEnd);
-    note(w + " steps", static_cast<double>(x.steps), static_cast<double>(y.steps));
-    note(w + " trim", x.fTrim, y.fTrim);
-    note(w + " list", x.fList, y.fList);
-    note(w + " water", x.fWater, y.fWater);
-    note(w + " draftF", x.fDraftF, y.fDraftF);
-    note(w + " draftA", x.fDraftA, y.fDraftA);
-    note(w + " events", static_cast<double>(x.events.size()), static_cast<double>(y.events.size()));
+    same(w + " foundered", x.foundered, y.foundered);
+    same(w + " founderT", x.founderT, y.founderT);
+    same(w + " tEnd", x.tEnd, y.tEnd);
+    same(w + " steps", static_cast<double>(x.steps), static_cast<double>(y.steps));
+    for (int f = 0; f < kComparedFinal; ++f) same(w + " " + kFinal[f].shortName, x.*kFinal[f].field, y.*kFinal[f].field);
+    same(w + " events", static_cast<double>(x.events.size()), static_cast<double>(y.events.size()));
     for (std::size_t k = 0; k < std::min(x.events.size(), y.events.size()); ++k) {
-      note(w + " event " + x.events[k].id + " t", x.events[k].t, y.events[k].t);
-      if (x.events[k].id != y.events[k].id) {
-        ++d.differing;
-        if (d.first.empty()) d.first = w + " event id " + x.events[k].id + " vs " + y.events[k].id;
-      }
+      same(w + " event " + x.events[k].id + " t", x.events[k].t, y.events[k].t);
+      if (x.events[k].id == y.events[k].id) continue;
+      ++d.differing;
+      if (d.first.empty()) d.first = w + " event id " + x.events[k].id + " vs " + y.events[k].id;
     }
-    note(w + " curve length", static_cast<double>(x.curve.size()), static_cast<double>(y.curve.size()));
-    for (std::size_t k = 0; k < std::min(x.curve.size(), y.curve.size()); ++k) {
-      const std::string c = w + " curve[" + std::to_string(k) + "]";
-      note(c + " t", x.curve[k].t, y.curve[k].t);
-      note(c + " trim", x.curve[k].trim, y.curve[k].trim);
-      note(c + " list", x.curve[k].list, y.curve[k].list);
-      note(c + " water", x.curve[k].water, y.curve[k].water);
-      note(c + " inflow", x.curve[k].inflow, y.curve[k].inflow);
-      note(c + " draftF", x.curve[k].dF, y.curve[k].dF);
-      note(c + " draftA", x.curve[k].dA, y.curve[k].dA);
-    }
+    same(w + " curve length", static_cast<double>(x.curve.size()), static_cast<double>(y.curve.size()));
+    for (std::size_t k = 0; k < std::min(x.curve.size(), y.curve.size()); ++k)
+      for (const CurveColumn& col : kCurve)
+        same(w + " curve[" + std::to_string(k) + "] " + col.name, x.curve[k].*col.field, y.curve[k].*col.field);
   }
   return d;
 }
@@ -274,48 +314,17 @@ Diff compare_results(const Results& a, const Results& b) {
 // ----------------------------------------------------------------------------- traces
 
 void TraceColumns::push_record(const double* rec, std::int32_t nodes) {
+  // the record layout of the device: ten scalars, then vol, level, cx, cy, cz per node
   ++n;
-  t.push_back(rec[0]); zO.push_back(rec[1]); pitch.push_back(rec[2]); roll.push_back(rec[3]);
-  vz.push_back(rec[4]); wth.push_back(rec[5]); wph.push_back(rec[6]);
-  inflow.push_back(rec[7]); Vb.push_back(rec[8]); hullTop.push_back(rec[9]);
-  const double* p = rec + 10;
-  vol.insert(vol.end(), p, p + nodes); p += nodes;
-  level.insert(level.end(), p, p + nodes); p += nodes;
-  cx.insert(cx.end(), p, p + nodes); p += nodes;
-  cy.insert(cy.end(), p, p + nodes); p += nodes;
-  cz.insert(cz.end(), p, p + nodes);
-}
-
-namespace {
-
-const char* const kTraceFields[] = {"t", "zO", "pitch", "roll", "vz", "wth", "wph", "inflow", "Vb", "hullTop", "vol", "level", "cx", "cy", "cz"};
-
-const std::vector<double>& trace_field(const TraceColumns& c, int i) {
-  const std::vector<double>* f[] = {&c.t, &c.zO, &c.pitch, &c.roll, &c.vz, &c.wth, &c.wph, &c.inflow, &c.Vb, &c.hullTop,
-                                    &c.vol, &c.level, &c.cx, &c.cy, &c.cz};
-  return *f[i];
-}
-
-Value trace_columns(const TraceColumns& c, Fnv1a64& chain, Value& hash, const std::string& name) {
-  Value v = Value::object();
-  v.set("n", Value::integer(c.n));
-  for (int i = 0; i < 15; ++i) {
-    const std::vector<double>& src = trace_field(c, i);
-    v.set(kTraceFields[i], Value::numbers(src));
-    Fnv1a64 one;
-    one.f64(src.data(), src.size());
-    chain.f64(src.data(), src.size());
-    hash.set(name + "." + kTraceFields[i], Value::string(one.hex()));
+  for (int f = 0; f < 10; ++f) (this->*kTrace[f].field).push_back(rec[f]);
+  for (int f = 10; f < 15; ++f) {
+    const double* p = rec + 10 + (f - 10) * nodes;
+    (this->*kTrace[f].field).insert((this->*kTrace[f].field).end(), p, p + nodes);
   }
-  return v;
 }
-
-}  // namespace
 
 void save_trace(const Trace& tr, const std::string& path) {
-  Value doc = Value::object();
-  doc.set("format", Value::string("sinksim.trace"));
-  doc.set("formatVersion", Value::integer(1));
+  Value doc = header("sinksim.trace");
   doc.set("role", Value::string(tr.role));
   doc.set("ship", Value::string(tr.ship));
   doc.set("sim", Value::string(tr.sim));
@@ -323,7 +332,7 @@ void save_trace(const Trace& tr, const std::string& path) {
   meta.set("title", Value::string(tr.title));
   meta.set("producer", Value::string(tr.producer));
   meta.set("engine", Value::string(tr.engine));
-  doc.set("meta", meta);
+  doc.set("meta", std::move(meta));
   doc.set("dt", Value::number(tr.dt));
   doc.set("nodes", Value::integer(tr.nodes));
   doc.set("denseSteps", Value::integer(tr.denseSteps));
@@ -332,21 +341,34 @@ void save_trace(const Trace& tr, const std::string& path) {
   doc.set("tEnd", Value::number(tr.tEnd));
   doc.set("foundered", Value::boolean(tr.foundered));
   doc.set("founderT", Value::number(tr.founderT));
-  Value ev = Value::array();
+  Value events = Value::array();
   for (const TraceEvent& e : tr.events) {
     Value x = Value::object();
     x.set("t", Value::number(e.t));
     x.set("id", Value::string(e.id));
     x.set("label", Value::string(e.label));
-    ev.push(x);
+    events.push(std::move(x));
   }
-  doc.set("events", ev);
+  doc.set("events", std::move(events));
+  // both blocks column by column, each column hashed alone and into the chain of all of them (dense, then samples)
   Value hash = Value::object();
   Fnv1a64 chain;
-  doc.set("dense", trace_columns(tr.dense, chain, hash, "dense"));
-  doc.set("samples", trace_columns(tr.samples, chain, hash, "samples"));
+  const std::pair<const char*, const TraceColumns*> blocks[] = {{"dense", &tr.dense}, {"samples", &tr.samples}};
+  for (const auto& [name, cols] : blocks) {
+    Value block = Value::object();
+    block.set("n", Value::integer(cols->n));
+    for (const TraceField& f : kTrace) {
+      const std::vector<double>& v = cols->*f.field;
+      block.set(f.name, Value::numbers(v));
+      Fnv1a64 own;
+      own.f64(v.data(), v.size());
+      chain.f64(v.data(), v.size());
+      hash.set(std::string(name) + "." + f.name, Value::string(own.hex()));
+    }
+    doc.set(name, std::move(block));
+  }
   hash.set("all", Value::string(chain.hex()));
-  doc.set("hash", hash);
+  doc.set("hash", std::move(hash));
   json::write_file(path, doc, 2);
 }
 
