@@ -279,6 +279,15 @@ int ssb_adjoint_info(const ssb_adjoint* a, int32_t* connections, int32_t* team_w
  * denominator of the engine's roofline; operations per second through *ops_per_s. No counterpart in the reference. */
 int ssb_measure_add_mul_peak(int32_t fp64, int32_t device, double* ops_per_s);
 
+/* Loads and verifies a compiled ship and sim without running anything (no device needed): formats and versions,
+ * every array's length and integer range, every array's FNV-1a hash and the chained hash against the ones the files
+ * state, and that the sim was compiled for this ship (io::load_ship / io::load_sim / io::check_pairing,
+ * engine/src/compiled.cpp:82-279). SSB_ERUNTIME with the first problem found (ssb_last_error), else SSB_OK. */
+int ssb_check_model(const char* ship_path, const char* sim_path);
+/* The same checks, then a sweep file against that sim (sweep::load_sweep, engine/src/sweep.cpp:25-70): its format,
+ * version and the connection kinds it names. */
+int ssb_check_sweep(const char* ship_path, const char* sim_path, const char* sweep_path);
+
 /* FNV-1a 64-bit over n bytes, continuing from `state` (0xcbf29ce484222325 to start): the hash the compiled-file
  * loaders verify (the reference's engine/include/sinksim/hash.hpp and tools/js/lib/fnv.js), for writers of compiled
  * files such as the hull compiler. Needs no device. */

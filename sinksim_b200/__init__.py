@@ -112,6 +112,8 @@ _SIGNATURES = {
     "ssb_adjoint_samples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "ssb_adjoint_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint64),
                                    C.POINTER(C.c_uint64)]),
+    "ssb_check_model": (C.c_int, [C.c_char_p, C.c_char_p]),
+    "ssb_check_sweep": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p]),
     "ssb_launch_plan": (C.c_int, [C.POINTER(_Options), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
 }
 
@@ -146,6 +148,15 @@ def add_mul_peak(fp64=True, device=0):
     v = C.c_double()
     _check(lib().ssb_measure_add_mul_peak(1 if fp64 else 0, device, C.byref(v)))
     return v.value
+
+
+def check_model(ship_path, sim_path, sweep_path=None):
+    """Verifies a compiled ship and sim (and a sweep file against them) without running anything: formats, lengths,
+    ranges, every hash and the pairing. Raises SinksimError with the first problem."""
+    if sweep_path is None:
+        _check(lib().ssb_check_model(_b(ship_path), _b(sim_path)))
+    else:
+        _check(lib().ssb_check_sweep(_b(ship_path), _b(sim_path), _b(sweep_path)))
 
 
 def library_path():

@@ -155,10 +155,10 @@ int ssb_batch_create(const char* ship_path, const char* sim_path, const ssb_batc
     need(ship_path, "ship_path"); need(sim_path, "sim_path"); need(opt, "opt"); need(out, "out");
     *out = nullptr;
     const ssb::BatchOptions bo = to_options(*opt);
-    need_device();
     auto ship = ssb::load_ship(ship_path);
     const ssb::CompiledSim sim = ssb::load_sim(sim_path);
     ssb::check_pairing(*ship, sim);
+    need_device();
     auto h = std::make_unique<ssb_batch>();
     h->batch = std::make_shared<ssb::Batch>(ship, sim, bo);
     *out = h.release();
@@ -625,5 +625,24 @@ int ssb_adjoint_info(const ssb_adjoint* a, int32_t* connections, int32_t* team_w
     if (teams) *teams = a->adj->teams();
     if (h2d_bytes) *h2d_bytes = a->adj->upload_bytes();
     if (d2h_bytes) *d2h_bytes = a->adj->download_bytes();
+  });
+}
+
+int ssb_check_model(const char* ship_path, const char* sim_path) {
+  return guard([&] {
+    need(ship_path, "ship_path"); need(sim_path, "sim_path");
+    const auto ship = ssb::load_ship(ship_path);
+    const ssb::CompiledSim sim = ssb::load_sim(sim_path);
+    ssb::check_pairing(*ship, sim);
+  });
+}
+
+int ssb_check_sweep(const char* ship_path, const char* sim_path, const char* sweep_path) {
+  return guard([&] {
+    need(ship_path, "ship_path"); need(sim_path, "sim_path"); need(sweep_path, "sweep_path");
+    const auto ship = ssb::load_ship(ship_path);
+    const ssb::CompiledSim sim = ssb::load_sim(sim_path);
+    ssb::check_pairing(*ship, sim);
+    ssb::load_sweep(sweep_path, sim);
   });
 }

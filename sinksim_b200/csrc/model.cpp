@@ -200,17 +200,24 @@ void hash_into(Fnv1a64& h, const ArraySpec& s) {
 // in table order; returns the chained hash.
 std::string read_arrays(const Document& d, const std::vector<ArraySpec>& table) {
   for (const ArraySpec& s : table) read_one(d, s);
+  // the "hash" block names each array by its dotted path as one key ("columns.x"), plus "all" for the chain
+  const Value& stated_hashes = d.at("hash");
+  auto stated_hash = [&](const std::string& key) {
+    const Value* v = stated_hashes.find(key);
+    if (!v || !v->is_string()) d.fail("the hash block has no " + key);
+    return v->as_string();
+  };
   Fnv1a64 chain;
   for (const ArraySpec& s : table) {
     if (!s.hashed) continue;
     Fnv1a64 own;
     hash_into(own, s);
     hash_into(chain, s);
-    const std::string stated = d.text(std::string("hash.") + s.path);
+    const std::string stated = stated_hash(s.path);
     if (own.hex() != stated)
       d.fail(std::string("hash mismatch on ") + s.path + ": the values hash to " + own.hex() + ", the file states " + stated);
   }
-  const std::string stated = d.text("hash.all");
+  const std::string stated = stated_hash("all");
   if (chain.hex() != stated) d.fail("hash mismatch on the chain of all arrays: " + chain.hex() + ", the file states " + stated);
   return chain.hex();
 }
