@@ -279,6 +279,11 @@ int ssb_adjoint_info(const ssb_adjoint* a, int32_t* connections, int32_t* team_w
  * denominator of the engine's roofline; operations per second through *ops_per_s. No counterpart in the reference. */
 int ssb_measure_add_mul_peak(int32_t fp64, int32_t device, double* ops_per_s);
 
+/* Health of the last run: *flags receives 0, or bit 1 when an instance's rigid-body state (heave, pitch, roll or a rate)
+ * was not finite when the kernel stored it (a NaN or infinity in an input, or a diverging model). The reference has no
+ * such report; its engine computes on with NaNs. The results are unchanged; this says that some cannot be trusted. */
+int ssb_batch_health(const ssb_batch* b, int32_t* flags);
+
 /* Loads and verifies a compiled ship and sim without running anything (no device needed): formats and versions,
  * every array's length and integer range, every array's FNV-1a hash and the chained hash against the ones the files
  * state, and that the sim was compiled for this ship (io::load_ship / io::load_sim / io::check_pairing,

@@ -19,6 +19,7 @@ __all__ = ["Batch", "Adjoint", "SinksimError", "available", "device_info", "run_
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsinksim_b200.so")
 NUMERICS = {"portable": 0, "portable32": 1}
+HEALTH_NON_FINITE = 1
 STOP_REASONS = {0: "running", 1: "foundered", 2: "tmax", 3: "sink-rule", 4: "settle-rule", 5: "stable"}
 _ERRORS = {-1: "invalid argument", -2: "runtime error", -3: "call out of order", -4: "unsupported", -5: "no CUDA device"}
 
@@ -113,6 +114,7 @@ _SIGNATURES = {
     "ssb_adjoint_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint64),
                                    C.POINTER(C.c_uint64)]),
     "ssb_check_model": (C.c_int, [C.c_char_p, C.c_char_p]),
+    "ssb_batch_health": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "ssb_check_sweep": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p]),
     "ssb_launch_plan": (C.c_int, [C.POINTER(_Options), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
 }
@@ -340,6 +342,12 @@ class Batch:
 
     def download(self):
         _check(lib().ssb_batch_download(self._h))
+
+    def health(self):
+        """Flags of the last run: 0, or 1 when an instance's state went NaN or infinite (HEALTH_NON_FINITE)."""
+        f = C.c_int32()
+        _check(lib().ssb_batch_health(self._h, C.byref(f)))
+        return f.value
 
     def transfer_bytes(self):
         a, b = C.c_uint64(), C.c_uint64()

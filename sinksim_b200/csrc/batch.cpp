@@ -96,6 +96,7 @@ struct Batch::Impl {
   std::vector<std::int32_t> hOrder0;
   DevBuf<std::int32_t> order0, order0Count;
   std::vector<float> lastPhaseMs;
+  std::vector<std::int32_t> lastHealth;       // the error word (HealthBit flags) of the last launch()
   std::vector<unsigned long long> lastPhaseSteps;
 
 
@@ -549,6 +550,8 @@ float Batch::launch() {
     float ms = 0;
     check(cudaEventElapsedTime(&ms, I.ev0, I.ev1), "cudaEventElapsedTime");
     I.phaseSteps.download(I.lastPhaseSteps, s);
+  I.error.download(I.lastHealth, s);
+    I.error.download(I.lastHealth, s);
     check(cudaStreamSynchronize(s), "copy to host");
     return ms;
   }
@@ -588,6 +591,7 @@ float Batch::launch() {
   float ms = 0;
   check(cudaEventElapsedTime(&ms, I.ev0, I.ev1), "cudaEventElapsedTime");
   I.phaseSteps.download(I.lastPhaseSteps, s);
+  I.error.download(I.lastHealth, s);
   check(cudaStreamSynchronize(s), "copy to host");
   return ms;
 }
@@ -650,6 +654,8 @@ std::vector<Batch::PhaseStats> Batch::phase_stats() const {
     v.push_back({cfg_.phases[k].teamWarps, I.lastPhaseMs[k], static_cast<std::int64_t>(I.lastPhaseSteps[k])});
   return v;
 }
+
+std::int32_t Batch::health() const { return I_->lastHealth.empty() ? 0 : I_->lastHealth.front(); }
 
 std::int64_t Batch::total_steps() const {
   if (!I_->downloaded) throw std::logic_error("Batch: results before run");

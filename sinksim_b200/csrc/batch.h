@@ -124,6 +124,9 @@ class Batch {
   const BatchOptions& options() const { return opt_; }
   const LaunchConfig& launch_config() const { return cfg_; }
   std::int64_t total_steps() const;
+  // HealthBit flags of the last launch() (0: nothing to report): kHealthNonFinite when an instance's state went NaN or
+  // infinite. Read back with the run's timing; the results themselves are unchanged.
+  std::int32_t health() const;
   // The last launch() by phase: its team size, device time (CUDA events around its kernel launches) and the steps its
   // kernels took.
   struct PhaseStats {

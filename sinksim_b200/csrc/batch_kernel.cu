@@ -165,6 +165,8 @@ __device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
     B.evCount[inst] = R.evCount;  // the leader is lane 0 of warp 0, which keeps the event log
     B.steps[inst] = done;
     B.stop[inst] = stop;
+    if (!(isfinite(R.zO) && isfinite(R.pitch) && isfinite(R.roll) && isfinite(R.vz) && isfinite(R.wth) && isfinite(R.wph)))
+      atomicOr(B.error, kHealthNonFinite);
     if (traced) { B.denseCount[inst] = denseCount; B.sampleCount[inst] = sampleCount; B.nextSample[inst] = nextSample; }
     if (B.curveEvery > 0) { B.curveCount[inst] = curveCount; B.nextCurve[inst] = nextCurve; }
     if (stop != kRunning) atomicSub(B.remaining, 1);

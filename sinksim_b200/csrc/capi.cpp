@@ -646,3 +646,10 @@ int ssb_check_sweep(const char* ship_path, const char* sim_path, const char* swe
     ssb::load_sweep(sweep_path, sim);
   });
 }
+
+int ssb_batch_health(const ssb_batch* b, int32_t* flags) {
+  return guard([&] {
+    need(b, "batch"); need(flags, "flags");
+    *flags = b->batch->health();
+  });
+}

@@ -88,6 +88,11 @@ struct RetireRule {
 // (engine/src/simulation.cpp:179-182), which its GPU runner refused (apps/sinksim_cuda_run.cpp:28).
 enum StopReason : std::int32_t { kRunning = 0, kFoundered = 1, kTimeLimit = 2, kSinkRule = 3, kSettleRule = 4, kStable = 5 };
 
+// Bits of DevBatch::error, which a batch run reports to the host: kHealthNonFinite, an instance's rigid-body state
+// (heave, pitch, roll or their rates) was not finite when the kernel stored it (a NaN or infinity in an input, or a
+// model that diverged). The physics is not changed by it: the instance's results are what the step computed.
+enum HealthBit : std::int32_t { kHealthNonFinite = 1 };
+
 struct DevBatch {
   std::int32_t count;
   // connection fields per instance [count * nc]
@@ -132,7 +137,7 @@ struct DevBatch {
   // have held for more than 1,200 s; exclusive with `rule` (both keep their timer in state slot 7)
   std::int32_t stopWhenStable;
   std::int32_t* queue;         // work-queue head (atomic), reset to 0 before each launch
-  std::int32_t* error;         // first error code seen by any warp (0 = none)
+  std::int32_t* error;         // HealthBit flags of the run (0 = none), or-ed by the kernels and read back by the host
   // adaptive team size: instances not yet stopped (atomic, set to count before the first launch); a launch with
   // yieldBelow > 0 pauses its instances and stops claiming new ones once at most yieldBelow remain, so that the
   // next launch resumes them with larger teams (shorter steps)
