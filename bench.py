@@ -10,12 +10,14 @@ complete batch: every instance from its initial state to its end, in one persist
           the engine's stream), inputs resident in HBM
   e2e     the same through the public API (Batch upload + launch + download: host inputs -> device, run, results ->
           host) timed on the host around each run
-The CPU baseline is the reference CPU engine (oracle/_ref, built from the reference's own sources) run by its own
-sweep tool on a bounded sample of the same workload with all host cores. --impl reference times that tool alone.
+The CPU baseline is the reference CPU engine (oracle/_ref, built from the reference's own sources) on a seeded random
+sample of whole runs of the same instances (founder, sink/settle rule or tMax, as on the GPU), all host cores;
+--impl reference times that alone.
 
 Other workloads: --workload fleet (a mixed fleet of generated hulls, one instance each, in one batch) and
---workload gradient (gradients/s: central-difference gradients of a 10-parameter trajectory objective on the
-generated liner, 21 runs per gradient, every point's stencil in one batch; one step is one public value_and_grad call).
+--workload gradient (gradients/s of a 10-parameter trajectory objective on the generated liner by the hand-written
+adjoint, one step = one public gradient call over the points; the finite-difference arm, 21 runs per gradient, and one
+forward run of the same points are timed beside it).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--numerics portable|portable32]
                     [--model titanic64|liner] [--workload uneven|fleet|gradient]
@@ -67,6 +69,7 @@ def parse():
     ap.add_argument("--hulls", type=int, default=2048, help="fleet: hulls per GPU (one instance each)")
     ap.add_argument("--fleet-tmax", type=float, default=7200.0, help="fleet: s; instances also stop when they founder or calm down")
     ap.add_argument("--points", type=int, default=256, help="gradient: parameter points per GPU (one gradient each)")
+    ap.add_argument("--fd-steps", type=int, default=1, help="gradient: timed calls of the finite-difference arm")
     ap.add_argument("--autotune", action="store_true", help="pick the launch shape by timing candidates first (outside the timed region)")
     args = ap.parse_args()
     if args.model is None:
@@ -225,6 +228,52 @@ def _reference_sweep(ship_p, sim_p, sw, numerics, threads):
     return int(m.group(1)), float(m.group(2))
 
 
+def workload_sweep(sim, count, t_max):
+    """The uneven workload's instances 0 .. count-1 as a sweep document (each instance's areas and door overrides)."""
+    from sinksim_b200.workloads import batch_uneven
+
+    sw = {"format": "sinksim.sweep", "formatVersion": 1, "ship": "", "sim": "", "tMax": t_max, "every": 30, "stopWhenStable": False,
+          "instances": []}
+    for i, (area, enabled) in enumerate(batch_uneven(sim, count)):
+        conns = [{"conn": c, "area": a} for c, a in area.items()] + [{"conn": c, "enabled": bool(e)} for c, e in enabled.items()]
+        sw["instances"].append({"id": f"i{i}", "connections": conns})
+    return sw
+
+
+RUN_SAMPLE_SEED = 20261206
+
+
+def cpu_whole_runs_rate(ship_p, sim_p, ship, sim, numerics, count, sample, t_max, threads):
+    """The reference CPU engine (oracle/_ref/libsinksim_ref.so, Simulation::run) on a seeded random sample of whole runs
+    of the GPU workload's `count` instances: each sampled instance from its initial state to its founder, the sink or
+    settle rule or t_max, exactly as the GPU batch runs it, so both engines take the same mix of steps. Returns
+    (steps/s, steps, s, sample indices)."""
+    import ctypes as C
+
+    import numpy as np
+
+    from sinksim_b200.workloads import deck_edge_rule
+
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libsinksim_ref.so"))
+    f = lib.ssref_time_sweep_runs
+    f.restype = C.c_longlong
+    f.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_int, C.POINTER(C.c_double)]
+    lib.ssref_last_error.restype = C.c_char_p
+    picks = np.sort(np.random.default_rng(RUN_SAMPLE_SEED).choice(count, size=min(sample, count), replace=False)).astype(np.int32)
+    r = deck_edge_rule(ship)
+    rule = np.array([r["pitch"], r["x"], r["y"], r["z"], r["wth"], r["settle"]], dtype=np.float64)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "workload.sweep.json")
+        with open(path, "w") as fh:
+            json.dump(workload_sweep(sim, count, t_max), fh)
+        secs = C.c_double()
+        steps = f(ship_p.encode(), sim_p.encode(), path.encode(), numerics.encode(), picks.ctypes.data, picks.size, t_max, rule.ctypes.data,
+                  threads, C.byref(secs))
+    if steps < 0:
+        raise RuntimeError(lib.ssref_last_error().decode())
+    return steps / secs.value, int(steps), secs.value, picks
+
+
 def cpu_reference_rate(ship_p, sim_p, sim, numerics, instances, t_max, threads, first=0):
     """The reference CPU engine's own sweep tool on `instances` instances of the workload; returns (steps/s, steps, s)."""
     from sinksim_b200.workloads import batch_uneven
@@ -238,8 +287,8 @@ def cpu_reference_rate(ship_p, sim_p, sim, numerics, instances, t_max, threads, 
     return steps / secs, steps, secs
 
 
-# The gradient workload: gradients of a trajectory objective by central differences over 10 parameters, every point's
-# 2 P + 1 = 21 runs in one batch (the finite-difference arm; the hand-written adjoint is not built).
+# The gradient workload: gradients of a trajectory objective over 10 parameters, by the adjoint (one run forward and back
+# per point) and, beside it, by central differences (2 P + 1 = 21 runs per point, every stencil in one batch).
 GRADIENT_KINDS = ("door", "over", "down", "top")
 GRADIENT_BREACHES = 6
 GRADIENT_SEED = 20261205
@@ -307,16 +356,40 @@ def reference_arm(args):
     threads = os.cpu_count() or 1
     if args.workload == "gradient":
         return reference_gradient_arm(args, ship_p, sim_p, sim, threads)
-    n, t_max = 4 * threads, 1800.0
+    if args.workload == "fleet":
+        return reference_fleet_arm(args, threads)
+    ship, _ = load_model(ship_p, sim_p)
+    n = 8 * threads
     for _ in range(args.warmup):
-        cpu_reference_rate(ship_p, sim_p, sim, args.numerics, n, t_max, threads)
+        cpu_whole_runs_rate(ship_p, sim_p, ship, sim, args.numerics, args.count, n, args.tmax, threads)
     tot_steps, tot_s = 0, 0.0
     for _ in range(args.steps):
-        _, s, secs = cpu_reference_rate(ship_p, sim_p, sim, args.numerics, n, t_max, threads)
+        _, s, secs, _ = cpu_whole_runs_rate(ship_p, sim_p, ship, sim, args.numerics, args.count, n, args.tmax, threads)
         tot_steps += s
         tot_s += secs
     v = tot_steps / tot_s
-    sample = f"{n} instances of the workload x <= {t_max:.0f} s each per step, reference sinksim_sweep --threads {threads}"
+    sample = (f"a seeded random sample of {n} of the {args.count} instances, each run whole (to its founder, the sink or settle rule or "
+              f"{args.tmax:.0f} s) by the reference engine's Simulation::run on {threads} threads; the same runs every step")
+    print(json.dumps({"impl": "reference", "metric": "sim-steps/s", "value": v, "unit": "sim-steps/s", "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.numerics == "portable" else "f32+f64",
+                      "data": "synthetic", "config": workload_config(args),
+                      "cpu_baseline": {"value": v, "unit": "sim-steps/s", "cores": threads, "kind": "reference", "sample": sample},
+                      "e2e": {"value": v, "unit": "sim-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
+def reference_fleet_arm(args, threads):
+    """--impl reference for the fleet: the reference engine's sweep tool on the fleet's first `threads` hulls, one
+    process per hull in parallel."""
+    hulls = fleet_models(threads, 0)
+    tot_steps, tot_s = 0, 0.0
+    for _ in range(args.steps):
+        _, s, secs, n = cpu_fleet_rate(hulls, args.numerics, threads, args.fleet_tmax)
+        tot_steps += s
+        tot_s += secs
+    v = tot_steps / tot_s
+    sample = f"the fleet's first {threads} hulls, one reference sinksim_sweep process each, each to its founder, calm or {args.fleet_tmax:.0f} s"
     print(json.dumps({"impl": "reference", "metric": "sim-steps/s", "value": v, "unit": "sim-steps/s", "n_gpus": args.gpus,
                       "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps, "higher_is_better": True,
                       "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.numerics == "portable" else "f32+f64",
@@ -363,8 +436,8 @@ def workload_config(args):
                 "points": "kind scales lognormal(0, 0.3), breach areas U(0.1, 0.4) m2 (seeded); the target trajectory is the run at "
                           "a hidden point from the same distribution",
                 "objective": "sum of squared trim (deg) and heave (m) residuals at 8 times, 990 s apart, to 7,920 s",
-                "gradient": "central differences, relative step 1e-2, 21 runs per gradient, all points' stencils in one batch",
-                "adjoint": "not built (finite-difference arm only)",
+                "gradient": "hand-written FP64 discrete adjoint, checkpoints every 256 steps, one run forward and back per gradient; "
+                            "finite-difference arm beside it: central differences, relative step 1e-2, 21 runs per gradient",
                 "numerics": args.numerics, "t_max_s": 7920.0, "dt_s": 0.25, "retire": "founder | tMax",
                 "parallelism": f"points sharded over {args.gpus} GPU(s), no collective in the step",
                 "l2": "working set (geometry 0.6 MB, per-instance state) is L2-resident by design; every step is a full batch from initial state"}
@@ -383,84 +456,107 @@ def workload_config(args):
 
 
 def gradient_bench(args):
-    """The gradient workload on the GPU: each step is one public value_and_grad call over the rank's points (their
-    stencils in one batch); value from the CUDA-event time of its launch, e2e from its host time."""
+    """The gradient workload on the GPU. One step is one public gradient evaluation of the rank's points by the
+    hand-written adjoint (AdjointEvaluator.value_and_grad: every point forward with FP64 checkpoints every 256 steps,
+    then back); value from its kernel's CUDA-event time, e2e from its host time. Beside it: the same points' forward run
+    alone (the adjoint's cost in forward runs) and the finite-difference arm (value_and_grad: 21 runs per gradient in one
+    batch)."""
     import numpy as np
 
     import sinksim_b200 as ssb
-    from sinksim_b200.calibrate import DEFAULT_FD_STEP, BatchEvaluator, TrajectoryObjective, value_and_grad
+    from sinksim_b200.calibrate import DEFAULT_FD_STEP, AdjointEvaluator, BatchEvaluator, TrajectoryObjective, value_and_grad
     from sinksim_b200.files import load_model
     from sinksim_b200.shard import Ranks, shard_bounds
 
-    ranks = Ranks(backend="nccl", timeout_s=600)
+    ranks = Ranks(backend="nccl", timeout_s=900)
     world, rank, local = ranks.world, ranks.rank, ranks.local
     ship_p, sim_p = model_paths(args.model)
     ship, sim = load_model(ship_p, sim_p)
     space = gradient_space(sim)
     times, every = gradient_times()
-    ev = BatchEvaluator(ship_p, sim_p, space=space, numerics=args.numerics, t_max=times[-1], curve_every=every, device=local)
+    ev = BatchEvaluator(ship_p, sim_p, space=space, numerics="portable", t_max=times[-1], curve_every=every, device=local)
     target = TrajectoryObjective.from_target(ev.run(gradient_point(space, -1)[None, :])[0], times)
+    adj = AdjointEvaluator(ship_p, sim_p, space=space, t_max=times[-1], device=local)
     first, _ = shard_bounds(args.points * world, world, rank)
     thetas = np.stack([gradient_point(space, first + k) for k in range(args.points)])
-    h = DEFAULT_FD_STEP
     for _ in range(args.warmup):
-        value_and_grad(ev, target, thetas, h)
+        adj.value_and_grad(thetas, target)
     ranks.barrier()
     dev_ms, e2e_s, sim_steps = 0.0, 0.0, 0
-    phase_ms, phase_steps = None, None
     with Clocks(local) as clocks:
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            f, g = value_and_grad(ev, target, thetas, h)
+            f, g, steps = adj.value_and_grad(thetas, target)
             e2e_s += time.perf_counter() - t0
-            last = ev.last
-            dev_ms += last["device_ms"]
-            sim_steps += last["steps"]
-            ps = last["phases"]
-            phase_ms = [p["device_ms"] for p in ps] if phase_ms is None else [a + p["device_ms"] for a, p in zip(phase_ms, ps)]
-            phase_steps = [p["steps"] for p in ps] if phase_steps is None else [a + p["steps"] for a, p in zip(phase_steps, ps)]
+            dev_ms += adj.last["device_ms"]
+            sim_steps += adj.last["steps"]
     ranks.barrier()
     if not (np.all(np.isfinite(f)) and np.all(np.isfinite(g))):
         raise RuntimeError("non-finite objective or gradient")
+    # the same points' forward run alone (one batch, the objective's curves): one forward run's device time
+    fwd_ms = []
+    for k in range(2):
+        ev.run(thetas)
+        if k:
+            fwd_ms.append(ev.last["device_ms"])
+    # the finite-difference arm: every point's 21 runs in one batch
+    fd_ms, fd_s = 0.0, 0.0
+    value_and_grad(ev, target, thetas[: max(1, args.points)], DEFAULT_FD_STEP)
+    for _ in range(args.fd_steps):
+        t0 = time.perf_counter()
+        value_and_grad(ev, target, thetas, DEFAULT_FD_STEP)
+        fd_s += time.perf_counter() - t0
+        fd_ms += ev.last["device_ms"]
     dev_s_max = ranks.max(dev_ms / 1e3)
     e2e_max = ranks.max(e2e_s)
+    fd_dev_max = ranks.max(fd_ms / 1e3)
+    fd_e2e_max = ranks.max(fd_s)
+    fwd_max = ranks.max(min(fwd_ms) / 1e3)
     grads = ranks.sum(float(args.points * args.steps))
+    fd_grads = ranks.sum(float(args.points * args.fd_steps))
     all_steps = ranks.sum(float(sim_steps))
     clk = clocks.summary()
     if rank == 0:
-        h2d, d2h = last["transfer"]
+        info = adj.last["info"]
         fp64_peak = ssb.add_mul_peak(True, local)
-        top = max(range(len(phase_ms)), key=lambda k: phase_ms[k])
         if args.model == "titanic64":
             ops_per_step, ops_source = FP64_OPS_PER_STEP, "exact unit counts of titanic64 (the C restatement's counters)"
         else:
             ops_per_step = estimated_ops_per_step(len(ship["x"]), len(ship["segCol"]), len(ship["segCount"]), len(sim["ca"]))
             ops_source = "estimated from the model's size with titanic64's per-step ratios"
-        achieved = ops_per_step * phase_steps[top] / (phase_ms[top] / 1e3)
-        phases = [{"team_warps": p["team_warps"], "device_ms_per_run": m / args.steps, "share": m / sum(phase_ms),
-                   "sim_steps_per_run": s / args.steps} for p, m, s in zip(last["phases"], phase_ms, phase_steps)]
+        adjoint_s = dev_s_max / args.steps
+        # the kernel steps every run three times (forward with checkpoints, recompute with the tape, reverse); the
+        # reverse of a step sweeps the same geometry as its forward (the node passes' and columns' reverses), so each is
+        # counted as one step's FP64 work
+        achieved = 3 * ops_per_step * (all_steps / args.steps) / adjoint_s
+        n_params = space.dim
         out = {"metric": "gradients/s", "value": grads / dev_s_max, "unit": "gradients/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": dev_s_max * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "f64" if args.numerics == "portable" else "f32+f64", "data": "synthetic",
-               "config": workload_config(args),
-               "e2e": {"value": grads / e2e_max, "unit": "gradients/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-               "gpu_launches": args.steps * last["launch"]["kernels"], "launch": last["launch"],
-               "sim_steps_per_s": all_steps / dev_s_max, "runs_per_step": args.points * (2 * space.dim + 1),
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(args),
+               "e2e": {"value": grads / e2e_max, "unit": "gradients/s", "h2d_bytes_per_step": info["h2d_bytes"],
+                       "d2h_bytes_per_step": info["d2h_bytes"]},
+               "gpu_launches": args.steps, "adjoint": {"team_warps": info["team_warps"], "teams": info["teams"], "checkpoint_every": 256,
+                                                      "device_s_per_call": adjoint_s, "forward_run_s": fwd_max,
+                                                      "cost_in_forward_runs": adjoint_s / fwd_max,
+                                                      "sim_steps_per_run": all_steps / args.steps},
+               "finite_difference_arm": {"value": fd_grads / fd_dev_max, "unit": "gradients/s", "e2e": fd_grads / fd_e2e_max,
+                                         "runs_per_gradient": 2 * n_params + 1, "relative_step": DEFAULT_FD_STEP, "calls": args.fd_steps},
                "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
                             "frac": achieved / fp64_peak, "traffic": None, "ops_source": ops_source,
-                            "kernel": f"run_batch<{args.numerics}, {phases[top]['team_warps']}-warp teams> (launch phase {top})",
-                            "phases": phases,
+                            "kernel": f"adjoint_batch<{info['team_warps']}-warp teams>",
+                            "work": "3 step-equivalents per sim-step (forward, recompute, reverse)",
                             "peak_source": "measured on this GPU: separately rounded FP64 add+mul microbenchmark (no FMA, as the bits require)",
                             "ops_per_sim_step": ops_per_step},
                "clocks": clk}
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             k = max(1, threads // 2)
-            v, s, secs = cpu_gradient_rate(ship_p, sim_p, space, thetas[:k], h, args.numerics, threads)
+            v, s, secs = cpu_gradient_rate(ship_p, sim_p, space, thetas[:k], DEFAULT_FD_STEP, "portable", threads)
             out["cpu_baseline"] = {"value": v, "unit": "gradients/s", "cores": threads, "kind": "reference",
-                                   "sample": f"the stencils of the first {k} points ({k * (2 * space.dim + 1)} runs, {s} steps in {secs:.1f} s), "
-                                             f"reference sinksim_sweep --numerics {args.numerics} --threads {threads}"}
+                                   "sample": f"central differences (21 runs each) at the first {k} points ({s} steps in {secs:.1f} s), "
+                                             f"reference sinksim_sweep --numerics portable --threads {threads}"}
         print(json.dumps(out))
+    adj.close()
     ranks.close()
     return 0
 
@@ -578,11 +674,12 @@ def main():
                                              f"founder or 1800 s ({s} steps in {secs:.1f} s)"}
         elif world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            n, t_max = 16 * threads, 3600.0
-            v, s, secs = cpu_reference_rate(ship_p, sim_p, sim, args.numerics, n, t_max, threads)
+            n = 8 * threads
+            v, s, secs, _ = cpu_whole_runs_rate(ship_p, sim_p, ship, sim, args.numerics, args.count, n, args.tmax, threads)
             out["cpu_baseline"] = {"value": v, "unit": "sim-steps/s", "cores": threads, "kind": "reference",
-                                   "sample": f"{n} instances of the workload, each to its founder or {t_max:.0f} s ({s} steps in {secs:.1f} s), "
-                                             f"reference sinksim_sweep --numerics {args.numerics} --threads {threads}"}
+                                   "sample": f"a seeded random sample of {n} of the {args.count} instances, each run whole (founder, sink or "
+                                             f"settle rule, {args.tmax:.0f} s) by the reference engine on {threads} threads "
+                                             f"({s} steps in {secs:.1f} s): the same step mix as the GPU batch"}
         print(json.dumps(out))
     batch.close()
     ranks.close()

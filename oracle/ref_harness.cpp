@@ -257,4 +257,58 @@ long long ssref_time_steps(const char* shipPath, const char* simPath, const char
   return total;
 }
 
+// Times the reference CPU engine on whole runs of chosen sweep instances: instance instances[k] of the sweep file, each
+// run by Simulation::run from the compiled initial state to its founder, tMax or the extra retire predicate (rule,
+// may be null), as the GPU batch runs them; `threads` std::threads pull the instances from an atomic counter (the
+// scheduling of sweep::run_cpu, engine/src/sweep.cpp:121-160). Returns the total steps; seconds gets the wall time of
+// the runs (the models are loaded before the clock starts).
+long long ssref_time_sweep_runs(const char* shipPath, const char* simPath, const char* sweepPath, const char* numerics, const int* instances, int n,
+                                double tMax, const double* rule, int threads, double* seconds) {
+  long long total = -1;
+  guard([&] {
+    Numerics num;
+    if (!numerics_of(numerics, num)) throw std::invalid_argument("unknown numerics");
+    const auto ship = io::load_ship(shipPath);
+    const CompiledSim sim = io::load_sim(simPath);
+    io::check_pairing(*ship, sim);
+    const sweep::Sweep sw = sweep::load_sweep(sweepPath, sim);
+    for (int k = 0; k < n; ++k)
+      if (instances[k] < 0 || static_cast<std::size_t>(instances[k]) >= sw.instances.size()) throw std::out_of_range("sweep instance");
+    std::atomic<int> next{0};
+    std::atomic<long long> steps{0};
+    const auto t0 = std::chrono::steady_clock::now();
+    auto worker = [&] {
+      for (;;) {
+        const int k = next.fetch_add(1);
+        if (k >= n) return;
+        Simulation S(ship, sim, num);
+        sweep::apply(sw.instances[static_cast<std::size_t>(instances[k])], sim, S);
+        RunOptions opt;
+        opt.tMax = tMax;
+        opt.every = 1e9;  // no readout curve beyond the first record
+        std::function<bool(Simulation&)> onStep;
+        double calm = 0;
+        if (rule) {
+          const Retire R{rule[0], rule[1], rule[2], rule[3], rule[4], rule[5]};
+          onStep = [&calm, R](Simulation& Sm) {
+            const State& st = Sm.state();
+            const Frame F = kernel::pose_frame<PortableMath>(Sm.sim_view().body, st.zO, st.pitch, st.roll);
+            const Real zp = kernel::world_z(F, R.xDeck, R.yDeck, R.zDeck), zs = kernel::world_z(F, R.xDeck, -R.yDeck, R.zDeck);
+            if (ss_abs(st.pitch) > R.pitchLimit && (zp < 0 || zs < 0)) return false;
+            calm = ss_abs(st.wth) < R.wthLimit ? calm + Sm.sim_view().dt : 0;
+            return calm < R.settleTime;
+          };
+        }
+        steps += S.run(opt, onStep).steps;
+      }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
+    for (auto& t : pool) t.join();
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    total = steps.load();
+  });
+  return total;
+}
+
 }  // extern "C"
