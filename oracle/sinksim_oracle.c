@@ -94,7 +94,16 @@ struct sso_engine {
   void* hookUser;
   int32_t* passSlot;
   double lastPose[14], lastBuoy[4];
+  /* the branch digest (tests only, on while digestOn): FNV-1a over every discrete decision of every step */
+  int digestOn;
+  uint64_t digest;
 };
+
+/* Adds one decision code to the branch digest. */
+static void decide(sso_engine* e, uint64_t code) {
+  if (!e->digestOn) return;
+  for (int k = 0; k < 8; ++k) { e->digest ^= (code >> (8 * k)) & 0xffu; e->digest *= 1099511628211ULL; }
+}
 
 #define DUP(dst, src, n, T)                                   \
   do {                                                        \
@@ -285,6 +294,18 @@ static Pass node_pass(sso_engine* e, const Pose* F, int32_t n, double h) {
   r.dv = tot.dv * mu * iR;
   r.mx = tot.mx * mu; r.my = tot.my * mu; r.mz = tot.mz * mu;
   r.zmin = tot.zmin; r.zmax = tot.zmax;
+  if (e->digestOn) {
+    /* which segments the level cuts (their count per lane tree is the regime of the pass), and which segment is the
+       extent's bottom and top, as the numbers of partial segments and the extent's value bits do not say: count them */
+    int64_t partial = 0, wet = 0;
+    for (int32_t j = s0; j < s1; ++j) {
+      const int32_t i = e->segCol[j];
+      const double base = F->R20 * e->x[i] + F->R21 * e->y[i] + F->tz;
+      const double zp = (h - base) * iR;
+      if (zp > e->segA[j]) { ++wet; if (zp < e->segE[j]) ++partial; }
+    }
+    decide(e, (uint64_t)n << 40 ^ (uint64_t)wet << 20 ^ (uint64_t)partial);
+  }
   if (e->passHook) {
     const double rec[8] = {h, r.vol, r.dv, r.mx, r.my, r.mz, r.zmin, r.zmax};
     e->passHook(e->hookUser, n, e->passSlot[n]++, rec);
@@ -324,6 +345,7 @@ static void solve_single(sso_engine* e, const Pose* F, int32_t n) {
     if (err > 0) b = h; else a = h;
     double hn = p.dv > SLOPE_MIN ? h - err / p.dv : 0.5 * (a + b);
     if (!(hn > a && hn < b)) hn = 0.5 * (a + b);
+    decide(e, 0x60000000u + (uint64_t)n * 4 + (err > 0 ? 1u : 0u) + (hn == 0.5 * (a + b) ? 2u : 0u));
     h = hn;
     p = node_pass(e, F, n, h);
   }
@@ -394,6 +416,7 @@ static void solve_group(sso_engine* e, const Pose* F, const int32_t* m, int32_t 
     for (int32_t k = 0; k < N; ++k) dv += P[k].dv;
     double hn = dv > SLOPE_MIN ? h - err / dv : 0.5 * (a + b);
     if (!(hn > a && hn < b)) hn = 0.5 * (a + b);
+    decide(e, 0x70000000u + (uint64_t)m[0] * 4 + (err > 0 ? 1u : 0u) + (hn == 0.5 * (a + b) ? 2u : 0u));
     h = hn;
     for (int32_t k = 0; k < N; ++k) P[k] = node_pass(e, F, m[k], h);
   }
@@ -480,7 +503,7 @@ static double flow(sso_engine* e, const Pose* F, int32_t c) {
       q = e->coef[c] * e->area[c] * WEIR_COEFFICIENT * e->sq2g * H1 * sqrt(H1) * f * (Ha >= Hb ? 1.0 : -1.0);
     }
   }
-  if (q == 0) { e->q[c] = 0; return 0; }
+  if (q == 0) { e->q[c] = 0; decide(e, 0x10000000u + (uint64_t)c); return 0; }
   double dV = q * e->dt;
   const int32_t src = dV > 0 ? a : b, dst = dV > 0 ? b : a;
   const double hs = src < 0 ? 0.0 : e->hEff[src];
@@ -489,6 +512,7 @@ static double flow(sso_engine* e, const Pose* F, int32_t c) {
   const int32_t degRef = src < 0 ? e->deg[dst] : (dst < 0 ? e->deg[src] : (e->deg[src] > e->deg[dst] ? e->deg[src] : e->deg[dst]));
   const double share = LIMITER_SHARE / (double)(degRef > 1 ? degRef : 1);
   double lim = inv > 0 ? share * (hs - jmax(hd, zo)) / inv : fabs(dV);
+  decide(e, 0x20000000u + (uint64_t)c * 8 + (lim < 0 ? 1u : 0u) + (fabs(dV) > (lim < 0 ? 0 : lim) ? 2u : 0u) + (dV > 0 ? 4u : 0u));
   if (lim < 0) lim = 0;
   if (fabs(dV) > lim) dV = dV > 0 ? lim : -lim;
   e->q[c] = dV / e->dt;
@@ -525,13 +549,13 @@ static double flows_and_volumes(sso_engine* e, const Pose* F) {
   for (int32_t k = 0; k < e->nsea; ++k) seaIn += e->dV[e->sea[k]];
   for (int32_t n = 0; n < NN; ++n) {
     double v = e->vol[n] + e->acc[n];
-    if (v < 0) v = 0;
+    if (v < 0) { v = 0; decide(e, 0x30000000u + (uint64_t)n); }
     const double vm = e->vmax[n];
     double excess = 0;
     if (v > vm) {
       const double head = jmax(0.0, -e->zmaxN[n]);
       const double cap = vm + e->aov[n] * head;
-      if (v > cap) { excess = v - cap; v = cap; }
+      if (v > cap) { excess = v - cap; v = cap; decide(e, 0x40000000u + (uint64_t)n); }
     }
     e->excess[n] = excess;
     e->vol[n] = v;
@@ -581,6 +605,8 @@ static void body_and_events(sso_engine* e, const Pose* F, const Buoy* hb) {
   const double aph = (Mph - e->cDph * e->wph - e->qph * fabs(e->wph) * e->wph) / Iph;
   e->vz += az * dt; e->wth += ath * dt; e->wph += aph * dt;
   e->zO += e->vz * dt; e->pitch += e->wth * dt; e->roll += e->wph * dt;
+  decide(e, 0x50000000u + (uint64_t)(e->pitch > PITCH_CLAMP) + 2u * (uint64_t)(e->pitch < -PITCH_CLAMP) + 4u * (uint64_t)(e->roll > ROLL_CLAMP) +
+                8u * (uint64_t)(e->roll < -ROLL_CLAMP));
   if (e->pitch > PITCH_CLAMP) { e->pitch = PITCH_CLAMP; e->wth = 0; }
   if (e->pitch < -PITCH_CLAMP) { e->pitch = -PITCH_CLAMP; e->wth = 0; }
   if (e->roll > ROLL_CLAMP) { e->roll = ROLL_CLAMP; e->wph = 0; }
@@ -821,3 +847,10 @@ void sso_solved_state(const sso_engine* e, double* volS, double* levelS, double*
   memcpy(pose14, e->lastPose, sizeof e->lastPose);
   memcpy(buoy4, e->lastBuoy, sizeof e->lastBuoy);
 }
+
+void sso_digest_start(sso_engine* e) {
+  e->digestOn = 1;
+  e->digest = 14695981039346656037ULL;
+}
+
+uint64_t sso_digest(const sso_engine* e) { return e->digest; }

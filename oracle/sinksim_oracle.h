@@ -96,6 +96,13 @@ void sso_set_hooks(sso_engine* e, sso_pass_hook pass, sso_solved_hook solved, vo
 void sso_solved_state(const sso_engine* e, double* volS, double* levelS, double* areaS, double* cxS, double* cyS, double* czS, double* zmaxS,
                       int32_t* merged, double* pose14, double* buoy4);
 
+/* The branch digest, for finite-difference checks of gradients: from sso_digest_start on, every discrete decision
+ * of every step (per node pass the numbers of wet and partial segments, the Newton or bisection branch of every
+ * level update, a flow that is zero or limited, a volume clipped at 0 or at its cap, an angle at its clamp) goes into
+ * one FNV-1a hash. Two runs with the same digest took the same branch path: their difference is the derivative's. */
+void sso_digest_start(sso_engine* e);
+uint64_t sso_digest(const sso_engine* e);
+
 #ifdef __cplusplus
 }
 #endif

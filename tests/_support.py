@@ -113,6 +113,9 @@ def oracle_lib():
         lib.sso_foundered.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         lib.sso_counters_get.argtypes = [C.c_void_p, C.POINTER(_Counters)]
         lib.sso_flows.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.sso_digest_start.argtypes = [C.c_void_p]
+        lib.sso_digest.argtypes = [C.c_void_p]
+        lib.sso_digest.restype = C.c_uint64
         _oracle_lib = lib
     return _oracle_lib
 
@@ -188,6 +191,12 @@ class Oracle:
         c = _Counters()
         self.lib.sso_counters_get(self.h, C.byref(c))
         return {k: getattr(c, k) for k, _ in _Counters._fields_}
+
+    def digest_start(self):
+        self.lib.sso_digest_start(self.h)
+
+    def digest(self):
+        return int(self.lib.sso_digest(self.h))
 
     def flows(self):
         q = np.empty(self.nconn)
