@@ -464,6 +464,100 @@ def lbfgs_batched(fg, x0, max_iter=50, memory=8, f_target=None, rel_tol=1e-12, c
     return x, f, {"iterations": iters, "evaluations": calls, "history": history}
 
 
+def lbfgs_device(fg, x0, max_iter=30, memory=8, rel_target=None, c1=1e-4, max_backtracks=12, device="cuda", callback=None):
+    """L-BFGS on many independent starting points at once with its state on the GPU: points, gradients, the curvature
+    pairs of every restart (a ring of `memory` pairs each), the two-loop recursion and the Armijo backtracking are
+    torch float64 tensors on `device`, computed for all restarts together. fg(X) takes and returns device tensors
+    (X [R, P] -> f [R], g [R, P]) and is called on every row each time (rows that stopped keep their point), so the
+    evaluator's batch keeps its size. A restart stops when f <= rel_target x its starting f, after max_iter accepted
+    steps, or after max_backtracks halvings of one step. Returns (x, f, info) as tensors on the device; info holds
+    the evaluation count and the best objective after each evaluation."""
+    import torch
+
+    x = torch.as_tensor(x0, dtype=torch.float64, device=device).clone()
+    R, P = x.shape
+    f, g = fg(x)
+    f0 = f.clone()
+    S = torch.zeros(R, memory, P, dtype=torch.float64, device=device)
+    Y = torch.zeros_like(S)
+    rho = torch.zeros(R, memory, dtype=torch.float64, device=device)
+    count = torch.zeros(R, dtype=torch.long, device=device)
+    head = torch.zeros(R, dtype=torch.long, device=device)
+    active = torch.ones(R, dtype=torch.bool, device=device)
+    if rel_target is not None:
+        active &= f > rel_target * f0
+    iters = torch.zeros(R, dtype=torch.long, device=device)
+    backtracks = torch.zeros(R, dtype=torch.long, device=device)
+    step = torch.ones(R, dtype=torch.float64, device=device)
+    d = torch.zeros_like(x)
+    fresh = torch.ones(R, dtype=torch.bool, device=device)
+    rows = torch.arange(R, device=device)
+    history = [float(f.min())]
+    calls = 1
+
+    def direction(gr):
+        q = gr.clone()
+        alphas = []
+        for j in range(memory):
+            idx = (head - 1 - j) % memory
+            valid = (j < count).to(torch.float64)
+            s_, y_, r_ = S[rows, idx], Y[rows, idx], rho[rows, idx]
+            a = valid * r_ * (s_ * q).sum(1)
+            q = q - a[:, None] * y_
+            alphas.append((a, idx, valid))
+        newest = (head - 1) % memory
+        s_n, y_n = S[rows, newest], Y[rows, newest]
+        gamma = torch.where(count > 0, (s_n * y_n).sum(1) / (y_n * y_n).sum(1).clamp_min(1e-300), torch.ones_like(f))
+        q = q * gamma[:, None]
+        for a, idx, valid in reversed(alphas):
+            b = valid * rho[rows, idx] * (Y[rows, idx] * q).sum(1)
+            q = q + (a - b)[:, None] * S[rows, idx]
+        return -q
+
+    while bool(active.any()):
+        if bool(fresh.any()):
+            nd = direction(g)
+            descent = (nd * g).sum(1) < 0
+            nd = torch.where(descent[:, None], nd, -g)
+            count = torch.where(fresh & ~descent, torch.zeros_like(count), count)
+            d = torch.where(fresh[:, None], nd, d)
+            gnorm = g.norm(dim=1)
+            first = torch.where(count > 0, torch.ones_like(step), torch.clamp(0.1 / gnorm.clamp_min(1e-300), max=1.0))
+            step = torch.where(fresh, first, step)
+            backtracks = torch.where(fresh, torch.zeros_like(backtracks), backtracks)
+            fresh = torch.zeros_like(fresh)
+        trial = torch.where(active[:, None], x + step[:, None] * d, x)
+        ft, gt = fg(trial)
+        calls += 1
+        slope = (d * g).sum(1)
+        ok = active & (ft <= f + c1 * step * slope)
+        # accepted steps: store the curvature pair when it is positive
+        s_new, y_new = trial - x, gt - g
+        sy = (s_new * y_new).sum(1)
+        keep = ok & (sy > 1e-300)
+        S[rows[keep], head[keep]] = s_new[keep]
+        Y[rows[keep], head[keep]] = y_new[keep]
+        rho[rows[keep], head[keep]] = 1.0 / sy[keep]
+        head = torch.where(keep, (head + 1) % memory, head)
+        count = torch.where(keep, torch.clamp(count + 1, max=memory), count)
+        x = torch.where(ok[:, None], trial, x)
+        f = torch.where(ok, ft, f)
+        g = torch.where(ok[:, None], gt, g)
+        iters = iters + ok.long()
+        fresh = ok.clone()
+        failed = active & ~ok
+        step = torch.where(failed, step * 0.5, step)
+        backtracks = backtracks + failed.long()
+        done = (iters >= max_iter) | (backtracks > max_backtracks)
+        if rel_target is not None:
+            done |= f <= rel_target * f0
+        active &= ~done
+        history.append(float(f.min()))
+        if callback:
+            callback(calls, x, f)
+    return x, f, {"iterations": iters, "evaluations": calls, "history": history, "f0": f0}
+
+
 def random_search(evaluator, objective, kinds=KIND_PARAMS, rounds=5, batch=264, span=0.3, shrink=0.5, seed=20261008, log=None):
     """The reference's batched search (tools/py/calibrate_gpu.py:96-125): each round one batch of log-uniform points
     around the current best (the origin, the compiled model's own values, first), keep the best, shrink the box.
@@ -546,6 +640,11 @@ def main(argv=None):
     ap.add_argument("--restarts", type=int, default=64)
     ap.add_argument("--iters", type=int, default=30)
     ap.add_argument("--h", type=float, default=DEFAULT_FD_STEP, help="relative central-difference step")
+    ap.add_argument("--gradient", default="fd", choices=("fd", "adjoint"),
+                    help="fd: central differences on the batched forward (L-BFGS in host numpy); adjoint: the engine's adjoint "
+                         "with the L-BFGS state on the GPU (torch)")
+    ap.add_argument("--rel-target", type=float, default=None, help="stop a restart once its objective falls below this fraction of its start")
+    ap.add_argument("--t-end", type=float, default=7920.0, help="s: the last of the 8 objective times")
     args = ap.parse_args(argv)
     ship, sim = _model_paths(args)
     if args.mode == "search":
@@ -566,20 +665,35 @@ def main(argv=None):
     from .shard import Ranks
 
     ranks = Ranks(backend="nccl")
-    times = default_times()
+    times = default_times(args.t_end)
     rng = np.random.default_rng(args.seed)
     ev = BatchEvaluator(ship, sim, numerics=args.numerics, t_max=times[-1], curve_every=times[1] - times[0], device=ranks.local)
     hidden = rng.normal(0.0, 0.3, size=ev.space.dim)
     target = TrajectoryObjective.from_target(ev.run(hidden[None, :])[0], times)
     x0 = rng.normal(0.0, 0.3, size=(args.restarts, ev.space.dim))
     t0 = time.time()
-    x, fx, info = lbfgs_batched(lambda X: value_and_grad(ev, target, X, args.h, ranks=ranks), x0, max_iter=args.iters)
+    if args.gradient == "adjoint":
+        import torch
+
+        adj = AdjointEvaluator(ship, sim, space=ev.space, t_max=times[-1], device=ranks.local)
+        dev = torch.device("cuda", ranks.local)
+
+        def fg(X):
+            f, g, _ = adj.value_and_grad(X.cpu().numpy(), target)
+            return torch.as_tensor(f, device=dev), torch.as_tensor(g, device=dev)
+
+        xt, ft, info = lbfgs_device(fg, x0, max_iter=args.iters, rel_target=args.rel_target, device=dev)
+        x, fx = xt.cpu().numpy(), ft.cpu().numpy()
+        ev.device_ms += adj.device_ms
+        ev.instances += adj.instances
+    else:
+        x, fx, info = lbfgs_batched(lambda X: value_and_grad(ev, target, X, args.h, ranks=ranks), x0, max_iter=args.iters)
     wall = ranks.max(time.time() - t0)
     device_s = ranks.max(ev.device_ms / 1e3)
     instances = ranks.sum(float(ev.instances))
     best = int(np.argmin(fx))
     if ranks.rank == 0:
-        print(json.dumps({"restarts": args.restarts, "gpus": ranks.world, "best_objective": float(fx[best]),
+        print(json.dumps({"gradient": args.gradient, "restarts": args.restarts, "gpus": ranks.world, "best_objective": float(fx[best]),
                           "recovery_error": float(np.max(np.abs(x[best] - hidden))), "evaluations": info["evaluations"],
                           "instances": instances, "wall_s": wall, "device_s": device_s}))
     ranks.close()

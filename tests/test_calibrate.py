@@ -130,3 +130,27 @@ def test_two_gloo_ranks_split_the_stencil_and_agree(tmp_path):
     assert all(r["same_values"] and r["same_lbfgs"] for r in res)  # the same bits as one process, on every rank
     assert res[0]["x"] == res[1]["x"]
     assert res[0]["parts"] == res[1]["parts"] == [0.0, 2.5]  # rank 1 sent nothing
+
+
+def test_lbfgs_device_minimises_a_batch_of_quadratics():
+    """The device L-BFGS (torch tensors; here on the CPU) drives every restart of a badly scaled quadratic to its
+    minimum, and stops a restart once its relative target is met."""
+    import torch
+
+    from sinksim_b200.calibrate import lbfgs_device
+
+    rng = np.random.default_rng(3)
+    A = np.diag([1.0, 10.0, 100.0, 0.5])
+    xs = rng.normal(size=(6, 4))
+
+    def fg(X):
+        d = X - torch.as_tensor(xs, dtype=torch.float64)
+        Ad = d @ torch.as_tensor(A)
+        return (d * Ad).sum(1), 2 * Ad
+
+    x0 = np.zeros((6, 4))
+    x, f, info = lbfgs_device(fg, x0, max_iter=60, device="cpu")
+    assert float(f.max()) < 1e-12
+    np.testing.assert_allclose(x.numpy(), xs, atol=1e-6)
+    x, f, info = lbfgs_device(fg, x0, max_iter=60, rel_target=1e-4, device="cpu")
+    assert bool((f <= 1e-4 * info["f0"]).all())
