@@ -530,18 +530,27 @@ SSB_HD bool unit_reverse(const DevModel& M, const PoseD& F, const Tape& t, const
       if (np) pass_sweep(M, F, r.members[k], np, hs, pv, pmx, pmy, pmz, scratch, lane, width, aP);
     }
   }
-  // the free-surface area of every pass: dv = (sum of the cut segments' footprints) mu / R22
-  for (int k = 0; k < N; ++k)
-    for (int j = 0; j <= K && j < kMaxPasses; ++j)
-      if (adv[k][j] != 0) aP.iR += adv[k][j] * rec(t, r.members[k], j)[2] / F.iR;
+  // the free-surface area of every pass: dv = (sum of the cut segments' footprints) mu / R22. Every lane of the warp
+  // holds these scalars; lane 0 alone adds them to the pose adjoint, which is summed over the lanes afterwards.
+  if (lane == 0)
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j <= K && j < kMaxPasses; ++j)
+        if (adv[k][j] != 0) aP.iR += adv[k][j] * rec(t, r.members[k], j)[2] / F.iR;
   // the extent: bottom and top of the unit's start passes
   if (N > 0) {
     aZmin0[r.loSrc] += aLo;
     aZmax0[r.hiSrc] += aHi;
   }
+  // (every lane finds the same segment; lane 0 alone adds its terms)
   for (int k = 0; k < N; ++k) {
-    if (aZmin0[k] != 0) extreme_reverse(M, pass_extreme(M, F, r.members[k], true, lane, width), true, aZmin0[k], aP);
-    if (aZmax0[k] != 0) extreme_reverse(M, pass_extreme(M, F, r.members[k], false, lane, width), false, aZmax0[k], aP);
+    if (aZmin0[k] != 0) {
+      const int j = pass_extreme(M, F, r.members[k], true, lane, width);
+      if (lane == 0) extreme_reverse(M, j, true, aZmin0[k], aP);
+    }
+    if (aZmax0[k] != 0) {
+      const int j = pass_extreme(M, F, r.members[k], false, lane, width);
+      if (lane == 0) extreme_reverse(M, j, false, aZmax0[k], aP);
+    }
   }
   // the start level and the unit's volume
   if (r.single) {
