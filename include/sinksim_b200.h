@@ -45,8 +45,9 @@ typedef struct ssb_batch_options {
   double curve_every;        /* s between readout-curve records of every instance; 0: none */
   double t_max;              /* s: every instance stops here if it has not foundered */
   int64_t steps_per_launch;  /* 0: one persistent launch; > 0: bounded launches (the reference's stepsPerLaunch) */
-  int32_t team_warps;        /* warps stepping one simulation in the main phase: 1, 2, 4 or 8; 0: chosen */
-  int32_t tail_team_warps;   /* warps per simulation once few instances remain: 0 no tail phase, -1 chosen */
+  int32_t team_warps;        /* warps stepping one simulation in the main phase: 1, 2, 4, 8 or 16; 0: chosen */
+  int32_t tail_team_warps;   /* warps per simulation of the last phase (the phases double the team size up to it): 8 or
+                                16 (a whole 512-thread block per simulation); 0 no tail phase, -1 chosen */
   int32_t teams_per_block;   /* simulations per block in the main phase; 0: chosen */
   int32_t yield_below;       /* the main phase hands its instances to the tail phase once at most this many remain;
                                 -1: from handover_factor */

@@ -211,7 +211,7 @@ void Batch::init(std::vector<std::pair<std::shared_ptr<const CompiledShip>, Comp
                              std::to_string(optin) + " per block");
   auto plan = [&](int W, int teamsReq, int count) {
     PhaseConfig p;
-    if (!valid_team_size(W)) throw std::invalid_argument("Batch: warps per simulation must be 1, 2, 4 or 8");
+    if (!valid_team_size(W)) throw std::invalid_argument("Batch: warps per simulation must be 1, 2, 4, 8 or 16");
     p.teamWarps = W;
     p.layout = I.layout_for(W);
     const SlotLayout& L = p.layout;

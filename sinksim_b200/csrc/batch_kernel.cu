@@ -228,6 +228,7 @@ cudaError_t set_smem(int W, std::size_t bytes) {
     case 2: return cudaFuncSetAttribute(run_batch<MIXED, 2, FLEET>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     case 4: return cudaFuncSetAttribute(run_batch<MIXED, 4, FLEET>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     case 8: return cudaFuncSetAttribute(run_batch<MIXED, 8, FLEET>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    case 16: return cudaFuncSetAttribute(run_batch<MIXED, 16, FLEET>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   }
   return cudaErrorInvalidValue;
 }
@@ -239,6 +240,7 @@ cudaError_t occupancy(int W, int threads, std::size_t bytes, int* perSM) {
     case 2: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 2, FLEET>, threads, bytes);
     case 4: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 4, FLEET>, threads, bytes);
     case 8: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 8, FLEET>, threads, bytes);
+    case 16: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, run_batch<MIXED, 16, FLEET>, threads, bytes);
   }
   return cudaErrorInvalidValue;
 }
@@ -250,12 +252,13 @@ void launch(int W, const DevModel& M, const DevBatch& B, const SlotLayout& L, in
     case 2: run_batch<MIXED, 2, FLEET><<<grid, threads, smem, s>>>(M, B, L); break;
     case 4: run_batch<MIXED, 4, FLEET><<<grid, threads, smem, s>>>(M, B, L); break;
     case 8: run_batch<MIXED, 8, FLEET><<<grid, threads, smem, s>>>(M, B, L); break;
+    case 16: run_batch<MIXED, 16, FLEET><<<grid, threads, smem, s>>>(M, B, L); break;
   }
 }
 
 }  // namespace
 
-bool valid_team_size(int W) { return W == 1 || W == 2 || W == 4 || W == 8; }
+bool valid_team_size(int W) { return W == 1 || W == 2 || W == 4 || W == 8 || W == 16; }
 
 cudaError_t configure_batch_kernel(bool mixed, int teamWarps, std::size_t smemBytes, bool fleet) {
   if (!valid_team_size(teamWarps)) return cudaErrorInvalidValue;

@@ -118,6 +118,8 @@ def test_launch_shape_does_not_change_bits(model):
     shapes = [dict(), dict(team_warps=1, tail_team_warps=0, teams_per_block=1), dict(team_warps=1, teams_per_block=16, blocks=1),
               dict(steps_per_launch=777), dict(team_warps=2), dict(team_warps=4), dict(team_warps=8),
               dict(team_warps=1, tail_team_warps=4, yield_below=20), dict(team_warps=2, tail_team_warps=8, yield_below=20),
+              # a whole 16-warp block per simulation, alone and as the last of four phases
+              dict(team_warps=16), dict(team_warps=2, tail_team_warps=16, yield_below=20),
               # 4 teams for 20 instances, handing over once 19 remain: the next phase claims the 16 not yet started
               # before the 3 the first phase paused (fewest steps done first), or by index
               dict(team_warps=1, teams_per_block=4, blocks=1, tail_team_warps=4, yield_below=19),
