@@ -65,7 +65,8 @@ AdjointBatch::AdjointBatch(std::shared_ptr<const CompiledShip> ship, const Compi
   if (opt_.count < 1) throw std::invalid_argument("AdjointBatch: count must be at least 1");
   if (opt_.checkpointEvery < 1) throw std::invalid_argument("AdjointBatch: checkpointEvery must be at least 1");
   if (!(opt_.tMax > 0)) throw std::invalid_argument("AdjointBatch: tMax must be positive");
-  if (opt_.teamWarps != 0 && opt_.teamWarps != 4 && opt_.teamWarps != 8) throw std::invalid_argument("AdjointBatch: teamWarps must be 4 or 8");
+  if (opt_.teamWarps != 0 && opt_.teamWarps != 4 && opt_.teamWarps != 8 && opt_.teamWarps != 16)
+    throw std::invalid_argument("AdjointBatch: teamWarps must be 4, 8 or 16");
   std::string why;
   if (!cuda_available(&why)) throw std::runtime_error("AdjointBatch: " + why);
   Impl& I = *I_;

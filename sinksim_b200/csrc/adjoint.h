@@ -17,7 +17,7 @@ struct AdjointOptions {
   std::int32_t count = 1;
   double tMax = 7920;             // s: the runs stop here or at their founder
   std::int32_t checkpointEvery = 256;
-  std::int32_t teamWarps = 0;     // warps per instance, 4 or 8; 0: chosen from the count
+  std::int32_t teamWarps = 0;     // warps per instance, 4, 8 or 16; 0: chosen from the count
   int device = 0;
 };
 

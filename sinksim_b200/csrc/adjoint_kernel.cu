@@ -332,6 +332,7 @@ cudaError_t configure_adjoint_kernel(int W, std::size_t smem) {
   switch (W) {
     case 4: return cudaFuncSetAttribute(adjoint_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     case 8: return cudaFuncSetAttribute(adjoint_batch<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    case 16: return cudaFuncSetAttribute(adjoint_batch<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   }
   return cudaErrorInvalidValue;
 }
@@ -340,6 +341,7 @@ cudaError_t adjoint_occupancy(int W, std::size_t smem, int* blocksPerSM) {
   switch (W) {
     case 4: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSM, adjoint_batch<4>, 4 * 32, smem);
     case 8: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSM, adjoint_batch<8>, 8 * 32, smem);
+    case 16: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSM, adjoint_batch<16>, 16 * 32, smem);
   }
   return cudaErrorInvalidValue;
 }
@@ -350,6 +352,7 @@ cudaError_t launch_adjoint_kernel(int W, const DevModel& M, const AdjRun& B, con
   switch (W) {
     case 4: adjoint_batch<4><<<teams, 4 * 32, smem, stream>>>(M, B, SL, AL); break;
     case 8: adjoint_batch<8><<<teams, 8 * 32, smem, stream>>>(M, B, SL, AL); break;
+    case 16: adjoint_batch<16><<<teams, 16 * 32, smem, stream>>>(M, B, SL, AL); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
