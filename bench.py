@@ -289,33 +289,8 @@ def cpu_reference_rate(ship_p, sim_p, sim, numerics, instances, t_max, threads, 
 
 # The gradient workload: gradients of a trajectory objective over 10 parameters, by the adjoint (one run forward and back
 # per point) and, beside it, by central differences (2 P + 1 = 21 runs per point, every stencil in one batch).
-GRADIENT_KINDS = ("door", "over", "down", "top")
-GRADIENT_BREACHES = 6
-GRADIENT_SEED = 20261205
-
-
-def gradient_space(sim):
-    """The gradient workload's 10 parameters: log scale factors of the door, overflow, deck-opening and
-    weather-deck-opening connections, then the areas (m2) of the first six open breaches."""
-    import numpy as np
-
-    from sinksim_b200.calibrate import ParamSpace
-
-    names = list(sim["kindNames"])
-    kind, en = np.asarray(sim["kind"]), np.asarray(sim["en"])
-    breaches = np.nonzero((kind == names.index("breach")) & (en != 0))[0][:GRADIENT_BREACHES]
-    return ParamSpace(sim, kinds=GRADIENT_KINDS, conns=[int(c) for c in breaches])
-
-
-def gradient_point(space, i):
-    """Point i of the seeded stream (i = -1: the hidden point behind the target trajectory): kind log scales N(0, 0.3)
-    (lognormal(0, 0.3) factors), breach areas U(0.1, 0.4) m2. Each point has its own generator, so a rank's block of
-    points does not depend on the number of ranks."""
-    import numpy as np
-
-    rng = np.random.default_rng([GRADIENT_SEED, i + 1])
-    nk = len(space.kinds)
-    return np.concatenate([rng.normal(0.0, 0.3, nk), rng.uniform(0.1, 0.4, space.dim - nk)])
+from sinksim_b200.calibrate import workload_point as gradient_point  # noqa: E402
+from sinksim_b200.calibrate import workload_space as gradient_space  # noqa: E402
 
 
 def gradient_times():

@@ -309,6 +309,31 @@ def value_and_grad(evaluator, objective, thetas, h_rel=DEFAULT_FD_STEP, ranks=No
     return fd_reduce(thetas, vals, h_rel)
 
 
+# ------------------------------------------------------------------------------------------ the configurations' parameters
+
+WORKLOAD_KINDS = ("door", "over", "down", "top")
+WORKLOAD_BREACHES = 6
+WORKLOAD_SEED = 20261205
+
+
+def workload_space(sim):
+    """The 10 parameters of the gradient and calibration configurations: log scale factors of the door, overflow,
+    deck-opening and weather-deck-opening connections, then the areas (m2) of the first six open breaches."""
+    names = list(sim["kindNames"])
+    kind, en = np.asarray(sim["kind"]), np.asarray(sim["en"])
+    breaches = np.nonzero((kind == names.index("breach")) & (en != 0))[0][:WORKLOAD_BREACHES]
+    return ParamSpace(sim, kinds=WORKLOAD_KINDS, conns=[int(c) for c in breaches])
+
+
+def workload_point(space, i, seed=WORKLOAD_SEED):
+    """Point i of the seeded stream (i = -1: the hidden point behind the target trajectory): kind log scales N(0, 0.3)
+    (lognormal(0, 0.3) factors), breach areas U(0.1, 0.4) m2. Each point has its own generator, so a block of points
+    does not depend on how many there are."""
+    rng = np.random.default_rng([seed, i + 1])
+    nk = len(space.kinds)
+    return np.concatenate([rng.normal(0.0, 0.3, nk), rng.uniform(0.1, 0.4, space.dim - nk)])
+
+
 # ------------------------------------------------------------------------------------------ gradients by the adjoint
 
 class AdjointEvaluator:
@@ -645,7 +670,17 @@ def main(argv=None):
                          "with the L-BFGS state on the GPU (torch)")
     ap.add_argument("--rel-target", type=float, default=None, help="stop a restart once its objective falls below this fraction of its start")
     ap.add_argument("--t-end", type=float, default=7920.0, help="s: the last of the 8 objective times")
+    ap.add_argument("--liner", action="store_true", help="the generated benchmark liner (hullgen) instead of titanic64")
+    ap.add_argument("--space", default="kinds", choices=("kinds", "workload"),
+                    help="kinds: log scales of breach/over/down/top; workload: the configurations' 10 parameters "
+                         "(door/over/down/top log scales and the six open breaches' areas, points drawn as the configurations do)")
     args = ap.parse_args(argv)
+    if args.liner:
+        import tempfile
+
+        from . import hullgen
+
+        args.ship, args.sim = hullgen.write(os.path.join(tempfile.gettempdir(), "sinksim_b200_liner"))
     ship, sim = _model_paths(args)
     if args.mode == "search":
         if not args.observations:
@@ -667,11 +702,27 @@ def main(argv=None):
     ranks = Ranks(backend="nccl")
     times = default_times(args.t_end)
     rng = np.random.default_rng(args.seed)
-    ev = BatchEvaluator(ship, sim, numerics=args.numerics, t_max=times[-1], curve_every=times[1] - times[0], device=ranks.local)
-    hidden = rng.normal(0.0, 0.3, size=ev.space.dim)
+    space = None
+    if args.space == "workload":
+        from .files import load_model
+
+        space = workload_space(load_model(ship, sim)[1])
+    ev = BatchEvaluator(ship, sim, space=space, numerics=args.numerics, t_max=times[-1], curve_every=times[1] - times[0], device=ranks.local)
+    if args.space == "workload":
+        # fresh hidden parameters (the stream's points beyond the gradient workload's) and starts from the same law
+        hidden = workload_point(ev.space, 10_000 + args.seed % 1000)
+        x0 = np.stack([workload_point(ev.space, 20_000 + k) for k in range(args.restarts)])
+    else:
+        hidden = rng.normal(0.0, 0.3, size=ev.space.dim)
+        x0 = rng.normal(0.0, 0.3, size=(args.restarts, ev.space.dim))
     target = TrajectoryObjective.from_target(ev.run(hidden[None, :])[0], times)
-    x0 = rng.normal(0.0, 0.3, size=(args.restarts, ev.space.dim))
     t0 = time.time()
+    trace = []  # (wall s, best objective so far) after every evaluation
+
+    def note(f):
+        best_now = float(np.min(np.asarray(f)))
+        trace.append((time.time() - t0, min(best_now, trace[-1][1]) if trace else best_now))
+
     if args.gradient == "adjoint":
         import torch
 
@@ -680,6 +731,7 @@ def main(argv=None):
 
         def fg(X):
             f, g, _ = adj.value_and_grad(X.cpu().numpy(), target)
+            note(f)
             return torch.as_tensor(f, device=dev), torch.as_tensor(g, device=dev)
 
         xt, ft, info = lbfgs_device(fg, x0, max_iter=args.iters, rel_target=args.rel_target, device=dev)
@@ -687,15 +739,28 @@ def main(argv=None):
         ev.device_ms += adj.device_ms
         ev.instances += adj.instances
     else:
-        x, fx, info = lbfgs_batched(lambda X: value_and_grad(ev, target, X, args.h, ranks=ranks), x0, max_iter=args.iters)
+        def fg_fd(X):
+            f, g = value_and_grad(ev, target, X, args.h, ranks=ranks)
+            note(f)
+            return f, g
+
+        x, fx, info = lbfgs_batched(fg_fd, x0, max_iter=args.iters)
     wall = ranks.max(time.time() - t0)
     device_s = ranks.max(ev.device_ms / 1e3)
     instances = ranks.sum(float(ev.instances))
     best = int(np.argmin(fx))
     if ranks.rank == 0:
-        print(json.dumps({"gradient": args.gradient, "restarts": args.restarts, "gpus": ranks.world, "best_objective": float(fx[best]),
-                          "recovery_error": float(np.max(np.abs(x[best] - hidden))), "evaluations": info["evaluations"],
-                          "instances": instances, "wall_s": wall, "device_s": device_s}))
+        # the relative objective: the best objective over the best of the starting points'
+        start = trace[0][1]
+        reached = {}
+        for level in (1e-2, 1e-4, 1e-6):
+            hit = next((t for t, b in trace if b <= level * start), None)
+            reached[f"{level:g}"] = hit
+        print(json.dumps({"gradient": args.gradient, "restarts": args.restarts, "gpus": ranks.world, "space": args.space,
+                          "best_objective": float(fx[best]), "start_objective": start, "relative_objective": float(fx[best]) / start,
+                          "wall_s_to_relative": reached, "recovery_error": float(np.max(np.abs(x[best] - hidden))),
+                          "hidden": [float(v) for v in hidden], "best_point": [float(v) for v in x[best]],
+                          "evaluations": info["evaluations"], "instances": instances, "wall_s": wall, "device_s": device_s}))
     ranks.close()
     return 0
 

@@ -152,7 +152,7 @@ float AdjointBatch::run() {
   const ModelDev& m = *I.model;
   const int W = teamWarps_;
   const SlotLayout SL = I.slot_for(W);
-  const AdjLayout AL = adjoint_layout(m.NN, m.NC, I.nsamples, W);
+  const AdjLayout AL = adjoint_layout(m.NN, m.NC, m.NG, I.nsamples, W);
   const std::size_t smem = static_cast<std::size_t>(SL.bytes) + AL.bytes;
   if (smem > I.info.sharedPerBlockOptIn)
     throw std::runtime_error("AdjointBatch: a team needs " + std::to_string(smem) + " bytes of shared memory, the device allows " +

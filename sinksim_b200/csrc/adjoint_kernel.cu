@@ -111,6 +111,7 @@ struct AdjSmem {
   adj::AdjState as;
   double* grad;      // [nc]
   double* sampleS;   // [nsamples] state index of each sample (as doubles)
+  unsigned char* tape;  // one step's tape, staged for its reverse
 };
 
 __device__ __forceinline__ AdjSmem carve_adjoint(unsigned char* base, const AdjLayout& A) {
@@ -126,6 +127,7 @@ __device__ __forceinline__ AdjSmem carve_adjoint(unsigned char* base, const AdjL
   m.as.aVol = d(A.aVol); m.as.aLevel = d(A.aLevel); m.as.aCx = d(A.aCx); m.as.aCy = d(A.aCy); m.as.aCz = d(A.aCz);
   m.grad = d(A.grad);
   m.sampleS = d(A.sampleS);
+  m.tape = base + A.tape;
   return m;
 }
 
@@ -283,7 +285,19 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
       T.sync();
       for (long long st = s1 - 1; st >= s0; --st) {
         const adj::Tape tp = adj::tape_at(tapes + static_cast<std::size_t>(st - s0) * TL.bytes, TL);
-        adj::reverse_step(AT, M, tp, I.en(), I.area(), I.tOn(), A.rs, A.as, aSc, A.grad, &err);
+        // the step's tape into shared memory before its reverse reads it (the replay of the level solve and the
+        // reverse read every record several times, in dependent chains): the state and solved arrays, the integers,
+        // and of the pass records only the slots the step used
+        const adj::Tape sp = adj::tape_at(A.tape, TL);
+        for (std::size_t i = T.rank; i < TL.passes; i += 32 * W) sp.d[i] = tp.d[i];
+        for (std::size_t i = T.rank; i < TL.ints; i += 32 * W) sp.i[i] = tp.i[i];
+        T.sync();
+        for (int i = T.rank; i < M.nn * adj::kMaxPasses * adj::kPassFields; i += 32 * W) {
+          const int n = i / (adj::kMaxPasses * adj::kPassFields), k = (i / adj::kPassFields) % adj::kMaxPasses;
+          if (k < sp.i[TL.npass + n]) sp.d[TL.passes + i] = tp.d[TL.passes + i];
+        }
+        T.sync();
+        adj::reverse_step(AT, M, sp, I.en(), I.area(), I.tOn(), A.rs, A.as, aSc, A.grad, &err);
         for (int q = 0; q < NS; ++q)
           if (static_cast<long long>(A.sampleS[q]) == st) {
             const double tr = B.trim[static_cast<std::size_t>(inst) * NS + q], hv = B.heave[static_cast<std::size_t>(inst) * NS + q];
@@ -301,7 +315,7 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
 
 }  // namespace
 
-AdjLayout adjoint_layout(int nn, int nc, int nsamples, int W) {
+AdjLayout adjoint_layout(int nn, int nc, int ng, int nsamples, int W) {
   AdjLayout A{};
   std::uint32_t off = 0;
   auto take16 = [&](std::size_t bytes) {
@@ -321,6 +335,7 @@ AdjLayout adjoint_layout(int nn, int nc, int nsamples, int W) {
   A.aVol = take16(N); A.aLevel = take16(N); A.aCx = take16(N); A.aCy = take16(N); A.aCz = take16(N);
   A.grad = take16(C);
   A.sampleS = take16(sizeof(double) * static_cast<std::size_t>(std::max(nsamples, 1)));
+  A.tape = take16(adj::tape_layout(nn, ng).bytes);
   A.bytes = off;
   return A;
 }

@@ -41,10 +41,10 @@ struct AdjRun {
 // Byte offsets of a team's reverse arrays in shared memory, after its forward slot.
 struct AdjLayout {
   std::uint32_t hEff, aEff, dV, volPost, deg, clip, aVolPost, aCxs, aCys, aCzs, aVs, aAcc, aZmx, aLs, aAs, faHA, faHB, faAA, faAB, red;
-  std::uint32_t aVol, aLevel, aCx, aCy, aCz, grad, sampleS, bytes;
+  std::uint32_t aVol, aLevel, aCx, aCy, aCz, grad, sampleS, tape, bytes;
 };
 
-AdjLayout adjoint_layout(int nn, int nc, int nsamples, int teamWarps);
+AdjLayout adjoint_layout(int nn, int nc, int ng, int nsamples, int teamWarps);
 std::size_t adjoint_tape_bytes(int nn, int ng);
 cudaError_t configure_adjoint_kernel(int teamWarps, std::size_t smem);
 cudaError_t adjoint_occupancy(int teamWarps, std::size_t smem, int* blocksPerSM);
