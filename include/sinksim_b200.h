@@ -275,6 +275,10 @@ int ssb_adjoint_run(ssb_adjoint* a, double* J, double* grad, int64_t* steps, int
 int ssb_adjoint_samples(const ssb_adjoint* a, double* trim, double* heave);
 /* Connections, team size and teams of the last run; bytes sent to and read back from the device in the last run. */
 int ssb_adjoint_info(const ssb_adjoint* a, int32_t* connections, int32_t* team_warps, int32_t* teams, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
+/* Where the last run's time went, per instance (count x 3, row-major, nanoseconds of the device's global timer while
+ * the instance's team worked on it): the forward run with its checkpoints, the recomputation of segments from their
+ * checkpoints, the reverse steps. */
+int ssb_adjoint_phase_times(const ssb_adjoint* a, int64_t* ns);
 
 /* Measured rate of separately rounded adds and multiplies on the device (fp64 = 1: double, 0: float), the
  * denominator of the engine's roofline; operations per second through *ops_per_s. No counterpart in the reference. */

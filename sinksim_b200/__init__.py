@@ -111,6 +111,7 @@ _SIGNATURES = {
     "ssb_adjoint_set_objective": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ssb_adjoint_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_float)]),
     "ssb_adjoint_samples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ssb_adjoint_phase_times": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ssb_adjoint_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint64),
                                    C.POINTER(C.c_uint64)]),
     "ssb_check_model": (C.c_int, [C.c_char_p, C.c_char_p]),
@@ -481,6 +482,12 @@ class Adjoint:
         hv = np.empty((self.count, self.nsamples))
         _check(lib().ssb_adjoint_samples(self._h, tr.ctypes.data, hv.ctypes.data))
         return tr, hv
+
+    def phase_times(self):
+        """The last run's time per instance [count, 3] in seconds of its team: forward, recomputation, reverse."""
+        ns = np.empty((self.count, 3), dtype=np.int64)
+        _check(lib().ssb_adjoint_phase_times(self._h, ns.ctypes.data))
+        return ns * 1e-9
 
     def info(self):
         nc, w, t = C.c_int32(), C.c_int32(), C.c_int32()

@@ -26,11 +26,11 @@ struct AdjointBatch::Impl {
   DevBuf<std::uint8_t> en;
   DevBuf<double> area, tOn, st, vol, level, cx, cy, cz, times, trimT, heaveT, trim, heave, J, grad, ckpt, sink;
   DevBuf<unsigned char> tape;
-  DevBuf<long long> steps;
+  DevBuf<long long> steps, phase;
   DevBuf<std::int32_t> error, queue, isink;
   // results
   std::vector<double> rJ, rGrad, rTrim, rHeave;
-  std::vector<long long> rSteps;
+  std::vector<long long> rSteps, rPhase;
   std::vector<std::int32_t> rError;
   bool ran = false;
   std::size_t up = 0, down = 0;
@@ -179,7 +179,7 @@ float AdjointBatch::run() {
                                           I.hTrimT.size() + I.hHeaveT.size());
   // outputs and per-team memory
   I.trim.alloc(count * NS); I.heave.alloc(count * NS); I.J.alloc(count); I.grad.alloc(count * static_cast<std::size_t>(m.NC));
-  I.steps.alloc(count);
+  I.steps.alloc(count); I.phase.alloc(3 * count);
   I.error.alloc(count); check(cudaMemsetAsync(I.error.get(), 0, I.error.bytes(), s), "memset");
   I.queue.alloc(1); check(cudaMemsetAsync(I.queue.get(), 0, I.queue.bytes(), s), "memset");
   I.ckpt.alloc(static_cast<std::size_t>(teams_) * maxCkpt * recSize);
@@ -197,6 +197,7 @@ float AdjointBatch::run() {
   R.trim = I.trim.get(); R.heave = I.heave.get(); R.J = I.J.get(); R.grad = I.grad.get(); R.steps = I.steps.get();
   R.error = I.error.get(); R.queue = I.queue.get();
   R.K = K; R.maxCkpt = maxCkpt; R.ckpt = I.ckpt.get(); R.tape = I.tape.get(); R.sink = I.sink.get(); R.isink = I.isink.get();
+  R.phaseNs = I.phase.get();
   check(cudaEventRecord(I.ev0, s), "cudaEventRecord");
   check(launch_adjoint_kernel(W, m.dm, R, SL, AL, teams_, s), "adjoint kernel launch");
   check(cudaEventRecord(I.ev1, s), "cudaEventRecord");
@@ -204,9 +205,9 @@ float AdjointBatch::run() {
   float ms = 0;
   check(cudaEventElapsedTime(&ms, I.ev0, I.ev1), "cudaEventElapsedTime");
   I.J.download(I.rJ, s); I.grad.download(I.rGrad, s); I.trim.download(I.rTrim, s); I.heave.download(I.rHeave, s);
-  I.steps.download(I.rSteps, s); I.error.download(I.rError, s);
+  I.steps.download(I.rSteps, s); I.error.download(I.rError, s); I.phase.download(I.rPhase, s);
   check(cudaStreamSynchronize(s), "copy to host");
-  I.down = I.J.bytes() + I.grad.bytes() + I.trim.bytes() + I.heave.bytes() + I.steps.bytes() + I.error.bytes();
+  I.down = I.J.bytes() + I.grad.bytes() + I.trim.bytes() + I.heave.bytes() + I.steps.bytes() + I.error.bytes() + I.phase.bytes();
   I.ran = true;
   return ms;
 }
@@ -245,6 +246,12 @@ std::int32_t AdjointBatch::error(std::int32_t inst) const {
   if (!I_->ran) throw std::logic_error("AdjointBatch: results before run");
   check_inst(opt_.count, inst);
   return I_->rError[static_cast<std::size_t>(inst)];
+}
+
+const long long* AdjointBatch::phase_ns(std::int32_t inst) const {
+  if (!I_->ran) throw std::logic_error("AdjointBatch: results before run");
+  check_inst(opt_.count, inst);
+  return &I_->rPhase[3 * static_cast<std::size_t>(inst)];
 }
 
 std::size_t AdjointBatch::upload_bytes() const { return I_->up; }

@@ -49,6 +49,8 @@ class AdjointBatch {
   const double* samples_heave(std::int32_t inst) const;
   std::int64_t steps(std::int32_t inst) const;
   std::int32_t error(std::int32_t inst) const;
+  // the team's time on the instance in the last run, ns: forward, recomputation of the segments, reverse steps
+  const long long* phase_ns(std::int32_t inst) const;
   std::size_t upload_bytes() const;
   std::size_t download_bytes() const;
 

@@ -158,6 +158,12 @@ __device__ __forceinline__ void load_state(const double* c, SimRegs& R, Slot& S,
   T.sync();
 }
 
+__device__ __forceinline__ long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return static_cast<long long>(t);
+}
+
 // The objective's adjoint at the state with scalars (zO, pitch, roll): every thread adds the same values.
 __device__ __forceinline__ void add_sample_adjoint(const DevModel& M, double zO, double th, double ph, double aTrim, double aHeave, double* aSc) {
   const PoseD F = adj::pose_of(M, zO, th, ph);
@@ -192,6 +198,8 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
     const int inst = S.misc[0];
     T.sync();
     if (inst >= B.count) return;
+    const long long tStart = global_ns();
+    long long tRecompute = 0, tReverse = 0;
     const std::size_t ic = static_cast<std::size_t>(inst) * M.nc;
     const AdjInst I{B.en + ic, B.area + ic, B.tOn + ic, sink, isink, M.nmon};
     // the event bookkeeping sinks: overflow and mark times set (nothing fires), so events never write
@@ -251,6 +259,7 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
     }
     __threadfence_block();
     T.sync();
+    const long long tForward = global_ns() - tStart;
     // ---- 2. reverse
     double aSc[6] = {0, 0, 0, 0, 0, 0};
     for (int n = T.rank; n < M.nn; n += 32 * W) { A.as.aVol[n] = 0; A.as.aLevel[n] = 0; A.as.aCx[n] = 0; A.as.aCy[n] = 0; A.as.aCz[n] = 0; }
@@ -266,6 +275,7 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
     const long long nseg = (S_end + B.K - 1) / B.K;
     for (long long g = nseg - 1; g >= 0; --g) {
       const long long s0 = g * B.K, s1 = (s0 + B.K < S_end) ? s0 + B.K : S_end;
+      const long long tSeg = global_ns();
       load_state(ckpt + static_cast<std::size_t>(g) * recSize, R, S, M, T);
       F = make_pose(M, R.zO, R.pitch, R.roll);
       for (long long st = s0; st < s1; ++st) {
@@ -283,6 +293,8 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
       }
       __threadfence_block();
       T.sync();
+      const long long tRev = global_ns();
+      tRecompute += tRev - tSeg;
       for (long long st = s1 - 1; st >= s0; --st) {
         const adj::Tape tp = adj::tape_at(tapes + static_cast<std::size_t>(st - s0) * TL.bytes, TL);
         // the step's tape into shared memory before its reverse reads it (the replay of the level solve and the
@@ -304,11 +316,17 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
             add_sample_adjoint(M, tp.d[TL.scal + 1], tp.d[TL.scal + 2], tp.d[TL.scal + 3], 2 * (tr - trimT[q]), 2 * (hv - heaveT[q]), aSc);
           }
       }
+      tReverse += global_ns() - tRev;
     }
     T.sync();
     for (int c = T.rank; c < M.nc; c += 32 * W) B.grad[ic + c] = A.grad[c];
     if (err) atomicOr(B.error + inst, err);
-    if (T.leader()) { B.J[inst] = J; B.steps[inst] = S_end; }
+    if (T.leader()) {
+      B.J[inst] = J; B.steps[inst] = S_end;
+      B.phaseNs[3 * static_cast<std::size_t>(inst)] = tForward;
+      B.phaseNs[3 * static_cast<std::size_t>(inst) + 1] = tRecompute;
+      B.phaseNs[3 * static_cast<std::size_t>(inst) + 2] = tReverse;
+    }
     T.sync();
   }
 }

@@ -36,6 +36,8 @@ struct AdjRun {
   unsigned char* tape;                          // [teams x K x tape bytes]
   double* sink;                                 // [teams x (evCap + nmon + nmark + 1)]
   std::int32_t* isink;                          // [teams x (evCap + 1)]
+  long long* phaseNs;                           // [count x 3] the team's time on the instance (globaltimer ns):
+                                                // forward, recomputation of the segments, reverse steps
 };
 
 // Byte offsets of a team's reverse arrays in shared memory, after its forward slot.

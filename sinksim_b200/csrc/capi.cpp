@@ -628,6 +628,14 @@ int ssb_adjoint_info(const ssb_adjoint* a, int32_t* connections, int32_t* team_w
   });
 }
 
+int ssb_adjoint_phase_times(const ssb_adjoint* a, int64_t* ns) {
+  return guard([&] {
+    need(a, "adjoint"); need(ns, "ns");
+    const int32_t n = a->adj->count();
+    for (int32_t i = 0; i < n; ++i) std::memcpy(ns + 3 * static_cast<std::size_t>(i), a->adj->phase_ns(i), 3 * sizeof(int64_t));
+  });
+}
+
 int ssb_check_model(const char* ship_path, const char* sim_path) {
   return guard([&] {
     need(ship_path, "ship_path"); need(sim_path, "sim_path");
