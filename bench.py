@@ -69,7 +69,9 @@ def parse():
     ap.add_argument("--hulls", type=int, default=2048, help="fleet: hulls per GPU (one instance each)")
     ap.add_argument("--fleet-tmax", type=float, default=7200.0, help="fleet: s; instances also stop when they founder or calm down")
     ap.add_argument("--points", type=int, default=256, help="gradient: parameter points per GPU (one gradient each)")
-    ap.add_argument("--fd-steps", type=int, default=1, help="gradient: timed calls of the finite-difference arm")
+    ap.add_argument("--fd-steps", type=int, default=1, help="gradient: timed calls of the finite-difference arm (0: none)")
+    ap.add_argument("--t-end", type=float, default=7920.0, help="gradient: s, the last of the objective's 8 times and the runs' end")
+    ap.add_argument("--tape-gb", type=float, default=0.0, help="gradient: device memory for the adjoint's step records (0: chosen)")
     ap.add_argument("--autotune", action="store_true", help="pick the launch shape by timing candidates first (outside the timed region)")
     args = ap.parse_args()
     if args.model is None:
@@ -293,11 +295,12 @@ from sinksim_b200.calibrate import workload_point as gradient_point  # noqa: E40
 from sinksim_b200.calibrate import workload_space as gradient_space  # noqa: E402
 
 
-def gradient_times():
-    """The objective's 8 times, 990 s apart, to 2.2 h (7,920 s), and the curve interval that records exactly them."""
+def gradient_times(t_end=7920.0):
+    """The objective's 8 times, evenly spaced to t_end (by default 990 s apart, to 2.2 h), and the curve interval
+    that records exactly them."""
     from sinksim_b200.calibrate import default_times
 
-    times = default_times()
+    times = default_times(t_end)
     return times, times[1] - times[0]
 
 
@@ -404,16 +407,17 @@ def reference_gradient_arm(args, ship_p, sim_p, sim, threads):
 
 def workload_config(args):
     if args.workload == "gradient":
-        return {"workload": f"central-difference gradients of a trajectory objective on {args.model}, {args.points} points per GPU",
+        return {"workload": f"gradients of a trajectory objective on {args.model}, {args.points} points per GPU, by the adjoint",
                 "model": MODELS[args.model], "global_batch": args.points * args.gpus,
                 "parameters": "10: log scale factors of the door, overflow, deck-opening and weather-deck-opening connections; "
                               "areas of the first 6 open breaches",
                 "points": "kind scales lognormal(0, 0.3), breach areas U(0.1, 0.4) m2 (seeded); the target trajectory is the run at "
                           "a hidden point from the same distribution",
-                "objective": "sum of squared trim (deg) and heave (m) residuals at 8 times, 990 s apart, to 7,920 s",
-                "gradient": "hand-written FP64 discrete adjoint, checkpoints every 256 steps, one run forward and back per gradient; "
+                "objective": f"sum of squared trim (deg) and heave (m) residuals at 8 times, evenly spaced to {args.t_end:g} s",
+                "gradient": "hand-written FP64 discrete adjoint, one run forward (packed step records kept in HBM, checkpoints every "
+                            "256 steps for what the records' memory does not hold) and back per gradient; "
                             "finite-difference arm beside it: central differences, relative step 1e-2, 21 runs per gradient",
-                "numerics": args.numerics, "t_max_s": 7920.0, "dt_s": 0.25, "retire": "founder | tMax",
+                "numerics": args.numerics, "t_max_s": args.t_end, "dt_s": 0.25, "retire": "founder | tMax",
                 "parallelism": f"points sharded over {args.gpus} GPU(s), no collective in the step",
                 "l2": "working set (geometry 0.6 MB, per-instance state) is L2-resident by design; every step is a full batch from initial state"}
     if args.workload == "fleet":
@@ -448,10 +452,10 @@ def gradient_bench(args):
     ship_p, sim_p = model_paths(args.model)
     ship, sim = load_model(ship_p, sim_p)
     space = gradient_space(sim)
-    times, every = gradient_times()
+    times, every = gradient_times(args.t_end)
     ev = BatchEvaluator(ship_p, sim_p, space=space, numerics="portable", t_max=times[-1], curve_every=every, device=local)
     target = TrajectoryObjective.from_target(ev.run(gradient_point(space, -1)[None, :])[0], times)
-    adj = AdjointEvaluator(ship_p, sim_p, space=space, t_max=times[-1], device=local)
+    adj = AdjointEvaluator(ship_p, sim_p, space=space, t_max=times[-1], device=local, tape_budget=int(args.tape_gb * 2 ** 30))
     first, _ = shard_bounds(args.points * world, world, rank)
     thetas = np.stack([gradient_point(space, first + k) for k in range(args.points)])
     for _ in range(args.warmup):
@@ -476,7 +480,8 @@ def gradient_bench(args):
             fwd_ms.append(ev.last["device_ms"])
     # the finite-difference arm: every point's 21 runs in one batch
     fd_ms, fd_s = 0.0, 0.0
-    value_and_grad(ev, target, thetas[: max(1, args.points)], DEFAULT_FD_STEP)
+    if args.fd_steps:
+        value_and_grad(ev, target, thetas, DEFAULT_FD_STEP)
     for _ in range(args.fd_steps):
         t0 = time.perf_counter()
         value_and_grad(ev, target, thetas, DEFAULT_FD_STEP)
@@ -484,8 +489,9 @@ def gradient_bench(args):
         fd_ms += ev.last["device_ms"]
     dev_s_max = ranks.max(dev_ms / 1e3)
     e2e_max = ranks.max(e2e_s)
-    fd_dev_max = ranks.max(fd_ms / 1e3)
-    fd_e2e_max = ranks.max(fd_s)
+    fd_dev_max = ranks.max(fd_ms / 1e3) if args.fd_steps else None
+    fd_e2e_max = ranks.max(fd_s) if args.fd_steps else None
+    recomputed = ranks.sum(float(adj.last["recomputed"]))
     fwd_max = ranks.max(min(fwd_ms) / 1e3)
     grads = ranks.sum(float(args.points * args.steps))
     fd_grads = ranks.sum(float(args.points * args.fd_steps))
@@ -500,10 +506,11 @@ def gradient_bench(args):
             ops_per_step = estimated_ops_per_step(len(ship["x"]), len(ship["segCol"]), len(ship["segCount"]), len(sim["ca"]))
             ops_source = "estimated from the model's size with titanic64's per-step ratios"
         adjoint_s = dev_s_max / args.steps
-        # the kernel steps every run three times (forward with checkpoints, recompute with the tape, reverse); the
-        # reverse of a step sweeps the same geometry as its forward (the node passes' and columns' reverses), so each is
-        # counted as one step's FP64 work
-        achieved = 3 * ops_per_step * (all_steps / args.steps) / adjoint_s
+        # the kernel steps every run forward (recording every step), reverses every step and recomputes the steps its
+        # ring of records no longer holds; the reverse of a step sweeps the same geometry as its forward (the node
+        # passes' and columns' reverses), so each counts as one step's FP64 work
+        step_equivalents = 2 * all_steps / args.steps + recomputed
+        achieved = ops_per_step * step_equivalents / adjoint_s
         n_params = space.dim
         out = {"metric": "gradients/s", "value": grads / dev_s_max, "unit": "gradients/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": dev_s_max * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -513,13 +520,17 @@ def gradient_bench(args):
                "gpu_launches": args.steps, "adjoint": {"team_warps": info["team_warps"], "teams": info["teams"], "checkpoint_every": 256,
                                                       "device_s_per_call": adjoint_s, "forward_run_s": fwd_max,
                                                       "cost_in_forward_runs": adjoint_s / fwd_max,
-                                                      "sim_steps_per_run": all_steps / args.steps},
-               "finite_difference_arm": {"value": fd_grads / fd_dev_max, "unit": "gradients/s", "e2e": fd_grads / fd_e2e_max,
-                                         "runs_per_gradient": 2 * n_params + 1, "relative_step": DEFAULT_FD_STEP, "calls": args.fd_steps},
+                                                      "sim_steps_per_run": all_steps / args.steps, "recomputed_steps": recomputed,
+                                                      "ring_mb_per_team": adj.last["ring_bytes"] / 2 ** 20,
+                                                      "team_s": dict(zip(("forward", "recompute", "reverse"), adj.last["phase_team_s"]))},
+               "finite_difference_arm": None if not args.fd_steps else {
+                   "value": fd_grads / fd_dev_max, "unit": "gradients/s", "e2e": fd_grads / fd_e2e_max,
+                   "runs_per_gradient": 2 * n_params + 1, "relative_step": DEFAULT_FD_STEP, "calls": args.fd_steps},
                "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
                             "frac": achieved / fp64_peak, "traffic": None, "ops_source": ops_source,
                             "kernel": f"adjoint_batch<{info['team_warps']}-warp teams>",
-                            "work": "3 step-equivalents per sim-step (forward, recompute, reverse)",
+                            "work": f"{step_equivalents:.0f} step-equivalents per call (forward and reverse of every sim-step, "
+                                    f"plus {recomputed:.0f} recomputed)",
                             "peak_source": "measured on this GPU: separately rounded FP64 add+mul microbenchmark (no FMA, as the bits require)",
                             "ops_per_sim_step": ops_per_step},
                "clocks": clk}

@@ -268,6 +268,14 @@ int ssb_adjoint_set_connection_areas(ssb_adjoint* a, int32_t first, int32_t coun
                                      const double* areas);
 /* n sample times (ascending) and the targets trim[i * n + k], heave[i * n + k] of every instance. */
 int ssb_adjoint_set_objective(ssb_adjoint* a, int32_t n, const double* times, const double* trim, const double* heave);
+/* Memory for step records, all teams together, in bytes. A team keeps the records of its run's last steps in a ring
+ * of budget / teams bytes, at least one segment (checkpoint_every records of the largest size); the reverse recomputes
+ * from its checkpoint only a segment the ring no longer holds. 0, the default: room for a whole run of t_max with two
+ * level passes per node (about 15 KB a step on a 64-space model), within half the device memory free at the next run.
+ * The results do not depend on it. */
+int ssb_adjoint_set_tape_budget(ssb_adjoint* a, uint64_t bytes);
+/* The ring of each team in the last run, in bytes. */
+int ssb_adjoint_ring_bytes(const ssb_adjoint* a, uint64_t* bytes);
 /* Runs every instance forward and back. J (count), grad (count x connections, row-major), steps (count) and error
  * (count; nonzero where a step took a branch without an adjoint) may be NULL; device_ms receives the kernel's time. */
 int ssb_adjoint_run(ssb_adjoint* a, double* J, double* grad, int64_t* steps, int32_t* error, float* device_ms);
@@ -279,6 +287,8 @@ int ssb_adjoint_info(const ssb_adjoint* a, int32_t* connections, int32_t* team_w
  * the instance's team worked on it): the forward run with its checkpoints, the recomputation of segments from their
  * checkpoints, the reverse steps. */
 int ssb_adjoint_phase_times(const ssb_adjoint* a, int64_t* ns);
+/* Steps each instance recomputed from its checkpoints in the last run (count): 0 when its ring held the whole run. */
+int ssb_adjoint_recomputed_steps(const ssb_adjoint* a, int64_t* steps);
 
 /* Measured rate of separately rounded adds and multiplies on the device (fp64 = 1: double, 0: float), the
  * denominator of the engine's roofline; operations per second through *ops_per_s. No counterpart in the reference. */

@@ -112,6 +112,9 @@ _SIGNATURES = {
     "ssb_adjoint_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_float)]),
     "ssb_adjoint_samples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "ssb_adjoint_phase_times": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ssb_adjoint_set_tape_budget": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "ssb_adjoint_recomputed_steps": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ssb_adjoint_ring_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "ssb_adjoint_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint64),
                                    C.POINTER(C.c_uint64)]),
     "ssb_check_model": (C.c_int, [C.c_char_p, C.c_char_p]),
@@ -425,7 +428,7 @@ class Adjoint:
     sum_k (trim_k - trim_target[i, k])^2 + (heave_k - heave_target[i, k])^2 at the sample times, and run() returns it
     with its gradient with respect to every connection area."""
 
-    def __init__(self, ship_path, sim_path, count=1, t_max=7920.0, checkpoint_every=256, team_warps=0, device=0):
+    def __init__(self, ship_path, sim_path, count=1, t_max=7920.0, checkpoint_every=256, team_warps=0, device=0, tape_budget=0):
         h = C.c_void_p()
         _check(lib().ssb_adjoint_create(_b(ship_path), _b(sim_path), count, float(t_max), checkpoint_every, team_warps, device, C.byref(h)))
         self._h = h
@@ -434,6 +437,25 @@ class Adjoint:
         _check(lib().ssb_adjoint_info(self._h, C.byref(nc), None, None, None, None))
         self.connections = nc.value
         self.nsamples = 0
+        if tape_budget:
+            self.set_tape_budget(tape_budget)
+
+    def set_tape_budget(self, nbytes):
+        """Device memory for step records, all teams together (0: a whole run's, within half the free memory at the
+        next run); see ssb_adjoint_set_tape_budget. The results do not depend on it."""
+        _check(lib().ssb_adjoint_set_tape_budget(self._h, int(nbytes)))
+
+    def recomputed_steps(self):
+        """Steps each instance recomputed from its checkpoints in the last run [count]."""
+        n = np.empty(self.count, dtype=np.int64)
+        _check(lib().ssb_adjoint_recomputed_steps(self._h, n.ctypes.data))
+        return n
+
+    def ring_bytes(self):
+        """Each team's ring of step records in the last run, bytes."""
+        b = C.c_uint64()
+        _check(lib().ssb_adjoint_ring_bytes(self._h, C.byref(b)))
+        return b.value
 
     def close(self):
         if getattr(self, "_h", None):

@@ -338,8 +338,8 @@ def workload_point(space, i, seed=WORKLOAD_SEED):
 
 class AdjointEvaluator:
     """Objective and gradient of a TrajectoryObjective at many parameter points, by the engine's hand-written discrete
-    adjoint (sinksim_b200.Adjoint: the FP64 step reversed, checkpoints every `checkpoint_every` steps, recomputation
-    in between). One call runs every point forward and back on the GPU: 1 gradient per instance instead of the 2 P + 1
+    adjoint (sinksim_b200.Adjoint: the FP64 step reversed from the forward run's packed step records, kept in device
+    memory; checkpoints every `checkpoint_every` steps, and recomputation from them of what the memory does not hold). One call runs every point forward and back on the GPU: 1 gradient per instance instead of the 2 P + 1
     runs of central differences.
 
     The adjoint returns d J / d area[c] for every connection; the chain rule to theta is exact: a kind's log scale
@@ -347,13 +347,13 @@ class AdjointEvaluator:
     area parameter moves its connection's area one for one (and takes that connection out of its kind's sum, as it
     overrides the scaled area)."""
 
-    def __init__(self, ship_path, sim_path, space=None, t_max=7920.0, device=0, checkpoint_every=256):
+    def __init__(self, ship_path, sim_path, space=None, t_max=7920.0, device=0, checkpoint_every=256, tape_budget=0):
         from .files import load_model
 
         self.ship_path, self.sim_path = ship_path, sim_path
         _, self.sim = load_model(ship_path, sim_path)
         self.space = space or ParamSpace(self.sim)
-        self.t_max, self.device, self.k = float(t_max), device, checkpoint_every
+        self.t_max, self.device, self.k, self.tape_budget = float(t_max), device, checkpoint_every, tape_budget
         self._adj = None
         self.device_ms = 0.0
         self.instances = 0
@@ -365,7 +365,8 @@ class AdjointEvaluator:
         if self._adj is None or self._adj.count != count:
             if self._adj is not None:
                 self._adj.close()
-            self._adj = Adjoint(self.ship_path, self.sim_path, count=count, t_max=self.t_max, checkpoint_every=self.k, device=self.device)
+            self._adj = Adjoint(self.ship_path, self.sim_path, count=count, t_max=self.t_max, checkpoint_every=self.k, device=self.device,
+                                tape_budget=self.tape_budget)
         return self._adj
 
     def close(self):
@@ -386,7 +387,9 @@ class AdjointEvaluator:
             raise RuntimeError(f"the adjoint took a branch it does not differentiate in {int(np.count_nonzero(err))} instances (bits {sorted(set(err.tolist()))})")
         self.device_ms += ms
         self.instances += r
-        self.last = {"device_ms": ms, "steps": int(steps.sum()), "info": a.info()}
+        ph = a.phase_times()
+        self.last = {"device_ms": ms, "steps": int(steps.sum()), "info": a.info(), "recomputed": int(a.recomputed_steps().sum()),
+                     "phase_team_s": [float(v) for v in ph.sum(0)], "ring_bytes": a.ring_bytes()}
         col_of = {c: j for j, c in enumerate(cols)}
         g = np.zeros((r, self.space.dim))
         overridden = set(self.space.conns)

@@ -25,15 +25,18 @@ struct AdjointBatch::Impl {
   // device
   DevBuf<std::uint8_t> en;
   DevBuf<double> area, tOn, st, vol, level, cx, cy, cz, times, trimT, heaveT, trim, heave, J, grad, ckpt, sink;
-  DevBuf<unsigned char> tape;
-  DevBuf<long long> steps, phase;
+  DevBuf<unsigned char> arena;
+  DevBuf<long long> steps, phase, stepOff, recomputed;
   DevBuf<std::int32_t> error, queue, isink;
   // results
   std::vector<double> rJ, rGrad, rTrim, rHeave;
-  std::vector<long long> rSteps, rPhase;
+  std::vector<long long> rSteps, rPhase, rRecomputed;
   std::vector<std::int32_t> rError;
   bool ran = false;
   std::size_t up = 0, down = 0;
+  std::uint64_t tapeBudget = 0;   // bytes of the rings of all teams; 0: chosen at the first run
+  std::size_t ringBytes = 0;      // per team, as chosen
+  int ringTeams = 0;
 
   SlotLayout slot_for(int W) const {
     // the forward slot of a team of W warps, as the batch kernel lays it out for one model
@@ -179,11 +182,29 @@ float AdjointBatch::run() {
                                           I.hTrimT.size() + I.hHeaveT.size());
   // outputs and per-team memory
   I.trim.alloc(count * NS); I.heave.alloc(count * NS); I.J.alloc(count); I.grad.alloc(count * static_cast<std::size_t>(m.NC));
-  I.steps.alloc(count); I.phase.alloc(3 * count);
+  I.steps.alloc(count); I.phase.alloc(3 * count); I.recomputed.alloc(count);
   I.error.alloc(count); check(cudaMemsetAsync(I.error.get(), 0, I.error.bytes(), s), "memset");
   I.queue.alloc(1); check(cudaMemsetAsync(I.queue.get(), 0, I.queue.bytes(), s), "memset");
   I.ckpt.alloc(static_cast<std::size_t>(teams_) * maxCkpt * recSize);
-  I.tape.alloc(static_cast<std::size_t>(teams_) * K * tapeBytes);
+  I.stepOff.alloc(static_cast<std::size_t>(teams_) * (static_cast<std::size_t>(maxSteps) + 1));
+  // the rings: at least K records of the largest size per team (one segment); up to a whole run of them when memory
+  // allows. Unless the caller set a budget: a whole run of records with two passes per node (nodes take about 1.2 on
+  // average), within half the device memory free at the first run; the ring is kept for later runs.
+  const std::size_t minRing = static_cast<std::size_t>(K) * tapeBytes;
+  if (I.ringBytes == 0 || I.ringTeams != teams_) {
+    std::size_t perTeam = 0;
+    if (I.tapeBudget != 0) {
+      perTeam = static_cast<std::size_t>(I.tapeBudget / static_cast<std::uint64_t>(teams_));
+    } else {
+      std::size_t freeB = 0, totalB = 0;
+      check(cudaMemGetInfo(&freeB, &totalB), "cudaMemGetInfo");
+      const std::size_t usual = (static_cast<std::size_t>(maxSteps) + 1) * adjoint_record_bytes(m.NN, m.NG, 2 * m.NN);
+      perTeam = std::min(usual, (freeB + I.arena.bytes()) / 2 / static_cast<std::size_t>(teams_));
+    }
+    I.ringBytes = std::max(minRing, perTeam) & ~static_cast<std::size_t>(15);
+    I.ringTeams = teams_;
+  }
+  I.arena.alloc(static_cast<std::size_t>(teams_) * I.ringBytes);
   I.sink.alloc(static_cast<std::size_t>(teams_) * (m.evCap + m.nmon + m.nmark + 1));
   I.isink.alloc(static_cast<std::size_t>(teams_) * (m.evCap + 1));
   AdjRun R{};
@@ -196,8 +217,11 @@ float AdjointBatch::run() {
   R.sampleT = I.times.get(); R.trimT = I.trimT.get(); R.heaveT = I.heaveT.get();
   R.trim = I.trim.get(); R.heave = I.heave.get(); R.J = I.J.get(); R.grad = I.grad.get(); R.steps = I.steps.get();
   R.error = I.error.get(); R.queue = I.queue.get();
-  R.K = K; R.maxCkpt = maxCkpt; R.ckpt = I.ckpt.get(); R.tape = I.tape.get(); R.sink = I.sink.get(); R.isink = I.isink.get();
+  R.K = K; R.maxCkpt = maxCkpt; R.ckpt = I.ckpt.get();
+  R.arena = I.arena.get(); R.arenaBytes = I.ringBytes; R.stepOff = I.stepOff.get();
+  R.tapeForward = I.ringBytes > minRing ? 1 : 0; R.sink = I.sink.get(); R.isink = I.isink.get();
   R.phaseNs = I.phase.get();
+  R.recomputed = I.recomputed.get();
   check(cudaEventRecord(I.ev0, s), "cudaEventRecord");
   check(launch_adjoint_kernel(W, m.dm, R, SL, AL, teams_, s), "adjoint kernel launch");
   check(cudaEventRecord(I.ev1, s), "cudaEventRecord");
@@ -205,9 +229,9 @@ float AdjointBatch::run() {
   float ms = 0;
   check(cudaEventElapsedTime(&ms, I.ev0, I.ev1), "cudaEventElapsedTime");
   I.J.download(I.rJ, s); I.grad.download(I.rGrad, s); I.trim.download(I.rTrim, s); I.heave.download(I.rHeave, s);
-  I.steps.download(I.rSteps, s); I.error.download(I.rError, s); I.phase.download(I.rPhase, s);
+  I.steps.download(I.rSteps, s); I.error.download(I.rError, s); I.phase.download(I.rPhase, s); I.recomputed.download(I.rRecomputed, s);
   check(cudaStreamSynchronize(s), "copy to host");
-  I.down = I.J.bytes() + I.grad.bytes() + I.trim.bytes() + I.heave.bytes() + I.steps.bytes() + I.error.bytes() + I.phase.bytes();
+  I.down = I.J.bytes() + I.grad.bytes() + I.trim.bytes() + I.heave.bytes() + I.steps.bytes() + I.error.bytes() + I.phase.bytes() + I.recomputed.bytes();
   I.ran = true;
   return ms;
 }
@@ -253,6 +277,19 @@ const long long* AdjointBatch::phase_ns(std::int32_t inst) const {
   check_inst(opt_.count, inst);
   return &I_->rPhase[3 * static_cast<std::size_t>(inst)];
 }
+
+std::int64_t AdjointBatch::recomputed_steps(std::int32_t inst) const {
+  if (!I_->ran) throw std::logic_error("AdjointBatch: results before run");
+  check_inst(opt_.count, inst);
+  return I_->rRecomputed[static_cast<std::size_t>(inst)];
+}
+
+void AdjointBatch::set_tape_budget(std::uint64_t bytes) {
+  I_->tapeBudget = bytes;
+  I_->ringBytes = 0;
+}
+
+std::size_t AdjointBatch::ring_bytes() const { return I_->ringBytes; }
 
 std::size_t AdjointBatch::upload_bytes() const { return I_->up; }
 std::size_t AdjointBatch::download_bytes() const { return I_->down; }

@@ -51,6 +51,12 @@ class AdjointBatch {
   std::int32_t error(std::int32_t inst) const;
   // the team's time on the instance in the last run, ns: forward, recomputation of the segments, reverse steps
   const long long* phase_ns(std::int32_t inst) const;
+  std::int64_t recomputed_steps(std::int32_t inst) const;  // steps recomputed from checkpoints in the last run
+  // Bytes of step records all teams together may keep (0: a whole run's with two passes per node, within half the
+  // device memory free at the next run). With room for a whole run the reverse recomputes nothing; the least is one
+  // segment of K records per team, every segment then recomputed.
+  void set_tape_budget(std::uint64_t bytes);
+  std::size_t ring_bytes() const;  // per team, as the last run used
   std::size_t upload_bytes() const;
   std::size_t download_bytes() const;
 

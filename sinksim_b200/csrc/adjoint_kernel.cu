@@ -5,13 +5,16 @@
 // A persistent grid of teams (W warps each, one instance at a time from a work queue), per instance:
 //   1. forward: the instance runs from its initial state to tMax or its founder, exactly as the batch kernel steps it
 //      (the same team_step, so the same bits), keeping the state every K steps (a checkpoint: t, pose, rates and every
-//      node's volume, level and centroid, FP64) and the objective's readouts at the sample times;
-//   2. reverse: segment by segment, last first, the team restores the segment's checkpoint, recomputes its K steps with
-//      the tape hooks on (every node pass of the level solve, the solved levels, pose and buoyancy go to the team's
-//      tape in global memory), then runs the reverse of each step, last first (adjoint_step.cuh), adding the
-//      objective's adjoint at the sample states.
-// Memory per team: the checkpoints of one run and the tape of one segment; the adjoint of the state lives in shared
-// memory. Recomputing between checkpoints costs one more forward pass; the reverse sweep costs about one more.
+//      node's volume, level and centroid, FP64) and the objective's readouts at the sample times. With the tape hooks
+//      on (tapeForward), every step's tape (every node pass of the level solve, the solved levels, pose and buoyancy)
+//      goes to shared memory and from there, packed, into the team's ring of step records in global memory;
+//   2. reverse: segment by segment, last first. A segment whose records the ring still holds is reversed from them;
+//      any other is recomputed from its checkpoint with the tape hooks on, into the ring, first. Each step's record is
+//      unpacked into shared memory and reversed (adjoint_step.cuh), adding the objective's adjoint at the sample
+//      states.
+// Memory per team: the checkpoints of one run and the ring; the adjoint of the state lives in shared memory. When the
+// ring holds a whole run (the usual case: a packed record is about 12 KB on a 64-node model) nothing is recomputed;
+// with a ring of K records every segment is recomputed once, which costs one more forward pass.
 //
 // The objective: J = sum_k (trim(s_k) - trim*_k)^2 + (heave(s_k) - heave*_k)^2, trim in degrees and heave the mean of
 // the forward and aft drafts, where s_k is the state at which a readout curve recorded every sample time would take its
@@ -111,7 +114,8 @@ struct AdjSmem {
   adj::AdjState as;
   double* grad;      // [nc]
   double* sampleS;   // [nsamples] state index of each sample (as doubles)
-  unsigned char* tape;  // one step's tape, staged for its reverse
+  unsigned char* tape;  // one step's tape: written by the step's hooks, or unpacked from its record for its reverse
+  std::int32_t* poff;   // [nn + 1] first pass record of each node in a packed record, then their total
 };
 
 __device__ __forceinline__ AdjSmem carve_adjoint(unsigned char* base, const AdjLayout& A) {
@@ -124,10 +128,12 @@ __device__ __forceinline__ AdjSmem carve_adjoint(unsigned char* base, const AdjL
   m.rs.aAcc = d(A.aAcc); m.rs.aZmx = d(A.aZmx); m.rs.aLs = d(A.aLs); m.rs.aAs = d(A.aAs);
   m.rs.faHA = d(A.faHA); m.rs.faHB = d(A.faHB); m.rs.faAA = d(A.faAA); m.rs.faAB = d(A.faAB);
   m.rs.red = d(A.red);
+  m.rs.work = reinterpret_cast<adj::UnitWork*>(base + A.work);
   m.as.aVol = d(A.aVol); m.as.aLevel = d(A.aLevel); m.as.aCx = d(A.aCx); m.as.aCy = d(A.aCy); m.as.aCz = d(A.aCz);
   m.grad = d(A.grad);
   m.sampleS = d(A.sampleS);
   m.tape = base + A.tape;
+  m.poff = reinterpret_cast<std::int32_t*>(base + A.poff);
   return m;
 }
 
@@ -158,6 +164,103 @@ __device__ __forceinline__ void load_state(const double* c, SimRegs& R, Slot& S,
   T.sync();
 }
 
+// A packed step record: the tape's int32 (pass counts, merged flags; padded to 8 bytes), its doubles up to the pass
+// records, then only the pass records the step used, node by node (min(count, kMaxPasses) per node), the whole
+// rounded up to 16 bytes. The pass records dominate the unpacked tape (kMaxPasses slots per node), and a node takes
+// about 1.2 passes per step, so a record is about a third of the tape.
+__host__ __device__ __forceinline__ std::size_t record_ints_bytes(const adj::TapeLayout& L) {
+  return (L.ints * sizeof(std::int32_t) + 7) & ~static_cast<std::size_t>(7);
+}
+
+__host__ __device__ __forceinline__ std::size_t record_bytes(const adj::TapeLayout& L, int records) {
+  return (record_ints_bytes(L) + (L.passes + static_cast<std::size_t>(records) * adj::kPassFields) * sizeof(double) + 15) &
+         ~static_cast<std::size_t>(15);
+}
+
+// poff[n] = the first pass record of node n in the packed order, poff[nn] = their total (warp 0 scans the counts).
+template <int W>
+__device__ __forceinline__ void pass_offsets(const std::int32_t* npass, int nn, std::int32_t* poff, const Team<W>& T) {
+  if (T.warp == 0) {
+    int carry = 0;
+    for (int base = 0; base < nn; base += 32) {
+      const int n = base + T.lane;
+      const int v = n < nn ? min(npass[n], adj::kMaxPasses) : 0;
+      int x = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (T.lane >= o) x += y;
+      }
+      if (n < nn) poff[n] = carry + x - v;
+      carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (T.lane == 0) poff[nn] = carry;
+  }
+  T.sync();
+}
+
+// Packs the step's tape (shared memory) into dst (global); returns the record's bytes. Every thread of the team calls
+// it; the tape may be overwritten once it returns.
+template <int W>
+__device__ __forceinline__ std::size_t store_record(const adj::Tape& tp, int nn, std::int32_t* poff, unsigned char* dst, const Team<W>& T) {
+  const adj::TapeLayout& L = tp.L;
+  pass_offsets(tp.i + L.npass, nn, poff, T);
+  std::int32_t* di = reinterpret_cast<std::int32_t*>(dst);
+  for (std::size_t i = T.rank; i < L.ints; i += 32 * W) di[i] = tp.i[i];
+  double* dd = reinterpret_cast<double*>(dst + record_ints_bytes(L));
+  for (std::size_t i = T.rank; i < L.passes; i += 32 * W) dd[i] = tp.d[i];
+  constexpr int kPerNode = adj::kMaxPasses * adj::kPassFields;
+  for (int i = T.rank; i < nn * kPerNode; i += 32 * W) {
+    const int n = i / kPerNode, k = (i / adj::kPassFields) % adj::kMaxPasses, f = i % adj::kPassFields;
+    if (k < tp.i[L.npass + n]) dd[L.passes + static_cast<std::size_t>(poff[n] + k) * adj::kPassFields + f] = tp.d[L.passes + i];
+  }
+  const std::size_t bytes = record_bytes(L, poff[nn]);
+  T.sync();
+  return bytes;
+}
+
+// Unpacks a record (global) into the step's tape in shared memory: the pass records go to their slots; slots the
+// step did not use are left as they are (the replay reads only the used ones).
+template <int W>
+__device__ __forceinline__ void load_record(const unsigned char* src, const adj::Tape& tp, int nn, std::int32_t* poff, const Team<W>& T) {
+  const adj::TapeLayout& L = tp.L;
+  const std::int32_t* si = reinterpret_cast<const std::int32_t*>(src);
+  for (std::size_t i = T.rank; i < L.ints; i += 32 * W) tp.i[i] = si[i];
+  const double* sd = reinterpret_cast<const double*>(src + record_ints_bytes(L));
+  for (std::size_t i = T.rank; i < L.passes; i += 32 * W) tp.d[i] = sd[i];
+  T.sync();
+  pass_offsets(tp.i + L.npass, nn, poff, T);
+  constexpr int kPerNode = adj::kMaxPasses * adj::kPassFields;
+  for (int i = T.rank; i < nn * kPerNode; i += 32 * W) {
+    const int n = i / kPerNode, k = (i / adj::kPassFields) % adj::kMaxPasses, f = i % adj::kPassFields;
+    if (k < tp.i[L.npass + n]) tp.d[L.passes + i] = sd[L.passes + static_cast<std::size_t>(poff[n] + k) * adj::kPassFields + f];
+  }
+  T.sync();
+}
+
+// The step's inputs into its tape, before the step: the scalars and every node's state, pass counts cleared.
+template <int W>
+__device__ __forceinline__ void tape_inputs(const adj::Tape& tp, const SimRegs& R, const Slot& S, int nn, const Team<W>& T) {
+  const adj::TapeLayout& L = tp.L;
+  if (T.leader()) {
+    tp.d[L.scal] = R.t; tp.d[L.scal + 1] = R.zO; tp.d[L.scal + 2] = R.pitch; tp.d[L.scal + 3] = R.roll;
+    tp.d[L.scal + 4] = R.vz; tp.d[L.scal + 5] = R.wth; tp.d[L.scal + 6] = R.wph;
+  }
+  for (int n = T.rank; n < nn; n += 32 * W) {
+    tp.d[L.volIn + n] = S.vol[n]; tp.d[L.levelIn + n] = S.level[n];
+    tp.d[L.cxIn + n] = S.cx[n]; tp.d[L.cyIn + n] = S.cy[n]; tp.d[L.czIn + n] = S.cz[n];
+    tp.i[L.npass + n] = 0;
+  }
+  T.sync();
+}
+
+// The ring: a record at virtual offset v sits at v mod cap; a record that would run past the end starts the next lap
+// instead. After the last write at virtual end E the ring holds exactly the records at offsets >= E - cap.
+__device__ __forceinline__ long long ring_place(long long v, std::size_t cap, std::size_t maxRecord) {
+  const long long c = static_cast<long long>(cap);
+  if (v % c + static_cast<long long>(maxRecord) > c) v = (v / c + 1) * c;
+  return v;
+}
+
 __device__ __forceinline__ long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -186,11 +289,14 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
   Slot S = carve_slot(smem, SL);
   AdjSmem A = carve_adjoint(smem + SL.bytes, AL);
   const adj::TapeLayout TL = adj::tape_layout(M.nn, M.ng);
+  const std::size_t recMax = record_bytes(TL, M.nn * adj::kMaxPasses);
   const std::size_t recSize = 7 + 5 * static_cast<std::size_t>(M.nn);
   double* const ckpt = B.ckpt + static_cast<std::size_t>(team) * B.maxCkpt * recSize;
-  unsigned char* const tapes = B.tape + static_cast<std::size_t>(team) * B.K * TL.bytes;
+  unsigned char* const ring = B.arena + static_cast<std::size_t>(team) * B.arenaBytes;
+  long long* const off = B.stepOff + static_cast<std::size_t>(team) * (B.maxSteps + 1);
   double* const sink = B.sink + static_cast<std::size_t>(team) * (M.evCap + M.nmon + M.nmark + 1);
   std::int32_t* const isink = B.isink + static_cast<std::size_t>(team) * (M.evCap + 1);
+  const adj::Tape sp = adj::tape_at(A.tape, TL);
   const int NS = B.nsamples;
   for (;;) {
     if (T.leader()) S.misc[0] = atomicAdd(B.queue, 1);
@@ -199,7 +305,7 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
     T.sync();
     if (inst >= B.count) return;
     const long long tStart = global_ns();
-    long long tRecompute = 0, tReverse = 0;
+    long long tRecompute = 0, tReverse = 0, nRecomputed = 0;
     const std::size_t ic = static_cast<std::size_t>(inst) * M.nc;
     const AdjInst I{B.en + ic, B.area + ic, B.tOn + ic, sink, isink, M.nmon};
     // the event bookkeeping sinks: overflow and mark times set (nothing fires), so events never write
@@ -219,14 +325,14 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
       T.sync();
       load_state(c, R, S, M, T);
     }
-    // ---- 1. forward with checkpoints and the objective's samples
+    // ---- 1. forward with checkpoints, the objective's samples and (tapeForward) every step's record
     Pose& F = *S.pose;
     F = make_pose(M, R.zO, R.pitch, R.roll);
     const double* trimT = B.trimT + static_cast<std::size_t>(inst) * NS;
     const double* heaveT = B.heaveT + static_cast<std::size_t>(inst) * NS;
     double J = 0;
     int k = 0;
-    long long s = 0;
+    long long s = 0, v = 0;
     for (;; ++s) {
       if (s % B.K == 0 && s > 0) {
         save_state(ckpt + static_cast<std::size_t>(s / B.K) * recSize, R, S, M.nn, T);
@@ -243,10 +349,22 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
         }
         ++k;
       }
-      team_step<false, W>(M, F, R, S, I, T);
+      if (B.tapeForward) {
+        tape_inputs(sp, R, S, M.nn, T);
+        team_step<false, W>(M, F, R, S, I, T, GpuTape{sp});
+        T.sync();
+        v = ring_place(v, B.arenaBytes, recMax);
+        if (T.leader()) off[s] = v;
+        v += static_cast<long long>(store_record(sp, M.nn, A.poff, ring + v % static_cast<long long>(B.arenaBytes), T));
+      } else {
+        team_step<false, W>(M, F, R, S, I, T);
+      }
       F = make_pose(M, R.zO, R.pitch, R.roll);
     }
     const long long S_end = s;
+    // the ring holds the records at virtual offsets >= v - cap: a segment is reversed from the ring when its first
+    // step's record is among them
+    const long long kept = B.tapeForward ? v - static_cast<long long>(B.arenaBytes) : LLONG_MAX;
     const double zE = R.zO, thE = R.pitch, phE = R.roll;
     for (; k < NS; ++k) {
       double tr, hv;
@@ -276,45 +394,35 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
     for (long long g = nseg - 1; g >= 0; --g) {
       const long long s0 = g * B.K, s1 = (s0 + B.K < S_end) ? s0 + B.K : S_end;
       const long long tSeg = global_ns();
-      load_state(ckpt + static_cast<std::size_t>(g) * recSize, R, S, M, T);
-      F = make_pose(M, R.zO, R.pitch, R.roll);
-      for (long long st = s0; st < s1; ++st) {
-        const adj::Tape tp = adj::tape_at(tapes + static_cast<std::size_t>(st - s0) * TL.bytes, TL);
-        if (T.leader()) { tp.d[TL.scal] = R.t; tp.d[TL.scal + 1] = R.zO; tp.d[TL.scal + 2] = R.pitch; tp.d[TL.scal + 3] = R.roll;
-                          tp.d[TL.scal + 4] = R.vz; tp.d[TL.scal + 5] = R.wth; tp.d[TL.scal + 6] = R.wph; }
-        for (int n = T.rank; n < M.nn; n += 32 * W) {
-          tp.d[TL.volIn + n] = S.vol[n]; tp.d[TL.levelIn + n] = S.level[n];
-          tp.d[TL.cxIn + n] = S.cx[n]; tp.d[TL.cyIn + n] = S.cy[n]; tp.d[TL.czIn + n] = S.cz[n];
-          tp.i[TL.npass + n] = 0;
-        }
-        T.sync();
-        team_step<false, W>(M, F, R, S, I, T, GpuTape{tp});
+      if (!(B.tapeForward && off[s0] >= kept)) {
+        // recompute the segment from its checkpoint into the ring (every later segment has been reversed already, so
+        // the whole ring is free; it holds K records of the largest size)
+        load_state(ckpt + static_cast<std::size_t>(g) * recSize, R, S, M, T);
         F = make_pose(M, R.zO, R.pitch, R.roll);
+        long long w = 0;
+        nRecomputed += s1 - s0;
+        for (long long st = s0; st < s1; ++st) {
+          tape_inputs(sp, R, S, M.nn, T);
+          team_step<false, W>(M, F, R, S, I, T, GpuTape{sp});
+          T.sync();
+          if (T.leader()) off[st] = w;
+          w += static_cast<long long>(store_record(sp, M.nn, A.poff, ring + w, T));
+          F = make_pose(M, R.zO, R.pitch, R.roll);
+        }
       }
       __threadfence_block();
       T.sync();
       const long long tRev = global_ns();
       tRecompute += tRev - tSeg;
       for (long long st = s1 - 1; st >= s0; --st) {
-        const adj::Tape tp = adj::tape_at(tapes + static_cast<std::size_t>(st - s0) * TL.bytes, TL);
-        // the step's tape into shared memory before its reverse reads it (the replay of the level solve and the
-        // reverse read every record several times, in dependent chains): the state and solved arrays, the integers,
-        // and of the pass records only the slots the step used
-        const adj::Tape sp = adj::tape_at(A.tape, TL);
-        for (std::size_t i = T.rank; i < TL.passes; i += 32 * W) sp.d[i] = tp.d[i];
-        for (std::size_t i = T.rank; i < TL.ints; i += 32 * W) sp.i[i] = tp.i[i];
-        T.sync();
-        for (int i = T.rank; i < M.nn * adj::kMaxPasses * adj::kPassFields; i += 32 * W) {
-          const int n = i / (adj::kMaxPasses * adj::kPassFields), k = (i / adj::kPassFields) % adj::kMaxPasses;
-          if (k < sp.i[TL.npass + n]) sp.d[TL.passes + i] = tp.d[TL.passes + i];
-        }
-        T.sync();
+        load_record(ring + off[st] % static_cast<long long>(B.arenaBytes), sp, M.nn, A.poff, T);
         adj::reverse_step(AT, M, sp, I.en(), I.area(), I.tOn(), A.rs, A.as, aSc, A.grad, &err);
         for (int q = 0; q < NS; ++q)
           if (static_cast<long long>(A.sampleS[q]) == st) {
             const double tr = B.trim[static_cast<std::size_t>(inst) * NS + q], hv = B.heave[static_cast<std::size_t>(inst) * NS + q];
-            add_sample_adjoint(M, tp.d[TL.scal + 1], tp.d[TL.scal + 2], tp.d[TL.scal + 3], 2 * (tr - trimT[q]), 2 * (hv - heaveT[q]), aSc);
+            add_sample_adjoint(M, sp.d[TL.scal + 1], sp.d[TL.scal + 2], sp.d[TL.scal + 3], 2 * (tr - trimT[q]), 2 * (hv - heaveT[q]), aSc);
           }
+        T.sync();
       }
       tReverse += global_ns() - tRev;
     }
@@ -326,6 +434,7 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
       B.phaseNs[3 * static_cast<std::size_t>(inst)] = tForward;
       B.phaseNs[3 * static_cast<std::size_t>(inst) + 1] = tRecompute;
       B.phaseNs[3 * static_cast<std::size_t>(inst) + 2] = tReverse;
+      B.recomputed[inst] = nRecomputed;
     }
     T.sync();
   }
@@ -350,15 +459,18 @@ AdjLayout adjoint_layout(int nn, int nc, int ng, int nsamples, int W) {
   A.aZmx = take16(N); A.aLs = take16(N); A.aAs = take16(N);
   A.faHA = take16(C); A.faHB = take16(C); A.faAA = take16(C); A.faAB = take16(C);
   A.red = take16(sizeof(double) * 16 * static_cast<std::size_t>(W));
+  A.work = take16(sizeof(adj::UnitWork) * static_cast<std::size_t>(W));
   A.aVol = take16(N); A.aLevel = take16(N); A.aCx = take16(N); A.aCy = take16(N); A.aCz = take16(N);
   A.grad = take16(C);
   A.sampleS = take16(sizeof(double) * static_cast<std::size_t>(std::max(nsamples, 1)));
   A.tape = take16(adj::tape_layout(nn, ng).bytes);
+  A.poff = take16(sizeof(std::int32_t) * (static_cast<std::size_t>(std::max(nn, 1)) + 1));
   A.bytes = off;
   return A;
 }
 
-std::size_t adjoint_tape_bytes(int nn, int ng) { return adj::tape_layout(nn, ng).bytes; }
+std::size_t adjoint_tape_bytes(int nn, int ng) { return record_bytes(adj::tape_layout(nn, ng), nn * adj::kMaxPasses); }
+std::size_t adjoint_record_bytes(int nn, int ng, int passRecords) { return record_bytes(adj::tape_layout(nn, ng), passRecords); }
 
 cudaError_t configure_adjoint_kernel(int W, std::size_t smem) {
   const int b = static_cast<int>(smem);

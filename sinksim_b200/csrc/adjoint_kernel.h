@@ -33,21 +33,29 @@ struct AdjRun {
   std::int32_t K;                               // steps between checkpoints
   std::int32_t maxCkpt;                         // checkpoints per team
   double* ckpt;                                 // [teams x maxCkpt x (7 + 5 nn)]
-  unsigned char* tape;                          // [teams x K x tape bytes]
+  // Per team a ring of packed step records (adjoint_kernel.cu: store_record) of arenaBytes bytes, at least K records of
+  // the largest size, and the virtual offset of every step's record ([teams x (maxSteps + 1)]). With tapeForward the
+  // forward run records every step, and the reverse recomputes only the segments the ring no longer holds.
+  unsigned char* arena;
+  std::size_t arenaBytes;
+  long long* stepOff;
+  std::int32_t tapeForward;
   double* sink;                                 // [teams x (evCap + nmon + nmark + 1)]
   std::int32_t* isink;                          // [teams x (evCap + 1)]
   long long* phaseNs;                           // [count x 3] the team's time on the instance (globaltimer ns):
                                                 // forward, recomputation of the segments, reverse steps
+  long long* recomputed;                        // [count] steps recomputed from checkpoints
 };
 
 // Byte offsets of a team's reverse arrays in shared memory, after its forward slot.
 struct AdjLayout {
-  std::uint32_t hEff, aEff, dV, volPost, deg, clip, aVolPost, aCxs, aCys, aCzs, aVs, aAcc, aZmx, aLs, aAs, faHA, faHB, faAA, faAB, red;
-  std::uint32_t aVol, aLevel, aCx, aCy, aCz, grad, sampleS, tape, bytes;
+  std::uint32_t hEff, aEff, dV, volPost, deg, clip, aVolPost, aCxs, aCys, aCzs, aVs, aAcc, aZmx, aLs, aAs, faHA, faHB, faAA, faAB, red, work;
+  std::uint32_t aVol, aLevel, aCx, aCy, aCz, grad, sampleS, tape, poff, bytes;
 };
 
 AdjLayout adjoint_layout(int nn, int nc, int ng, int nsamples, int teamWarps);
-std::size_t adjoint_tape_bytes(int nn, int ng);
+std::size_t adjoint_tape_bytes(int nn, int ng);  // the largest packed step record
+std::size_t adjoint_record_bytes(int nn, int ng, int passRecords);  // a packed step record holding passRecords passes
 cudaError_t configure_adjoint_kernel(int teamWarps, std::size_t smem);
 cudaError_t adjoint_occupancy(int teamWarps, std::size_t smem, int* blocksPerSM);
 cudaError_t launch_adjoint_kernel(int teamWarps, const DevModel& M, const AdjRun& run, const SlotLayout& slot, const AdjLayout& layout, int teams,

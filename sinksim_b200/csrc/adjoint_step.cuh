@@ -228,16 +228,38 @@ SSB_HD void extreme_reverse(const DevModel& M, int j, bool bottom, double a_w, A
 
 // ----------------------------------------------------------------------------- node-pass reverse over segments
 
-// Reverse of np node passes of node n at levels h[i] with adjoints av/amx/amy/amz of their (permeability-scaled) vol and
-// moments: adds the pose adjoint to aP and returns in ah[i] this lane's share of d(outputs)/d h[i] (sum over the warp's
-// lanes for the total). Only segments the level cuts contribute (kernel/reduce.hpp:52-71: a full segment's height is
-// b - a, a dry one adds nothing).
-SSB_HD void pass_sweep(const DevModel& M, const PoseD& F, int n, int np, const double* h, const double* av, const double* amx,
-                       const double* amy, const double* amz, double* ah, int lane, int width, AdjPose& aP) {
+// Reverse of a node pass of node n at level h with adjoints av/amx/amy/amz of its (permeability-scaled) vol and
+// moments: adds the pose adjoint to aP and returns this lane's share of d(outputs)/d h (sum over the warp's lanes for
+// the total). Only segments the level cuts contribute (kernel/reduce.hpp:52-71: a full segment's height is b - a, a dry
+// one adds nothing).
+SSB_HD double pass_sweep1(const DevModel& M, const PoseD& F, int n, double h, double av, double amx, double amy, double amz, int lane, int width,
+                          AdjPose& aP) {
+  const int s0 = M.segStart[n], s1 = s0 + M.segCount[n];
+  const double mu = M.mu[n];
+  double aR20 = 0, aR21 = 0, atz = 0, aiR = 0, ah = 0;
+  for (int j = s0 + lane; j < s1; j += width) {
+    const double2 xy = M.segXY[j], ab = M.segLH[j];
+    const double base = F.R20 * xy.x + F.R21 * xy.y + F.tz;
+    const double zp = (h - base) * F.iR;
+    if (!(zp > ab.x && zp < ab.y)) continue;
+    const double L = zp - ab.x;
+    const double aL = M.segAr[j] * mu * (av + amx * xy.x + amy * xy.y + amz * (ab.x + L));
+    ah += aL * F.iR;
+    aiR += aL * (h - base);
+    const double abase = -aL * F.iR;
+    aR20 += abase * xy.x; aR21 += abase * xy.y; atz += abase;
+  }
+  aP.R20 += aR20; aP.R21 += aR21; aP.tz += atz; aP.iR += aiR;
+  return ah;
+}
+
+// The pose adjoint of np passes of node n at levels h[i] whose vol has the adjoint av[i] and whose moments have none
+// (their level adjoints are not needed).
+SSB_HD void pass_sweep_levels(const DevModel& M, const PoseD& F, int n, int np, const double* h, const double* av, int lane, int width,
+                              AdjPose& aP) {
   const int s0 = M.segStart[n], s1 = s0 + M.segCount[n];
   const double mu = M.mu[n];
   double aR20 = 0, aR21 = 0, atz = 0, aiR = 0;
-  for (int i = 0; i < np; ++i) ah[i] = 0;
   for (int j = s0 + lane; j < s1; j += width) {
     const double2 xy = M.segXY[j], ab = M.segLH[j];
     const double A = M.segAr[j];
@@ -245,9 +267,7 @@ SSB_HD void pass_sweep(const DevModel& M, const PoseD& F, int n, int np, const d
     for (int i = 0; i < np; ++i) {
       const double zp = (h[i] - base) * F.iR;
       if (!(zp > ab.x && zp < ab.y)) continue;
-      const double L = zp - ab.x;
-      const double aL = A * mu * (av[i] + amx[i] * xy.x + amy[i] * xy.y + amz[i] * (ab.x + L));
-      ah[i] += aL * F.iR;
+      const double aL = A * mu * av[i];
       aiR += aL * (h[i] - base);
       const double abase = -aL * F.iR;
       aR20 += abase * xy.x; aR21 += abase * xy.y; atz += abase;
@@ -300,13 +320,14 @@ struct Replay {
 
 SSB_HD const double* rec(const Tape& t, int n, int k) { return t.pass(n, k); }
 
-// Replays the solver's decisions (levels.hpp:13-49 for a node alone, :54-162 for a merged group) on the recorded passes.
-SSB_HD Replay replay_unit(const DevModel& M, const Tape& t, const int* members, int N, bool single) {
-  Replay r{};
+// Replays the solver's decisions (levels.hpp:13-49 for a node alone, :54-162 for a merged group) on the recorded passes,
+// into r.
+SSB_HD void replay_unit(const DevModel& M, const Tape& t, const int* members, int N, bool single, Replay& r) {
   r.N = N;
   r.single = single;
   r.ok = N <= kMaxMembers;
-  if (!r.ok) return r;
+  r.cs = 0; r.base = 0; r.K = 0; r.startSrc = 0; r.loSrc = 0; r.hiSrc = 0;
+  if (!r.ok) return;
   for (int k = 0; k < N; ++k) r.members[k] = members[k];
   const double* volIn = t.d + t.L.volIn;
   const double* levelIn = t.d + t.L.levelIn;
@@ -333,34 +354,36 @@ SSB_HD Replay replay_unit(const DevModel& M, const Tape& t, const int* members, 
   r.h0 = h;
   // the extent: the members' start passes
   double lo = rec(t, members[0], 0)[6], hi = rec(t, members[0], 0)[7];
-  r.loSrc = 0; r.hiSrc = 0;
+  int loSrc = 0, hiSrc = 0;
   for (int k = 1; k < N; ++k) {
     const double* p = rec(t, members[k], 0);
-    if (p[6] < lo) { lo = p[6]; r.loSrc = k; }
-    if (p[7] > hi) { hi = p[7]; r.hiSrc = k; }
+    if (p[6] < lo) { lo = p[6]; loSrc = k; }
+    if (p[7] > hi) { hi = p[7]; hiSrc = k; }
   }
   if (single) {
     // a node alone: the same extent as a group of one
-    r.loSrc = 0; r.hiSrc = 0;
+    loSrc = 0; hiSrc = 0;
   }
-  for (int k = 0; k < N; ++k) r.ok = r.ok && rec(t, members[k], 0)[0] == h;
-  if (V <= kEmptyVolume) { r.cs = 0; r.K = 0; return r; }
-  if (V >= Vmax * kFullFraction) { r.cs = 1; r.K = 1; return r; }
+  r.loSrc = loSrc; r.hiSrc = hiSrc;
+  bool ok = true;
+  for (int k = 0; k < N; ++k) ok = ok && rec(t, members[k], 0)[0] == h;
+  if (V <= kEmptyVolume) { r.cs = 0; r.K = 0; r.ok = ok; return; }
+  if (V >= Vmax * kFullFraction) { r.cs = 1; r.K = 1; r.ok = ok; return; }
   r.cs = 2;
-  r.base = 0;
-  r.startSrc = 0;
+  int base = 0;
   const bool clamp = single ? (h < lo || h > hi) : !(h >= lo && h <= hi);
   if (clamp) {
     const double hc = jmin(hi, jmax(lo, h));
     r.startSrc = h < lo ? kSrcLo : kSrcHi;
     h = hc;
-    r.base = 1;
-    for (int k = 0; k < N; ++k) r.ok = r.ok && rec(t, members[k], 1)[0] == h;
+    base = 1;
+    for (int k = 0; k < N; ++k) ok = ok && rec(t, members[k], 1)[0] == h;
   }
+  r.base = base;
   const double tol = jmax(1e-3 * Vmax, 0.5);
   double a = lo, b = hi;
   int aS = kSrcLo, bS = kSrcHi;
-  int k = r.base;
+  int k = base;
   for (int it = 0; it < kNewtonFast; ++it) {
     double sum = 0, dvs = 0;
     for (int q = 0; q < N; ++q) sum += rec(t, members[q], k)[1];
@@ -376,10 +399,10 @@ SSB_HD Replay replay_unit(const DevModel& M, const Tape& t, const int* members, 
     r.aSrc[k] = aS; r.bSrc[k] = bS;
     h = hn;
     ++k;
-    for (int q = 0; q < N; ++q) r.ok = r.ok && rec(t, members[q], k)[0] == h;
+    for (int q = 0; q < N; ++q) ok = ok && rec(t, members[q], k)[0] == h;
   }
   r.K = k;
-  return r;
+  r.ok = ok;
 }
 
 // Adjoint inputs and outputs of one unit, per member: the solved values' adjoints in, the start values' adjoints out.
@@ -389,6 +412,29 @@ struct UnitAdj {
   // out: adjoints of the step's starting volume, level and centroid
   double oVol[kMaxMembers], oLevel[kMaxMembers], oCx[kMaxMembers], oCy[kMaxMembers], oCz[kMaxMembers];
 };
+
+// Working memory of one unit's reverse, one per warp (shared memory on the device; the host harness keeps one on its
+// stack). Its scalars are the same for every lane of the warp: lane 0 alone writes them, and the lanes read them after
+// a warp sync, so no lane reads a value another is still updating.
+struct UnitWork {
+  Replay r;
+  UnitAdj u;
+  double av[kMaxMembers][kMaxPasses], adv[kMaxMembers][kMaxPasses];  // adjoints of each pass's vol and dv
+  double amx[kMaxMembers], amy[kMaxMembers], amz[kMaxMembers];        // of the final pass's moments
+  double hFinal[kMaxMembers];                                         // the final pass's level
+  double ah[kMaxPasses];                                              // adjoints of the levels h_j
+  double aZmin0[kMaxMembers], aZmax0[kMaxMembers];                    // of the members' extent bottom and top
+  double hs[kMaxMembers][kMaxPasses], pv[kMaxMembers][kMaxPasses];    // the earlier passes the pose sweep visits
+  int np[kMaxMembers];
+  double aV, aLo, aHi, aH0;
+  int err;
+};
+
+SSB_HD void warp_sync() {
+#if defined(__CUDA_ARCH__)
+  __syncwarp();
+#endif
+}
 
 // Centroid of a pass (set_centroid, levels.hpp:46): adjoint of cx = mx / vol etc. into the pass's vol and moments, or the
 // previous centroid's adjoint when the pass held too little water to move it.
@@ -403,164 +449,181 @@ SSB_HD void centroid_reverse(const double* p, double aCx, double aCy, double aCz
   }
 }
 
-// Reverse of one unit, run by the lanes of one warp (every lane holds the same scalars; the lanes split the segment
-// sweeps). Adds pose adjoints to aP (this lane's share) and returns false when the unit took a branch without an
-// adjoint here (the cascade of levels.hpp:136-155), its error bit in *err.
-SSB_HD bool unit_reverse(const DevModel& M, const PoseD& F, const Tape& t, const Replay& r, UnitAdj& u, int lane, int width, AdjPose& aP,
-                         int* err) {
+// Reverse of one unit, run by the lanes of one warp: lane 0 does the unit's scalar work in w, the lanes split the
+// segment sweeps. Adds pose adjoints to aP (this lane's share) and returns false when the unit took a branch without an
+// adjoint here (the cascade of levels.hpp:136-155), its error bit in *err. On entry w.r holds the replay and w.u's
+// inputs are set (written by lane 0, then a warp sync); on return w.u's outputs are set (lane 0's, before the caller's
+// warp sync).
+SSB_HD bool unit_reverse(const DevModel& M, const PoseD& F, const Tape& t, UnitWork& w, int lane, int width, AdjPose& aP, int* err) {
+  const Replay& r = w.r;
+  UnitAdj& u = w.u;
   const int N = r.N;
-  double av[kMaxMembers][kMaxPasses], adv[kMaxMembers][kMaxPasses], amx[kMaxMembers][kMaxPasses], amy[kMaxMembers][kMaxPasses],
-      amz[kMaxMembers][kMaxPasses];
-  double ah[kMaxPasses];
-  double aZmin0[kMaxMembers], aZmax0[kMaxMembers];
-  for (int k = 0; k < N; ++k) {
-    for (int i = 0; i < kMaxPasses; ++i) av[k][i] = adv[k][i] = amx[k][i] = amy[k][i] = amz[k][i] = 0;
-    aZmin0[k] = 0;
-    aZmax0[k] = u.aZmax[k];  // each member's own extent top is recorded from its start pass
-    u.oVol[k] = u.oLevel[k] = u.oCx[k] = u.oCy[k] = u.oCz[k] = 0;
-  }
-  for (int i = 0; i < kMaxPasses; ++i) ah[i] = 0;
-  double aV = 0, aLo = 0, aHi = 0, aH0 = 0;
   const int K = r.K;
-
-  if (r.cs == 0) {
-    // empty: the level is the member's own extent bottom; a group empties its members, a node alone keeps its volume
+  if (lane == 0) {
     for (int k = 0; k < N; ++k) {
-      aZmin0[k] += u.aLevel[k];
-      if (r.single) aV += u.aVol[k];
-      u.oCx[k] += u.aCx[k]; u.oCy[k] += u.aCy[k]; u.oCz[k] += u.aCz[k];
+      for (int i = 0; i <= K; ++i) w.av[k][i] = w.adv[k][i] = 0;
+      w.amx[k] = w.amy[k] = w.amz[k] = 0;
+      w.aZmin0[k] = 0;
+      w.aZmax0[k] = u.aZmax[k];  // each member's own extent top is recorded from its start pass
+      w.np[k] = 0;
+      u.oVol[k] = u.oLevel[k] = u.oCx[k] = u.oCy[k] = u.oCz[k] = 0;
     }
-  } else if (r.cs == 1) {
-    // full: volumes vmax + dh aov (the last takes the rest), level hi + dh, centroids at the top (levels.hpp:29-35, :91-111)
-    double aSum = 0;
-    for (int k = 0; k < N; ++k) aSum += M.aov[r.members[k]];
-    double aDh = 0;
-    aV += u.aVol[N - 1];
-    for (int k = 0; k < N - 1; ++k) aDh += (u.aVol[k] - u.aVol[N - 1]) * M.aov[r.members[k]];
-    for (int k = 0; k < N; ++k) { aDh += u.aLevel[k]; aHi += u.aLevel[k]; }
-    if (r.V - r.Vmax > 0) aV += aDh / aSum;
-    for (int k = 0; k < N; ++k) {
-      const double* p = rec(t, r.members[k], 1);
-      centroid_reverse(p, u.aCx[k], u.aCy[k], u.aCz[k], av[k][1], amx[k][1], amy[k][1], amz[k][1], u.oCx[k], u.oCy[k], u.oCz[k]);
-      double hh = p[0], a1 = 0;
-      pass_sweep(M, F, r.members[k], 1, &hh, &av[k][1], &amx[k][1], &amy[k][1], &amz[k][1], &a1, lane, width, aP);
-      aHi += lane_sum(a1, width);
-    }
-  } else {
-    // Newton: level h_K, area and centroid of the final passes, the group's water shared in proportion to them
-    for (int k = 0; k < N; ++k) {
-      ah[K] += u.aLevel[k];
-      adv[k][K] += u.aArea[k];
-      const double* p = rec(t, r.members[k], K);
-      centroid_reverse(p, u.aCx[k], u.aCy[k], u.aCz[k], av[k][K], amx[k][K], amy[k][K], amz[k][K], u.oCx[k], u.oCy[k], u.oCz[k]);
-    }
-    if (r.single) {
-      aV += u.aVol[0];
-    } else {
-      double tot = 0;
-      for (int k = 0; k < N; ++k) tot += rec(t, r.members[k], K)[1];
-      double assigned = 0, aTot = 0;
-      aV += u.aVol[N - 1];
-      for (int k = 0; k < N - 1; ++k) {
-        const double pk = rec(t, r.members[k], K)[1];
-        double v = tot > 0 ? r.V * pk / tot : r.V / static_cast<double>(N);
-        const bool capped = v > M.vmax[r.members[k]];
-        if (capped) v = M.vmax[r.members[k]];
-        assigned += v;
-        const double a = u.aVol[k] - u.aVol[N - 1];
-        if (capped) continue;
-        if (tot > 0) {
-          aV += a * pk / tot;
-          av[k][K] += a * r.V / tot;
-          aTot -= a * v / tot;
-        } else {
-          aV += a / static_cast<double>(N);
-        }
+    for (int i = 0; i <= K; ++i) w.ah[i] = 0;
+    w.aV = w.aLo = w.aHi = w.aH0 = 0;
+    w.err = 0;
+    if (r.cs == 0) {
+      // empty: the level is the member's own extent bottom; a group empties its members, a node alone keeps its volume
+      for (int k = 0; k < N; ++k) {
+        w.aZmin0[k] += u.aLevel[k];
+        if (r.single) w.aV += u.aVol[k];
+        u.oCx[k] += u.aCx[k]; u.oCy[k] += u.aCy[k]; u.oCz[k] += u.aCz[k];
       }
-      if (r.V - assigned > M.vmax[r.members[N - 1]]) { *err |= kErrCascade; return false; }
-      if (aTot != 0)
-        for (int k = 0; k < N; ++k) av[k][K] += aTot;
-    }
-    // the final passes: their level derivative (volume and moments) before the chain of updates
-    for (int k = 0; k < N; ++k) {
-      double hh = rec(t, r.members[k], K)[0], a1 = 0;
-      pass_sweep(M, F, r.members[k], 1, &hh, &av[k][K], &amx[k][K], &amy[k][K], &amz[k][K], &a1, lane, width, aP);
-      ah[K] += lane_sum(a1, width);
-    }
-    // the updates, last first: h_{j+1} = h_j - err_j / dv_j (Newton) or the bracket's midpoint (bisection)
-    for (int j = K - 1; j >= r.base; --j) {
-      if (r.newton[j]) {
-        double err = 0, dvs = 0;
-        for (int k = 0; k < N; ++k) { err += rec(t, r.members[k], j)[1]; dvs += rec(t, r.members[k], j)[2]; }
-        err = err - r.V;
-        ah[j] += ah[j + 1];
-        const double aErr = -ah[j + 1] / dvs;
-        const double aDvs = ah[j + 1] * err / (dvs * dvs);
-        aV -= aErr;
-        for (int k = 0; k < N; ++k) { av[k][j] += aErr; adv[k][j] += aDvs; }
+    } else if (r.cs == 1) {
+      // full: volumes vmax + dh aov (the last takes the rest), level hi + dh, centroids at the top (levels.hpp:29-35, :91-111)
+      double aSum = 0;
+      for (int k = 0; k < N; ++k) aSum += M.aov[r.members[k]];
+      double aDh = 0;
+      double aV = u.aVol[N - 1];
+      for (int k = 0; k < N - 1; ++k) aDh += (u.aVol[k] - u.aVol[N - 1]) * M.aov[r.members[k]];
+      double aHi = 0;
+      for (int k = 0; k < N; ++k) { aDh += u.aLevel[k]; aHi += u.aLevel[k]; }
+      if (r.V - r.Vmax > 0) aV += aDh / aSum;
+      w.aV = aV;
+      w.aHi = aHi;
+      for (int k = 0; k < N; ++k) {
+        const double* p = rec(t, r.members[k], 1);
+        centroid_reverse(p, u.aCx[k], u.aCy[k], u.aCz[k], w.av[k][1], w.amx[k], w.amy[k], w.amz[k], u.oCx[k], u.oCy[k], u.oCz[k]);
+        w.hFinal[k] = p[0];
+      }
+    } else {
+      // Newton: level h_K, area and centroid of the final passes, the group's water shared in proportion to them
+      for (int k = 0; k < N; ++k) {
+        w.ah[K] += u.aLevel[k];
+        w.adv[k][K] += u.aArea[k];
+        const double* p = rec(t, r.members[k], K);
+        centroid_reverse(p, u.aCx[k], u.aCy[k], u.aCz[k], w.av[k][K], w.amx[k], w.amy[k], w.amz[k], u.oCx[k], u.oCy[k], u.oCz[k]);
+        w.hFinal[k] = p[0];
+      }
+      if (r.single) {
+        w.aV += u.aVol[0];
       } else {
-        const double half = 0.5 * ah[j + 1];
-        const int srcs[2] = {r.aSrc[j], r.bSrc[j]};
-        for (int s = 0; s < 2; ++s) {
-          if (srcs[s] >= 0) ah[srcs[s]] += half;
-          else if (srcs[s] == kSrcLo) aLo += half;
-          else aHi += half;
+        double tot = 0;
+        for (int k = 0; k < N; ++k) tot += rec(t, r.members[k], K)[1];
+        double assigned = 0, aTot = 0;
+        double aV = u.aVol[N - 1];
+        for (int k = 0; k < N - 1; ++k) {
+          const double pk = rec(t, r.members[k], K)[1];
+          double v = tot > 0 ? r.V * pk / tot : r.V / static_cast<double>(N);
+          const bool capped = v > M.vmax[r.members[k]];
+          if (capped) v = M.vmax[r.members[k]];
+          assigned += v;
+          const double a = u.aVol[k] - u.aVol[N - 1];
+          if (capped) continue;
+          if (tot > 0) {
+            aV += a * pk / tot;
+            w.av[k][K] += a * r.V / tot;
+            aTot -= a * v / tot;
+          } else {
+            aV += a / static_cast<double>(N);
+          }
         }
+        w.aV = aV;
+        if (r.V - assigned > M.vmax[r.members[N - 1]]) w.err = kErrCascade;
+        else if (aTot != 0)
+          for (int k = 0; k < N; ++k) w.av[k][K] += aTot;
       }
-      // pass j's own level dependence: d vol / d h is its free-surface area, its area does not depend on h
-      for (int k = 0; k < N; ++k) ah[j] += av[k][j] * rec(t, r.members[k], j)[2];
     }
-    // the first Newton level: the clamped start (the extent's bottom or top) or the start itself
-    if (r.base == 1) {
-      if (r.startSrc == kSrcLo) aLo += ah[1]; else aHi += ah[1];
-    } else {
-      aH0 += ah[0];
-    }
-    // pose adjoints of the passes before the final one (their level adjoints are in the chain above)
+  }
+  warp_sync();
+  if (w.err) { *err |= w.err; return false; }
+  // the final passes: their level derivative (volume and moments), before the chain of updates
+  if (r.cs != 0)
     for (int k = 0; k < N; ++k) {
-      double hs[kMaxPasses], scratch[kMaxPasses];
-      double pv[kMaxPasses], pmx[kMaxPasses], pmy[kMaxPasses], pmz[kMaxPasses];
-      int np = 0;
-      for (int j = r.base; j < K; ++j) {
-        if (av[k][j] == 0) continue;
-        hs[np] = rec(t, r.members[k], j)[0];
-        pv[np] = av[k][j]; pmx[np] = pmy[np] = pmz[np] = 0;
-        ++np;
+      const double a1 = lane_sum(pass_sweep1(M, F, r.members[k], w.hFinal[k], w.av[k][K], w.amx[k], w.amy[k], w.amz[k], lane, width, aP), width);
+      if (lane == 0) {
+        if (r.cs == 1) w.aHi += a1;
+        else w.ah[K] += a1;
       }
-      if (np) pass_sweep(M, F, r.members[k], np, hs, pv, pmx, pmy, pmz, scratch, lane, width, aP);
+    }
+  if (lane == 0) {
+    if (r.cs == 2) {
+      // the updates, last first: h_{j+1} = h_j - err_j / dv_j (Newton) or the bracket's midpoint (bisection)
+      for (int j = K - 1; j >= r.base; --j) {
+        if (r.newton[j]) {
+          double e = 0, dvs = 0;
+          for (int k = 0; k < N; ++k) { e += rec(t, r.members[k], j)[1]; dvs += rec(t, r.members[k], j)[2]; }
+          e = e - r.V;
+          w.ah[j] += w.ah[j + 1];
+          const double aErr = -w.ah[j + 1] / dvs;
+          const double aDvs = w.ah[j + 1] * e / (dvs * dvs);
+          w.aV -= aErr;
+          for (int k = 0; k < N; ++k) { w.av[k][j] += aErr; w.adv[k][j] += aDvs; }
+        } else {
+          const double half = 0.5 * w.ah[j + 1];
+          const int srcs[2] = {r.aSrc[j], r.bSrc[j]};
+          for (int s = 0; s < 2; ++s) {
+            if (srcs[s] >= 0) w.ah[srcs[s]] += half;
+            else if (srcs[s] == kSrcLo) w.aLo += half;
+            else w.aHi += half;
+          }
+        }
+        // pass j's own level dependence: d vol / d h is its free-surface area, its area does not depend on h
+        for (int k = 0; k < N; ++k) w.ah[j] += w.av[k][j] * rec(t, r.members[k], j)[2];
+      }
+      // the first Newton level: the clamped start (the extent's bottom or top) or the start itself
+      if (r.base == 1) {
+        if (r.startSrc == kSrcLo) w.aLo += w.ah[1]; else w.aHi += w.ah[1];
+      } else {
+        w.aH0 += w.ah[0];
+      }
+      // the passes before the final one whose volume the chain reached: their pose adjoints come from a sweep
+      for (int k = 0; k < N; ++k) {
+        int np = 0;
+        for (int j = r.base; j < K; ++j) {
+          if (w.av[k][j] == 0) continue;
+          w.hs[k][np] = rec(t, r.members[k], j)[0];
+          w.pv[k][np] = w.av[k][j];
+          ++np;
+        }
+        w.np[k] = np;
+      }
+    }
+    // the extent: bottom and top of the unit's start passes
+    if (N > 0) {
+      w.aZmin0[r.loSrc] += w.aLo;
+      w.aZmax0[r.hiSrc] += w.aHi;
     }
   }
-  // the free-surface area of every pass: dv = (sum of the cut segments' footprints) mu / R22. Every lane of the warp
-  // holds these scalars; lane 0 alone adds them to the pose adjoint, which is summed over the lanes afterwards.
-  if (lane == 0)
-    for (int k = 0; k < N; ++k)
-      for (int j = 0; j <= K && j < kMaxPasses; ++j)
-        if (adv[k][j] != 0) aP.iR += adv[k][j] * rec(t, r.members[k], j)[2] / F.iR;
-  // the extent: bottom and top of the unit's start passes
-  if (N > 0) {
-    aZmin0[r.loSrc] += aLo;
-    aZmax0[r.hiSrc] += aHi;
-  }
+  warp_sync();
+  for (int k = 0; k < N; ++k)
+    if (w.np[k]) pass_sweep_levels(M, F, r.members[k], w.np[k], w.hs[k], w.pv[k], lane, width, aP);
   // (every lane finds the same segment; lane 0 alone adds its terms)
   for (int k = 0; k < N; ++k) {
-    if (aZmin0[k] != 0) {
+    if (w.aZmin0[k] != 0) {
       const int j = pass_extreme(M, F, r.members[k], true, lane, width);
-      if (lane == 0) extreme_reverse(M, j, true, aZmin0[k], aP);
+      if (lane == 0) extreme_reverse(M, j, true, w.aZmin0[k], aP);
     }
-    if (aZmax0[k] != 0) {
+    if (w.aZmax0[k] != 0) {
       const int j = pass_extreme(M, F, r.members[k], false, lane, width);
-      if (lane == 0) extreme_reverse(M, j, false, aZmax0[k], aP);
+      if (lane == 0) extreme_reverse(M, j, false, w.aZmax0[k], aP);
     }
   }
-  // the start level and the unit's volume
-  if (r.single) {
-    u.oLevel[0] += aH0;
-  } else if (r.allWet) {
-    for (int k = 0; k < N; ++k) u.oLevel[k] += aH0 / static_cast<double>(N);
-  } else {
-    u.oLevel[r.firstWet >= 0 ? r.firstWet : N - 1] += aH0;
+  if (lane == 0) {
+    // the free-surface area of every pass: dv = (sum of the cut segments' footprints) mu / R22; lane 0 alone adds it
+    // to the pose adjoint, which is summed over the lanes afterwards
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j <= K && j < kMaxPasses; ++j)
+        if (w.adv[k][j] != 0) aP.iR += w.adv[k][j] * rec(t, r.members[k], j)[2] / F.iR;
+    // the start level and the unit's volume
+    if (r.single) {
+      u.oLevel[0] += w.aH0;
+    } else if (r.allWet) {
+      for (int k = 0; k < N; ++k) u.oLevel[k] += w.aH0 / static_cast<double>(N);
+    } else {
+      u.oLevel[r.firstWet >= 0 ? r.firstWet : N - 1] += w.aH0;
+    }
+    for (int k = 0; k < N; ++k) u.oVol[k] += w.aV;
   }
-  for (int k = 0; k < N; ++k) u.oVol[k] += aV;
   return true;
 }
 
@@ -820,6 +883,7 @@ struct RevSlot {
   double *aVolPost, *aCxs, *aCys, *aCzs, *aVs, *aAcc, *aZmx, *aLs, *aAs;
   double *faHA, *faHB, *faAA, *faAB;     // per connection: its flow's adjoints at its a and b ends
   double* red;                           // team reduction scratch: nwarps x 16
+  UnitWork* work;                        // one per warp: the level solve's reverse, unit by unit
 };
 
 // The adjoint of the state between steps: per node in memory, the scalars (zO, pitch, roll, vz, wth, wph) in every
@@ -954,8 +1018,10 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
   }
   team.sync();
 
-  // ---- the level solve, unit by unit: a warp per merged group or node alone
+  // ---- the level solve, unit by unit: a warp per merged group or node alone, lane 0 replaying it into the warp's
+  // work area
   bool ok = true;
+  UnitWork& w = S.work[team.warp];
   for (int g = team.warp; g < M.ng; g += team.nwarps) {
     const int N = M.gCount[g];
     const int* mem = M.gNodes + M.gStart[g];
@@ -965,26 +1031,38 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
       const int* um = isMerged ? mem : mem + u;
       const int un = isMerged ? N : 1;
       if (un > kMaxMembers) { ok = false; *err |= kErrGroupSize; continue; }
-      Replay r = replay_unit(M, tp, um, un, !isMerged);
-      for (int k = 0; k < un; ++k) {
-        const int want = r.cs == 0 ? 1 : (r.cs == 1 ? 2 : r.K + 1);
-        r.ok = r.ok && tp.i[L.npass + um[k]] == want;
-      }
-      if (!r.ok) { ok = false; *err |= kErrReplay; continue; }
-      UnitAdj ua;
-      for (int k = 0; k < un; ++k) {
-        const int n = um[k];
-        ua.aLevel[k] = S.aLs[n]; ua.aArea[k] = S.aAs[n]; ua.aCx[k] = S.aCxs[n]; ua.aCy[k] = S.aCys[n]; ua.aCz[k] = S.aCzs[n];
-        ua.aVol[k] = S.aVs[n]; ua.aZmax[k] = S.aZmx[n];
-      }
-      int e = 0;
-      if (!unit_reverse(M, F, tp, r, ua, team.lane, team.width, aP, &e)) { ok = false; *err |= e; continue; }
-      if (team.lane == 0)
+      if (team.lane == 0) {
+        replay_unit(M, tp, um, un, !isMerged, w.r);
+        for (int k = 0; k < un; ++k) {
+          const int want = w.r.cs == 0 ? 1 : (w.r.cs == 1 ? 2 : w.r.K + 1);
+          w.r.ok = w.r.ok && tp.i[L.npass + um[k]] == want;
+        }
         for (int k = 0; k < un; ++k) {
           const int n = um[k];
-          a.aVol[n] = ua.oVol[k]; a.aLevel[n] = ua.oLevel[k];
-          a.aCx[n] = ua.oCx[k]; a.aCy[n] = ua.oCy[k]; a.aCz[n] = ua.oCz[k];
+          w.u.aLevel[k] = S.aLs[n]; w.u.aArea[k] = S.aAs[n]; w.u.aCx[k] = S.aCxs[n]; w.u.aCy[k] = S.aCys[n]; w.u.aCz[k] = S.aCzs[n];
+          w.u.aVol[k] = S.aVs[n]; w.u.aZmax[k] = S.aZmx[n];
         }
+      }
+      warp_sync();
+      bool done = w.r.ok;
+      if (!done) {
+        ok = false;
+        *err |= kErrReplay;
+      } else {
+        int e = 0;
+        if (!unit_reverse(M, F, tp, w, team.lane, team.width, aP, &e)) {
+          ok = false;
+          *err |= e;
+          done = false;
+        }
+      }
+      if (done && team.lane == 0)
+        for (int k = 0; k < un; ++k) {
+          const int n = um[k];
+          a.aVol[n] = w.u.oVol[k]; a.aLevel[n] = w.u.oLevel[k];
+          a.aCx[n] = w.u.oCx[k]; a.aCy[n] = w.u.oCy[k]; a.aCz[n] = w.u.oCz[k];
+        }
+      warp_sync();  // every lane is done with the work area before lane 0 fills it for the next unit
     }
   }
   team.sync();

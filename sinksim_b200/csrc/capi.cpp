@@ -591,6 +591,20 @@ int ssb_adjoint_set_objective(ssb_adjoint* a, int32_t n, const double* times, co
   });
 }
 
+int ssb_adjoint_set_tape_budget(ssb_adjoint* a, uint64_t bytes) {
+  return guard([&] {
+    need(a, "adjoint");
+    a->adj->set_tape_budget(bytes);
+  });
+}
+
+int ssb_adjoint_ring_bytes(const ssb_adjoint* a, uint64_t* bytes) {
+  return guard([&] {
+    need(a, "adjoint"); need(bytes, "bytes");
+    *bytes = a->adj->ring_bytes();
+  });
+}
+
 int ssb_adjoint_run(ssb_adjoint* a, double* J, double* grad, int64_t* steps, int32_t* error, float* device_ms) {
   return guard([&] {
     need(a, "adjoint");
@@ -633,6 +647,13 @@ int ssb_adjoint_phase_times(const ssb_adjoint* a, int64_t* ns) {
     need(a, "adjoint"); need(ns, "ns");
     const int32_t n = a->adj->count();
     for (int32_t i = 0; i < n; ++i) std::memcpy(ns + 3 * static_cast<std::size_t>(i), a->adj->phase_ns(i), 3 * sizeof(int64_t));
+  });
+}
+
+int ssb_adjoint_recomputed_steps(const ssb_adjoint* a, int64_t* steps) {
+  return guard([&] {
+    need(a, "adjoint"); need(steps, "steps");
+    for (int32_t i = 0; i < a->adj->count(); ++i) steps[i] = a->adj->recomputed_steps(i);
   });
 }
 

@@ -5,7 +5,9 @@
   relative (the device sums the pose adjoints in another order), and the FP64 tangent-linear restatement's within
   1e-9 relative, on titanic64 over 1,000 s (4,000 steps, 16 checkpoint segments) and on the generated liner.
 * Checkpointing does not change the numbers: intervals of 256, 100 and 4,000 steps give the same bits (the reverse
-  of every step runs on the same recomputed tape).
+  of every step runs on the same recomputed tape). Nor does the memory for step records: a ring of one segment (every
+  segment recomputed from its checkpoint), one that holds the last few segments of the run (the rest recomputed) and
+  one that holds the whole run (nothing recomputed: the phase times show no recomputation) give the same bits.
 * Its trim and heave at the sample times equal the batch engine's readout curve records bit for bit.
 """
 import numpy as np
@@ -40,15 +42,17 @@ def _setup(ship, sim, steps, count=len(SCALES)):
     return bconns, areas, samples, times, np.array(trim), np.array(heave)
 
 
-def _run(ship_p, sim_p, ship, sim, steps, k_every=256, count=len(SCALES)):
+def _run(ship_p, sim_p, ship, sim, steps, k_every=256, count=len(SCALES), tape_budget=0):
     bconns, areas, samples, times, trim, heave = _setup(ship, sim, steps, count)
-    a = ssb.Adjoint(ship_p, sim_p, count=count, t_max=steps * sim["dt"], checkpoint_every=k_every)
+    a = ssb.Adjoint(ship_p, sim_p, count=count, t_max=steps * sim["dt"], checkpoint_every=k_every, tape_budget=tape_budget)
     a.set_connection_areas(0, bconns, areas)
     a.set_objective(times, trim, heave)
     J, g, st, err, ms = a.run()
     tr, hv = a.samples()
+    phases, ring, recomputed = a.phase_times(), a.ring_bytes(), a.recomputed_steps()
     a.close()
-    return dict(J=J, g=g, steps=st, err=err, trim=tr, heave=hv, bconns=bconns, areas=areas, samples=samples, trimT=trim, heaveT=heave)
+    return dict(J=J, g=g, steps=st, err=err, trim=tr, heave=hv, bconns=bconns, areas=areas, samples=samples, trimT=trim, heaveT=heave,
+                phases=phases, ring=ring, recomputed=recomputed)
 
 
 def _host(ship, sim, r, i, steps):
@@ -98,6 +102,28 @@ def test_gpu_adjoint_does_not_depend_on_the_checkpoint_interval():
         other = _run(ship_p, sim_p, ship, sim, 2000, k, count=2)
         np.testing.assert_array_equal(other["J"], base["J"])
         np.testing.assert_array_equal(other["g"], base["g"], err_msg=f"checkpoints every {k} steps")
+
+
+def test_gpu_adjoint_does_not_depend_on_the_memory_for_step_records():
+    ship_p, sim_p = titanic()
+    ship, sim = load_model(ship_p, sim_p)
+    steps, k_every, count = 2000, 100, 2
+    whole = _run(ship_p, sim_p, ship, sim, steps, k_every, count=count)
+    assert (whole["recomputed"] == 0).all(), whole["recomputed"]
+    assert (whole["phases"][:, 1] < 0.01 * whole["phases"][:, 2]).all(), whole["phases"]
+    one = _run(ship_p, sim_p, ship, sim, steps, k_every, count=count, tape_budget=1)
+    seg = one["ring"]  # one segment of the largest records per team
+    assert whole["ring"] > seg
+    assert (one["recomputed"] == steps).all(), one["recomputed"]
+    some = _run(ship_p, sim_p, ship, sim, steps, k_every, count=count, tape_budget=count * 2 * seg)
+    assert some["ring"] == 2 * seg
+    # a record is about a third of the largest, so the ring holds the last few of the 20 segments
+    assert ((some["recomputed"] > 0) & (some["recomputed"] < steps - 2 * k_every)).all(), some["recomputed"]
+    assert (some["recomputed"] % k_every == 0).all()
+    for name, r in (("one segment", one), ("a few segments", some)):
+        np.testing.assert_array_equal(r["J"], whole["J"], err_msg=name)
+        np.testing.assert_array_equal(r["g"], whole["g"], err_msg=name)
+        np.testing.assert_array_equal(r["steps"], whole["steps"], err_msg=name)
 
 
 def test_gpu_adjoint_samples_equal_the_batch_curve():
