@@ -72,6 +72,7 @@ def parse():
     ap.add_argument("--fd-steps", type=int, default=1, help="gradient: timed calls of the finite-difference arm (0: none)")
     ap.add_argument("--t-end", type=float, default=7920.0, help="gradient: s, the last of the objective's 8 times and the runs' end")
     ap.add_argument("--tape-gb", type=float, default=0.0, help="gradient: device memory for the adjoint's step records (0: chosen)")
+    ap.add_argument("--stage-columns", action="store_true", help="uneven: every block holds the column table in shared memory")
     ap.add_argument("--autotune", action="store_true", help="pick the launch shape by timing candidates first (outside the timed region)")
     args = ap.parse_args()
     if args.model is None:
@@ -179,7 +180,8 @@ class Clocks:
 def make_batch(ssb, ship_p, sim_p, sim, rule, count, first, args, device, **shape):
     from sinksim_b200.workloads import batch_uneven
 
-    b = ssb.Batch(ship_p, sim_p, count=count, numerics=args.numerics, t_max=args.tmax, device=device, rule=rule, **shape)
+    b = ssb.Batch(ship_p, sim_p, count=count, numerics=args.numerics, t_max=args.tmax, device=device, rule=rule,
+                  stage_columns=getattr(args, "stage_columns", False), **shape)
     for i, (area, enabled) in enumerate(batch_uneven(sim, count, first=first)):
         for c, a in area.items():
             b.set_connection_area(i, c, a)
@@ -431,7 +433,8 @@ def workload_config(args):
             "global_batch": args.count * args.gpus, "numerics": args.numerics, "t_max_s": args.tmax, "dt_s": 0.25,
             "retire": "founder | sink (|trim|>15 deg, bow deck edge under) | settle (|pitch rate|<1e-5 rad/s for 600 s) | tMax",
             "parallelism": f"instances sharded over {args.gpus} GPU(s), no collective in the step",
-            "l2": "working set (geometry 0.6 MB, per-instance state) is L2-resident by design; every step is a full batch from initial state"}
+            "l2": "working set (geometry 0.6 MB, per-instance state) is L2-resident by design; every step is a full batch from initial state",
+            "column_table": "shared memory of every block (bulk asynchronous copies)" if args.stage_columns else "global memory, through L1"}
 
 
 def gradient_bench(args):

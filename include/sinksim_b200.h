@@ -69,6 +69,12 @@ typedef struct ssb_batch_options {
    * steps done first, so that the runs with the most work left get the larger teams first; 1 by index. The results
    * are the same either way. */
   int32_t claim_by_index;
+  /* 1: every block first copies the model's column table (the arrays the buoyancy integral reads, 40 bytes a column
+   * in portable numerics, 20 in portable32) into its shared memory beside its simulations' slots, by bulk
+   * asynchronous copies, and the buoyancy reads it from there; a phase whose blocks lack the room runs fewer
+   * simulations per block. Single-model batches only; the results are the same either way. 0 (the default): the
+   * table is read from global memory through the L1 cache. */
+  int32_t stage_columns;
 } ssb_batch_options;
 
 typedef struct ssb_device_info {
@@ -296,7 +302,9 @@ int ssb_measure_add_mul_peak(int32_t fp64, int32_t device, double* ops_per_s);
 
 /* Health of the last run: *flags receives 0, or bit 1 when an instance's rigid-body state (heave, pitch, roll or a rate)
  * was not finite when the kernel stored it (a NaN or infinity in an input, or a diverging model). The reference has no
- * such report; its engine computes on with NaNs. The results are unchanged; this says that some cannot be trusted. */
+ * such report; its engine computes on with NaNs. The results are unchanged; this says that some cannot be trusted.
+ * Bit 2: with stage_columns, a block's copy of the column table did not arrive within its wait limit and that block
+ * read the table from global memory (the results are the same). */
 int ssb_batch_health(const ssb_batch* b, int32_t* flags);
 
 /* Loads and verifies a compiled ship and sim without running anything (no device needed): formats and versions,

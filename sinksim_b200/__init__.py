@@ -20,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsinksim_b200.so")
 NUMERICS = {"portable": 0, "portable32": 1}
 HEALTH_NON_FINITE = 1
+HEALTH_STAGE_TIMEOUT = 2
 STOP_REASONS = {0: "running", 1: "foundered", 2: "tmax", 3: "sink-rule", 4: "settle-rule", 5: "stable"}
 _ERRORS = {-1: "invalid argument", -2: "runtime error", -3: "call out of order", -4: "unsupported", -5: "no CUDA device"}
 
@@ -37,7 +38,7 @@ class _Options(C.Structure):
                 ("blocks", C.c_int32), ("device", C.c_int32), ("rule_enabled", C.c_int32),
                 ("rule_pitch", C.c_double), ("rule_x", C.c_double), ("rule_y", C.c_double), ("rule_z", C.c_double),
                 ("rule_wth", C.c_double), ("rule_settle", C.c_double), ("stop_when_stable", C.c_int32), ("handover_factor", C.c_double),
-                ("claim_by_index", C.c_int32)]
+                ("claim_by_index", C.c_int32), ("stage_columns", C.c_int32)]
 
 
 class _DeviceInfo(C.Structure):
@@ -218,11 +219,14 @@ class Batch:
 
     numerics: "portable" (double precision) or "portable32" (single-precision column partials).
     rule: optional dict(pitch=, x=, y=, z=, wth=, settle=) for the extra sink/settle retire rule.
+    stage_columns: every block copies the column table into its shared memory and the buoyancy reads it from there
+    (ssb_batch_options.stage_columns); the results are the same.
     """
 
     def __init__(self, ship_path, sim_path, count=1, numerics="portable32", traced_instances=0, dense_steps=400, sample_every=60.0,
                  curve_every=0.0, t_max=5 * 3600.0, steps_per_launch=0, team_warps=0, tail_team_warps=-1, teams_per_block=0, yield_below=-1,
-                 blocks=0, device=0, rule=None, stop_when_stable=False, handover_factor=0.0, claim_by_index=False, _fleet=None):
+                 blocks=0, device=0, rule=None, stop_when_stable=False, handover_factor=0.0, claim_by_index=False, stage_columns=False,
+                 _fleet=None):
         if numerics not in NUMERICS:
             raise SinksimError(-4, f"numerics {numerics!r} is not available on the GPU (portable or portable32)")
         o = _Options()
@@ -234,6 +238,7 @@ class Batch:
         o.stop_when_stable = 1 if stop_when_stable else 0
         o.handover_factor = handover_factor
         o.claim_by_index = 1 if claim_by_index else 0
+        o.stage_columns = 1 if stage_columns else 0
         if rule:
             o.rule_enabled = 1
             o.rule_pitch, o.rule_x, o.rule_y, o.rule_z = rule["pitch"], rule["x"], rule["y"], rule["z"]
@@ -348,7 +353,9 @@ class Batch:
         _check(lib().ssb_batch_download(self._h))
 
     def health(self):
-        """Flags of the last run: 0, or 1 when an instance's state went NaN or infinite (HEALTH_NON_FINITE)."""
+        """Flags of the last run: 0, or 1 when an instance's state went NaN or infinite (HEALTH_NON_FINITE), 2 when a
+        block read the column table from global memory because its staged copy did not arrive in time
+        (HEALTH_STAGE_TIMEOUT)."""
         f = C.c_int32()
         _check(lib().ssb_batch_health(self._h, C.byref(f)))
         return f.value

@@ -405,14 +405,15 @@ class AdjointEvaluator:
 
 # ------------------------------------------------------------------------------------------ optimisers
 
-def lbfgs_batched(fg, x0, max_iter=50, memory=8, f_target=None, rel_tol=1e-12, c1=1e-4, max_backtracks=12, callback=None):
+def lbfgs_batched(fg, x0, max_iter=50, memory=8, f_target=None, rel_tol=1e-12, c1=1e-4, max_backtracks=12, callback=None, max_step=None):
     """L-BFGS on many independent starting points at once; fg(X [K, P]) -> (f [K], g [K, P]) evaluates all of its rows
     in one call (one GPU batch).
 
     Each iteration evaluates every active point's trial step together; a point whose trial fails the Armijo test
     halves its step and retries in the next call. A point stops when f <= f_target, when its relative decrease falls
-    below rel_tol, or after max_iter iterations. Returns (x, f, info) with info = {iterations, evaluations,
-    history: [best f after each call]}."""
+    below rel_tol, or after max_iter iterations. With max_step, a trial step is at most that long (Euclidean, in
+    parameter units): curvature pairs from a rough objective can make the quasi-Newton direction very long. Returns
+    (x, f, info) with info = {iterations, evaluations, history: [best f after each call]}."""
     x = np.array(x0, dtype=np.float64, copy=True)
     r, p = x.shape
     f, g = fg(x)
@@ -459,6 +460,8 @@ def lbfgs_batched(fg, x0, max_iter=50, memory=8, f_target=None, rel_tol=1e-12, c
                 dirs[i] = direction(i)
                 gnorm = float(np.linalg.norm(g[i]))
                 steps[i] = 1.0 if S[i] else min(1.0, 0.1 / max(gnorm, 1e-300))
+                if max_step is not None:
+                    steps[i] = min(steps[i], max_step / max(float(np.linalg.norm(dirs[i])), 1e-300))
                 backtracks[i] = 0
                 fresh[i] = False
         trial = x[idx] + steps[idx, None] * dirs[idx]
@@ -492,14 +495,15 @@ def lbfgs_batched(fg, x0, max_iter=50, memory=8, f_target=None, rel_tol=1e-12, c
     return x, f, {"iterations": iters, "evaluations": calls, "history": history}
 
 
-def lbfgs_device(fg, x0, max_iter=30, memory=8, rel_target=None, c1=1e-4, max_backtracks=12, device="cuda", callback=None):
+def lbfgs_device(fg, x0, max_iter=30, memory=8, rel_target=None, c1=1e-4, max_backtracks=12, device="cuda", callback=None, max_step=None):
     """L-BFGS on many independent starting points at once with its state on the GPU: points, gradients, the curvature
     pairs of every restart (a ring of `memory` pairs each), the two-loop recursion and the Armijo backtracking are
     torch float64 tensors on `device`, computed for all restarts together. fg(X) takes and returns device tensors
     (X [R, P] -> f [R], g [R, P]) and is called on every row each time (rows that stopped keep their point), so the
     evaluator's batch keeps its size. A restart stops when f <= rel_target x its starting f, after max_iter accepted
-    steps, or after max_backtracks halvings of one step. Returns (x, f, info) as tensors on the device; info holds
-    the evaluation count and the best objective after each evaluation."""
+    steps, or after max_backtracks halvings of one step. With max_step, a trial step is at most that long (as in
+    lbfgs_batched). Returns (x, f, info) as tensors on the device; info holds the evaluation count and the best
+    objective after each evaluation."""
     import torch
 
     x = torch.as_tensor(x0, dtype=torch.float64, device=device).clone()
@@ -551,6 +555,8 @@ def lbfgs_device(fg, x0, max_iter=30, memory=8, rel_target=None, c1=1e-4, max_ba
             d = torch.where(fresh[:, None], nd, d)
             gnorm = g.norm(dim=1)
             first = torch.where(count > 0, torch.ones_like(step), torch.clamp(0.1 / gnorm.clamp_min(1e-300), max=1.0))
+            if max_step is not None:
+                first = torch.minimum(first, max_step / d.norm(dim=1).clamp_min(1e-300))
             step = torch.where(fresh, first, step)
             backtracks = torch.where(fresh, torch.zeros_like(backtracks), backtracks)
             fresh = torch.zeros_like(fresh)
@@ -671,6 +677,7 @@ def main(argv=None):
     ap.add_argument("--gradient", default="fd", choices=("fd", "adjoint"),
                     help="fd: central differences on the batched forward (L-BFGS in host numpy); adjoint: the engine's adjoint "
                          "with the L-BFGS state on the GPU (torch)")
+    ap.add_argument("--max-step", type=float, default=0.3, help="longest L-BFGS trial step, in parameter units (0: no limit)")
     ap.add_argument("--rel-target", type=float, default=None, help="stop a restart once its objective falls below this fraction of its start")
     ap.add_argument("--t-end", type=float, default=7920.0, help="s: the last of the 8 objective times")
     ap.add_argument("--liner", action="store_true", help="the generated benchmark liner (hullgen) instead of titanic64")
@@ -737,7 +744,7 @@ def main(argv=None):
             note(f)
             return torch.as_tensor(f, device=dev), torch.as_tensor(g, device=dev)
 
-        xt, ft, info = lbfgs_device(fg, x0, max_iter=args.iters, rel_target=args.rel_target, device=dev)
+        xt, ft, info = lbfgs_device(fg, x0, max_iter=args.iters, rel_target=args.rel_target, device=dev, max_step=args.max_step or None)
         x, fx = xt.cpu().numpy(), ft.cpu().numpy()
         ev.device_ms += adj.device_ms
         ev.instances += adj.instances
@@ -747,7 +754,7 @@ def main(argv=None):
             note(f)
             return f, g
 
-        x, fx, info = lbfgs_batched(fg_fd, x0, max_iter=args.iters)
+        x, fx, info = lbfgs_batched(fg_fd, x0, max_iter=args.iters, max_step=args.max_step or None)
     wall = ranks.max(time.time() - t0)
     device_s = ranks.max(ev.device_ms / 1e3)
     instances = ranks.sum(float(ev.instances))
@@ -760,6 +767,7 @@ def main(argv=None):
             hit = next((t for t, b in trace if b <= level * start), None)
             reached[f"{level:g}"] = hit
         print(json.dumps({"gradient": args.gradient, "restarts": args.restarts, "gpus": ranks.world, "space": args.space,
+                          "t_end": args.t_end, "iters": args.iters, "max_step": args.max_step,
                           "best_objective": float(fx[best]), "start_objective": start, "relative_objective": float(fx[best]) / start,
                           "wall_s_to_relative": reached, "recovery_error": float(np.max(np.abs(x[best] - hidden))),
                           "hidden": [float(v) for v in hidden], "best_point": [float(v) for v in x[best]],

@@ -216,11 +216,15 @@ void Batch::init(std::vector<std::pair<std::shared_ptr<const CompiledShip>, Comp
     p.layout = I.layout_for(W);
     const SlotLayout& L = p.layout;
     if (L.bytes > optin) throw std::runtime_error("Batch: a " + std::to_string(W) + "-warp simulation needs more shared memory than a block has");
-    const int maxTeams = std::min(static_cast<int>(optin / L.bytes), kMaxWarpsPerBlock / W);
+    // the column table beside the slots when asked for and one simulation still fits beside it
+    const std::size_t table = opt_.stageColumns && !fleet ? column_stage_bytes(opt_.mixedPrecision, I.m0().dm.ncol) : 0;
+    p.stageColumns = table > 0 && table + L.bytes <= optin;
+    const std::size_t room = p.stageColumns ? optin - table : optin;
+    const int maxTeams = std::min(static_cast<int>(room / L.bytes), kMaxWarpsPerBlock / W);
     int tpb = teamsReq > 0 ? teamsReq : std::max(1, std::min(maxTeams, (count + sms - 1) / sms));
     tpb = std::max(1, std::min(tpb, maxTeams));
     p.teamsPerBlock = tpb;
-    const std::size_t smem = static_cast<std::size_t>(tpb) * L.bytes;
+    const std::size_t smem = static_cast<std::size_t>(tpb) * L.bytes + (p.stageColumns ? table : 0);
     check(configure_batch_kernel(opt_.mixedPrecision, W, smem, fleet), "cudaFuncSetAttribute");
     check(batch_kernel_occupancy(opt_.mixedPrecision, W, tpb, smem, &p.blocksPerSM, fleet), "occupancy");
     if (p.blocksPerSM < 1) throw std::runtime_error("Batch: the kernel cannot be resident with " + std::to_string(tpb) + " simulations per block");
@@ -498,6 +502,7 @@ float Batch::launch() {
     for (std::size_t k = 0; k < nph; ++k) {
       dbs[k] = I.devBatch(opt_, maxSteps, k == 0 ? 1 : 0);
       dbs[k].yieldBelow = cfg_.phases[k].yieldBelow;
+      dbs[k].stageColumns = cfg_.phases[k].stageColumns ? 1 : 0;
       dbs[k].phaseSteps = I.phaseSteps.get() + k;
       if (ordered_phase(opt_, cfg_, k)) { dbs[k].order = I.order.get(); dbs[k].orderCount = I.orderCount.get(); }
       if (k == 0 && !I.hOrder0.empty()) { dbs[k].order = I.order0.get(); dbs[k].orderCount = I.order0Count.get(); }
@@ -552,7 +557,6 @@ float Batch::launch() {
     float ms = 0;
     check(cudaEventElapsedTime(&ms, I.ev0, I.ev1), "cudaEventElapsedTime");
     I.phaseSteps.download(I.lastPhaseSteps, s);
-  I.error.download(I.lastHealth, s);
     I.error.download(I.lastHealth, s);
     check(cudaStreamSynchronize(s), "copy to host");
     return ms;
@@ -569,6 +573,7 @@ float Batch::launch() {
       check(cudaMemsetAsync(I.queue.get(), 0, sizeof(std::int32_t), s), "memset");
       DevBatch db = I.devBatch(opt_, maxSteps, first);
       db.yieldBelow = p.yieldBelow;
+      db.stageColumns = p.stageColumns ? 1 : 0;
       db.phaseSteps = I.phaseSteps.get() + k;
       if (k == 0 && !I.hOrder0.empty()) { db.order = I.order0.get(); db.orderCount = I.order0Count.get(); }
       check(launch_batch_kernel(opt_.mixedPrecision, p.teamWarps, I.m0().dm, db, p.layout, p.blocks, p.teamsPerBlock, s), "kernel launch");

@@ -36,6 +36,8 @@ struct BatchOptions {
   RetireRule rule{};
   bool stopWhenStable = false;     // the reference's calm rule (a sweep's "stopWhenStable"); exclusive with `rule`
   bool claimByIndex = false;       // phases after the first claim by index instead of fewest steps done first
+  bool stageColumns = false;       // every block copies the column table into its shared memory (single-model batches;
+                                   // a phase whose blocks lack the room takes simulations off its blocks to make it)
   int device = 0;
 };
 
@@ -53,6 +55,7 @@ DeviceInfo device_info(int device);
 struct PhaseConfig {
   int teamWarps = 0, teamsPerBlock = 0, blocks = 0, blocksPerSM = 0;
   int yieldBelow = 0;  // the phase pauses its instances once at most this many remain (0: never)
+  bool stageColumns = false;  // its blocks hold the column table in shared memory
   SlotLayout layout{};
 };
 

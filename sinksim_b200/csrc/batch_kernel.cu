@@ -25,6 +25,61 @@ namespace ssb {
 namespace {
 
 constexpr int kYieldCheckEvery = 64;
+// try_wait rounds a block waits for its column table to arrive before it reads the table from global memory instead
+constexpr int kStageWaitLimit = 1 << 20;
+
+// Copies the column table (xy, lh, area: ncol entries each) into the block's shared memory at dst, laid out as
+// staged_columns<T>: thread 0 starts one bulk asynchronous copy per array (the part that is a whole number of 16-byte
+// units; the rest, under 16 bytes, by plain copies) completing on an mbarrier after the table, and every thread waits
+// for the barrier's phase with a bounded number of try_wait rounds. Returns dst, or null when the wait ran out (the
+// health bit kHealthStageTimeout is set and the block reads the table from global memory). Every thread of the block
+// calls it once, before the teams diverge. The sources are cudaMalloc'd arrays, so 256-byte aligned.
+template <class T>
+__device__ const unsigned char* stage_column_table(const typename Vec2<T>::type* xy, const typename Vec2<T>::type* lh, const T* area, int ncol,
+                                                   unsigned char* dst, std::int32_t* error) {
+  using V2 = typename Vec2<T>::type;
+  const StagedColumns<T> c = staged_columns<T>(ncol);
+  const auto bar = static_cast<unsigned>(__cvta_generic_to_shared(dst + c.bytes));
+  const std::size_t n = static_cast<std::size_t>(ncol);
+  const std::size_t size[3] = {n * sizeof(V2), n * sizeof(V2), n * sizeof(T)};
+  const unsigned char* src[3] = {reinterpret_cast<const unsigned char*>(xy), reinterpret_cast<const unsigned char*>(lh),
+                                 reinterpret_cast<const unsigned char*>(area)};
+  const std::size_t off[3] = {c.xy, c.lh, c.area};
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned total = 0;
+    for (int k = 0; k < 3; ++k) total += static_cast<unsigned>(size[k] & ~static_cast<std::size_t>(15));
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total) : "memory");
+    for (int k = 0; k < 3; ++k) {
+      const auto bulk = static_cast<unsigned>(size[k] & ~static_cast<std::size_t>(15));
+      const auto to = static_cast<unsigned>(__cvta_generic_to_shared(dst + off[k]));
+      if (bulk)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(to), "l"(src[k]),
+                     "r"(bulk), "r"(bar)
+                     : "memory");
+      for (std::size_t b = bulk; b < size[k]; ++b) dst[off[k] + b] = src[k][b];
+    }
+  }
+  bool done = false;
+  for (int it = 0; it < kStageWaitLimit && !done; ++it) {
+    unsigned ready;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ready)
+        : "r"(bar)
+        : "memory");
+    done = ready != 0;
+  }
+  if (!__syncthreads_and(done ? 1 : 0)) {
+    if (threadIdx.x == 0) atomicOr(error, kHealthStageTimeout);
+    return nullptr;
+  }
+  return dst;
+}
 
 template <int W>
 __device__ __forceinline__ void write_record(double* rec, const SimRegs& R, const Slot& S, int nn, const Team<W>& T) {
@@ -88,7 +143,7 @@ __device__ bool run_instance(const DevModel& M, const DevBatch& B, Slot& S, int 
   if (traced && done == 0 && denseCount == 0) {
     // the initial record: buoyancy at the initial pose and no inflow (the reference's Simulation::record_trace)
     const Pose F0 = make_pose(M, R.zO, R.pitch, R.roll);
-    const Buoy hb = buoyancy<MIXED, W>(M, F0, T, S.hydro);
+    const Buoy hb = buoyancy<MIXED, W>(M, F0, T, S.hydro, S.cols);
     R.inflow = 0; R.Vb = hb.V; R.hullTop = hb.top; R.bx = hb.x; R.by = hb.y; R.bz = hb.z;
     write_record(denseBase, R, S, M.nn, T);
     write_record(sampleBase, R, S, M.nn, T);
@@ -196,6 +251,14 @@ __global__ void __launch_bounds__(kMaxWarpsPerBlock * 32, kMinBlocksPerSM) run_b
   T.bar = team + 1;
   unsigned char* const slot = smem + static_cast<std::size_t>(team) * L.bytes;
   Slot S = carve_slot(slot, L);
+  if constexpr (!FLEET) {
+    if (B.stageColumns) {
+      // the column table after the block's slots (one copy per block for the whole launch)
+      unsigned char* const table = smem + static_cast<std::size_t>(blockDim.x / (32 * W)) * L.bytes;
+      if constexpr (MIXED) S.cols = stage_column_table<float>(M.colXYf, M.colLHf, M.colAf, M.ncol, table, B.error);
+      else S.cols = stage_column_table<double>(M.colXY, M.colLH, M.colA, M.ncol, table, B.error);
+    }
+  }
   for (;;) {
     if (T.leader()) {
       const int q = atomicAdd(B.queue, 1);
@@ -260,6 +323,11 @@ void launch(int W, const DevModel& M, const DevBatch& B, const SlotLayout& L, in
 
 bool valid_team_size(int W) { return W == 1 || W == 2 || W == 4 || W == 8 || W == 16; }
 
+std::size_t column_stage_bytes(bool mixed, int ncol) {
+  // the table, then its 8-byte mbarrier (kept at a 16-byte boundary)
+  return (mixed ? staged_columns<float>(ncol).bytes : staged_columns<double>(ncol).bytes) + 16;
+}
+
 cudaError_t configure_batch_kernel(bool mixed, int teamWarps, std::size_t smemBytes, bool fleet) {
   if (!valid_team_size(teamWarps)) return cudaErrorInvalidValue;
   if (fleet) return mixed ? set_smem<true, true>(teamWarps, smemBytes) : set_smem<false, true>(teamWarps, smemBytes);
@@ -269,9 +337,9 @@ cudaError_t configure_batch_kernel(bool mixed, int teamWarps, std::size_t smemBy
 cudaError_t launch_batch_kernel(bool mixed, int teamWarps, const DevModel& M, const DevBatch& B, const SlotLayout& L, int grid,
                                 int teamsPerBlock, cudaStream_t stream) {
   if (!valid_team_size(teamWarps) || teamsPerBlock * teamWarps > kMaxWarpsPerBlock) return cudaErrorInvalidValue;
-  const std::size_t smem = static_cast<std::size_t>(teamsPerBlock) * L.bytes;
-  const int threads = teamsPerBlock * teamWarps * 32;
   const bool fleet = B.models != nullptr;
+  const std::size_t smem = static_cast<std::size_t>(teamsPerBlock) * L.bytes + (B.stageColumns && !fleet ? column_stage_bytes(mixed, M.ncol) : 0);
+  const int threads = teamsPerBlock * teamWarps * 32;
   if (fleet) {
     if (mixed) launch<true, true>(teamWarps, M, B, L, grid, threads, smem, stream);
     else launch<false, true>(teamWarps, M, B, L, grid, threads, smem, stream);

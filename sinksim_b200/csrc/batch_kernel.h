@@ -24,6 +24,8 @@ static_assert(kMaxWarpsPerBlock >= 8, "a block must hold an eight-warp team");
 
 bool valid_team_size(int teamWarps);
 cudaError_t configure_batch_kernel(bool mixed, int teamWarps, std::size_t smemBytes, bool fleet = false);
+// Shared memory a block needs beyond its slots to hold the column table (DevBatch::stageColumns).
+std::size_t column_stage_bytes(bool mixed, int ncol);
 cudaError_t launch_batch_kernel(bool mixed, int teamWarps, const DevModel& M, const DevBatch& B, const SlotLayout& L, int grid,
                                 int teamsPerBlock, cudaStream_t stream);
 cudaError_t batch_kernel_occupancy(bool mixed, int teamWarps, int teamsPerBlock, std::size_t smemBytes, int* blocksPerSM, bool fleet = false);

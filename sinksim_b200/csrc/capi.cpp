@@ -98,6 +98,7 @@ ssb::BatchOptions to_options(const ssb_batch_options& o) {
   b.stopWhenStable = o.stop_when_stable != 0;
   if (o.handover_factor > 0) b.handoverFactor = o.handover_factor;
   b.claimByIndex = o.claim_by_index != 0;
+  b.stageColumns = o.stage_columns != 0;
   return b;
 }
 

@@ -91,7 +91,9 @@ enum StopReason : std::int32_t { kRunning = 0, kFoundered = 1, kTimeLimit = 2, k
 // Bits of DevBatch::error, which a batch run reports to the host: kHealthNonFinite, an instance's rigid-body state
 // (heave, pitch, roll or their rates) was not finite when the kernel stored it (a NaN or infinity in an input, or a
 // model that diverged). The physics is not changed by it: the instance's results are what the step computed.
-enum HealthBit : std::int32_t { kHealthNonFinite = 1 };
+// kHealthStageTimeout: a block's copy of the column table into shared memory (stageColumns) did not complete within
+// its wait limit; that block read the table from global memory instead, with the same results.
+enum HealthBit : std::int32_t { kHealthNonFinite = 1, kHealthStageTimeout = 2 };
 
 struct DevBatch {
   std::int32_t count;
@@ -138,6 +140,9 @@ struct DevBatch {
   std::int32_t stopWhenStable;
   std::int32_t* queue;         // work-queue head (atomic), reset to 0 before each launch
   std::int32_t* error;         // HealthBit flags of the run (0 = none), or-ed by the kernels and read back by the host
+  // 1: every block first copies the model's column table (the arrays the buoyancy reads, in the arithmetic's type)
+  // into its shared memory after its slots, by bulk asynchronous copies, and the buoyancy reads it from there
+  std::int32_t stageColumns;
   // adaptive team size: instances not yet stopped (atomic, set to count before the first launch); a launch with
   // yieldBelow > 0 pauses its instances and stops claiming new ones once at most yieldBelow remain, so that the
   // next launch resumes them with larger teams (shorter steps)

@@ -140,35 +140,70 @@ template <class T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
+// A load of the column table: through the read-only data cache from global memory, or from shared memory (SMEM: the
+// table staged there).
+template <bool SMEM, class P>
+__device__ __forceinline__ P load_col(const P* p) {
+  if constexpr (SMEM) return *p;
+  else return __ldg(p);
+}
+
 // Lane `lane`'s partial of tree w: columns w*32 + lane + 256 k in increasing k, two at a time (loads of the second
 // column issue before the first is clipped; the clips stay in order).
-template <class T>
+template <class T, bool SMEM = false>
 __device__ __forceinline__ ColPartial<T> column_partial(const typename Vec2<T>::type* xy, const typename Vec2<T>::type* lh, const T* area,
                                                         int ncol, int first, T R20, T R21, T R22, T tz, T iR) {
   ColPartial<T> p{T(0), T(0), T(0), T(0), T(-1e9)};
   int i = first;
   for (; i + 256 < ncol; i += 512) {
-    const auto a0 = __ldg(xy + i), b0 = __ldg(lh + i), a1 = __ldg(xy + i + 256), b1 = __ldg(lh + i + 256);
-    const T A0 = __ldg(area + i), A1 = __ldg(area + i + 256);
+    const auto a0 = load_col<SMEM>(xy + i), b0 = load_col<SMEM>(lh + i), a1 = load_col<SMEM>(xy + i + 256), b1 = load_col<SMEM>(lh + i + 256);
+    const T A0 = load_col<SMEM>(area + i), A1 = load_col<SMEM>(area + i + 256);
     clip_column<T>(a0.x, a0.y, b0.x, b0.y, A0, R20, R21, R22, tz, iR, p);
     clip_column<T>(a1.x, a1.y, b1.x, b1.y, A1, R20, R21, R22, tz, iR, p);
   }
   if (i < ncol) {
-    const auto a0 = __ldg(xy + i), b0 = __ldg(lh + i);
-    clip_column<T>(a0.x, a0.y, b0.x, b0.y, __ldg(area + i), R20, R21, R22, tz, iR, p);
+    const auto a0 = load_col<SMEM>(xy + i), b0 = load_col<SMEM>(lh + i);
+    clip_column<T>(a0.x, a0.y, b0.x, b0.y, load_col<SMEM>(area + i), R20, R21, R22, tz, iR, p);
   }
   return p;
+}
+
+// The column table staged in shared memory (stage_columns): (x, y) pairs, (zlo, zhi) pairs and footprints of every
+// column, in the arithmetic's type, each array at a 16-byte boundary.
+template <class T>
+struct StagedColumns {
+  std::size_t xy, lh, area, bytes;
+};
+
+template <class T>
+__host__ __device__ __forceinline__ StagedColumns<T> staged_columns(int ncol) {
+  using V2 = typename Vec2<T>::type;
+  StagedColumns<T> c;
+  const std::size_t n = static_cast<std::size_t>(ncol);
+  auto up16 = [](std::size_t b) { return (b + 15) & ~static_cast<std::size_t>(15); };
+  c.xy = 0;
+  c.lh = up16(n * sizeof(V2));
+  c.area = c.lh + up16(n * sizeof(V2));
+  c.bytes = c.area + up16(n * sizeof(T));
+  return c;
 }
 
 // The eight trees are spread over the team's warps (warp v computes trees v, v + W, ...); the tree results meet in
 // shared memory and every thread adds them in the reference's order (trees 0..7).
 template <bool MIXED, int W>
-__device__ __forceinline__ Buoy buoyancy(const DevModel& M, const Pose& F, const Team<W>& T, double* trees) {
+__device__ __forceinline__ Buoy buoyancy(const DevModel& M, const Pose& F, const Team<W>& T, double* trees, const unsigned char* cols) {
   const int lane = T.lane;
   for (int w = T.warp; w < 8; w += W) {
     double g[5];
     if constexpr (!MIXED) {
-      ColPartial<double> p = column_partial<double>(M.colXY, M.colLH, M.colA, M.ncol, w * kLanes + lane, F.R20, F.R21, F.R22, F.tz, F.iR);
+      ColPartial<double> p;
+      if (cols) {
+        const StagedColumns<double> c = staged_columns<double>(M.ncol);
+        p = column_partial<double, true>(reinterpret_cast<const double2*>(cols + c.xy), reinterpret_cast<const double2*>(cols + c.lh),
+                                         reinterpret_cast<const double*>(cols + c.area), M.ncol, w * kLanes + lane, F.R20, F.R21, F.R22, F.tz, F.iR);
+      } else {
+        p = column_partial<double>(M.colXY, M.colLH, M.colA, M.ncol, w * kLanes + lane, F.R20, F.R21, F.R22, F.tz, F.iR);
+      }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
         p.V = bsum(p.V, off); p.Mx = bsum(p.Mx, off); p.My = bsum(p.My, off); p.Mz = bsum(p.Mz, off);
@@ -176,7 +211,14 @@ __device__ __forceinline__ Buoy buoyancy(const DevModel& M, const Pose& F, const
       }
       g[0] = p.V; g[1] = p.Mx; g[2] = p.My; g[3] = p.Mz; g[4] = p.top;
     } else {
-      ColPartial<float> p = column_partial<float>(M.colXYf, M.colLHf, M.colAf, M.ncol, w * kLanes + lane, F.fR20, F.fR21, F.fR22, F.ftz, F.fiR);
+      ColPartial<float> p;
+      if (cols) {
+        const StagedColumns<float> c = staged_columns<float>(M.ncol);
+        p = column_partial<float, true>(reinterpret_cast<const float2*>(cols + c.xy), reinterpret_cast<const float2*>(cols + c.lh),
+                                        reinterpret_cast<const float*>(cols + c.area), M.ncol, w * kLanes + lane, F.fR20, F.fR21, F.fR22, F.ftz, F.fiR);
+      } else {
+        p = column_partial<float>(M.colXYf, M.colLHf, M.colAf, M.ncol, w * kLanes + lane, F.fR20, F.fR21, F.fR22, F.ftz, F.fiR);
+      }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
         p.V = bsum(p.V, off); p.Mx = bsum(p.Mx, off); p.My = bsum(p.My, off); p.Mz = bsum(p.Mz, off);
@@ -330,6 +372,7 @@ struct Slot {
   Pose* pose;
   Buoy* buoy;
   Parked* parked;
+  const unsigned char* cols;  // the column table staged in the block's shared memory, or null (read from global)
 };
 
 __device__ __forceinline__ Slot carve_slot(unsigned char* base, const SlotLayout& L) {
@@ -355,6 +398,7 @@ __device__ __forceinline__ Slot carve_slot(unsigned char* base, const SlotLayout
   s.pose = reinterpret_cast<Pose*>(base + L.pose);
   s.buoy = reinterpret_cast<Buoy*>(base + L.buoy);
   s.parked = reinterpret_cast<Parked*>(base + L.parked);
+  s.cols = nullptr;
   return s;
 }
 
@@ -718,7 +762,7 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
   const int lane = T.lane, rank = T.rank;
   const double tNow = R.t;
   park(S.parked, R);  // until the volume update; no thread reads it before the barrier that ends that phase
-  *S.buoy = buoyancy<MIXED, W>(M, F, T, S.hydro);  // every thread stores the same values
+  *S.buoy = buoyancy<MIXED, W>(M, F, T, S.hydro, S.cols);  // every thread stores the same values
   solve_levels<MIXED, W>(M, F, S, T, tape);
   T.sync();
   tape.solved(M, S, T);

@@ -125,7 +125,10 @@ def test_launch_shape_does_not_change_bits(model):
               dict(team_warps=1, teams_per_block=4, blocks=1, tail_team_warps=4, yield_below=19),
               dict(team_warps=1, teams_per_block=4, blocks=1, tail_team_warps=4, yield_below=19, claim_by_index=True),
               # the caller's claim order for the first phase (last instance first)
-              dict(team_warps=1, teams_per_block=4, blocks=1, tail_team_warps=4, yield_below=19, _order=list(range(19, -1, -1)))]
+              dict(team_warps=1, teams_per_block=4, blocks=1, tail_team_warps=4, yield_below=19, _order=list(range(19, -1, -1))),
+              # the column table in every block's shared memory
+              dict(stage_columns=True), dict(team_warps=2, tail_team_warps=16, yield_below=20, stage_columns=True),
+              dict(steps_per_launch=777, stage_columns=True)]
     for kw in shapes:
         kw = dict(kw)
         order = kw.pop("_order", None)
@@ -144,3 +147,22 @@ def test_launch_shape_does_not_change_bits(model):
         else:
             np.testing.assert_array_equal(states, ref[0], err_msg=str(kw))
             assert steps == ref[1]
+
+
+@pytest.mark.parametrize("numerics", ["portable", "portable32"])
+def test_staged_column_table_gives_the_same_bits(model, numerics):
+    """Every block copies the column table into its shared memory by bulk asynchronous copies (stage_columns) and the
+    buoyancy reads it there: the same states, steps and curves as reading it from global memory, and no block gave up
+    waiting for its copy (health 0)."""
+    ship_p, sim_p, _, sim = model
+    out = []
+    for stage in (False, True):
+        b, _ = _perturbed_batch(ship_p, sim_p, sim, 40, numerics, 1800.0, curve_every=60.0, stage_columns=stage)
+        b.run()
+        assert b.health() == 0, (numerics, stage)
+        out.append((np.stack([b.state(i) for i in range(40)]), [b.summary(i)["steps"] for i in range(40)], [b.curve(i) for i in range(40)]))
+        b.close()
+    np.testing.assert_array_equal(out[1][0], out[0][0])
+    assert out[1][1] == out[0][1]
+    for i in range(40):
+        np.testing.assert_array_equal(out[1][2][i], out[0][2][i], err_msg=f"instance {i} curve")
