@@ -103,6 +103,7 @@ typedef struct ssb_launch_info {
   int32_t phases;       /* launch phases of one run: from the main team size up to the tail's */
   int32_t kernels;      /* kernel launches of one run to the end: the counters' reset, the phases and, before each
                            phase after the first, the two kernels of its claim order */
+  int32_t staged_phases; /* phases whose blocks hold the column table in shared memory (stage_columns) */
 } ssb_launch_info;
 
 /* The message of the last failure on this thread. */

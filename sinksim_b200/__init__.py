@@ -55,7 +55,7 @@ class _Summary(C.Structure):
 class _LaunchInfo(C.Structure):
     _fields_ = [(k, C.c_int32) for k in ("team_warps", "teams_per_block", "blocks", "blocks_per_sm", "yield_below", "tail_team_warps",
                                          "tail_teams_per_block", "tail_blocks", "tail_blocks_per_sm")] + [("slot_bytes", C.c_uint64), ("phases", C.c_int32),
-                                                                                            ("kernels", C.c_int32)]
+                                                                                            ("kernels", C.c_int32), ("staged_phases", C.c_int32)]
 
 
 _lib = None

@@ -217,7 +217,7 @@ void Batch::init(std::vector<std::pair<std::shared_ptr<const CompiledShip>, Comp
     const SlotLayout& L = p.layout;
     if (L.bytes > optin) throw std::runtime_error("Batch: a " + std::to_string(W) + "-warp simulation needs more shared memory than a block has");
     // the column table beside the slots when asked for and one simulation still fits beside it
-    const std::size_t table = opt_.stageColumns && !fleet ? column_stage_bytes(opt_.mixedPrecision, I.m0().dm.ncol) : 0;
+    const std::size_t table = opt_.stageColumns && !fleet ? column_stage_bytes(opt_.mixedPrecision, I.m0().ship->columns()) : 0;
     p.stageColumns = table > 0 && table + L.bytes <= optin;
     const std::size_t room = p.stageColumns ? optin - table : optin;
     const int maxTeams = std::min(static_cast<int>(room / L.bytes), kMaxWarpsPerBlock / W);

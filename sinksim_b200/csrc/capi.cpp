@@ -222,6 +222,8 @@ int ssb_batch_launch_info(const ssb_batch* b, ssb_launch_info* out) {
     out->slot_bytes = c.slotBytes;
     out->phases = static_cast<int32_t>(c.phases.size());
     out->kernels = ssb::kernels_per_run(b->batch->options(), c);
+    out->staged_phases = 0;
+    for (const ssb::PhaseConfig& p : c.phases) out->staged_phases += p.stageColumns ? 1 : 0;
   });
 }
 

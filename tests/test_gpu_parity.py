@@ -158,6 +158,8 @@ def test_staged_column_table_gives_the_same_bits(model, numerics):
     out = []
     for stage in (False, True):
         b, _ = _perturbed_batch(ship_p, sim_p, sim, 40, numerics, 1800.0, curve_every=60.0, stage_columns=stage)
+        info = b.launch_info()
+        assert (info["staged_phases"] == info["phases"]) if stage else info["staged_phases"] == 0, info
         b.run()
         assert b.health() == 0, (numerics, stage)
         out.append((np.stack([b.state(i) for i in range(40)]), [b.summary(i)["steps"] for i in range(40)], [b.curve(i) for i in range(40)]))
