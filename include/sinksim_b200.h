@@ -275,6 +275,11 @@ int ssb_adjoint_set_connection_areas(ssb_adjoint* a, int32_t first, int32_t coun
                                      const double* areas);
 /* n sample times (ascending) and the targets trim[i * n + k], heave[i * n + k] of every instance. */
 int ssb_adjoint_set_objective(ssb_adjoint* a, int32_t n, const double* times, const double* trim, const double* heave);
+/* The order in which the adjoint's teams claim the instances: order[0 .. n) a permutation of 0 .. count-1 (n == count;
+ * SSB_EINVAL otherwise), or order NULL / n 0 for index order (the default). When there are more instances than teams,
+ * the longest runs listed first (known from an earlier evaluation of similar points) end the call sooner. The results
+ * do not depend on it. */
+int ssb_adjoint_set_claim_order(ssb_adjoint* a, const int32_t* order, int32_t n);
 /* Memory for step records, all teams together, in bytes. A team keeps the records of its run's last steps in a ring
  * of budget / teams bytes, at least one segment (checkpoint_every records of the largest size); the reverse recomputes
  * from its checkpoint only a segment the ring no longer holds. 0, the default: room for a whole run of t_max with two

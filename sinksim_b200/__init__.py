@@ -114,6 +114,7 @@ _SIGNATURES = {
     "ssb_adjoint_samples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "ssb_adjoint_phase_times": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ssb_adjoint_set_tape_budget": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "ssb_adjoint_set_claim_order": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     "ssb_adjoint_recomputed_steps": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ssb_adjoint_ring_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "ssb_adjoint_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint64),
@@ -446,6 +447,15 @@ class Adjoint:
         self.nsamples = 0
         if tape_budget:
             self.set_tape_budget(tape_budget)
+
+    def set_claim_order(self, order):
+        """The order in which the teams claim the instances (a permutation of range(count)), or None for index order;
+        see ssb_adjoint_set_claim_order. The results do not depend on it."""
+        if order is None:
+            _check(lib().ssb_adjoint_set_claim_order(self._h, None, 0))
+            return
+        o = np.ascontiguousarray(order, dtype=np.int32)
+        _check(lib().ssb_adjoint_set_claim_order(self._h, o.ctypes.data, o.size))
 
     def set_tape_budget(self, nbytes):
         """Device memory for step records, all teams together (0: a whole run's, within half the free memory at the

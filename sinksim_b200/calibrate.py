@@ -355,6 +355,7 @@ class AdjointEvaluator:
         self.space = space or ParamSpace(self.sim)
         self.t_max, self.device, self.k, self.tape_budget = float(t_max), device, checkpoint_every, tape_budget
         self._adj = None
+        self._steps = None
         self.device_ms = 0.0
         self.instances = 0
         self.last = None
@@ -382,7 +383,10 @@ class AdjointEvaluator:
         cols, areas = self.space.area_matrix(thetas)
         a.set_connection_areas(0, cols, areas)
         a.set_objective(objective.times, objective.trim, objective.heave)
+        # the previous call's run lengths (nearby points in an optimisation loop) order the claims, longest first
+        a.set_claim_order(None if self._steps is None or self._steps.size != r else np.argsort(-self._steps, kind="stable"))
         J, G, steps, err, ms = a.run()
+        self._steps = np.asarray(steps, dtype=np.int64).copy()
         if np.any(err):
             raise RuntimeError(f"the adjoint took a branch it does not differentiate in {int(np.count_nonzero(err))} instances (bits {sorted(set(err.tolist()))})")
         self.device_ms += ms

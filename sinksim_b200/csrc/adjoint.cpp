@@ -27,7 +27,8 @@ struct AdjointBatch::Impl {
   DevBuf<double> area, tOn, st, vol, level, cx, cy, cz, times, trimT, heaveT, trim, heave, J, grad, ckpt, sink;
   DevBuf<unsigned char> arena;
   DevBuf<long long> steps, phase, stepOff, recomputed;
-  DevBuf<std::int32_t> error, queue, isink;
+  DevBuf<std::int32_t> error, queue, isink, order;
+  std::vector<std::int32_t> hOrder;  // the caller's claim order (empty: by index)
   // results
   std::vector<double> rJ, rGrad, rTrim, rHeave;
   std::vector<long long> rSteps, rPhase, rRecomputed;
@@ -217,6 +218,8 @@ float AdjointBatch::run() {
   R.sampleT = I.times.get(); R.trimT = I.trimT.get(); R.heaveT = I.heaveT.get();
   R.trim = I.trim.get(); R.heave = I.heave.get(); R.J = I.J.get(); R.grad = I.grad.get(); R.steps = I.steps.get();
   R.error = I.error.get(); R.queue = I.queue.get();
+  if (!I.hOrder.empty()) I.order.upload(I.hOrder, s);
+  R.order = I.hOrder.empty() ? nullptr : I.order.get();
   R.K = K; R.maxCkpt = maxCkpt; R.ckpt = I.ckpt.get();
   R.arena = I.arena.get(); R.arenaBytes = I.ringBytes; R.stepOff = I.stepOff.get();
   R.tapeForward = I.ringBytes > minRing ? 1 : 0; R.sink = I.sink.get(); R.isink = I.isink.get();
@@ -282,6 +285,21 @@ std::int64_t AdjointBatch::recomputed_steps(std::int32_t inst) const {
   if (!I_->ran) throw std::logic_error("AdjointBatch: results before run");
   check_inst(opt_.count, inst);
   return I_->rRecomputed[static_cast<std::size_t>(inst)];
+}
+
+void AdjointBatch::set_claim_order(const std::int32_t* order, std::int32_t n) {
+  if (order == nullptr || n == 0) {
+    I_->hOrder.clear();
+    return;
+  }
+  if (n != opt_.count) throw std::invalid_argument("AdjointBatch: a claim order lists every instance once (" + std::to_string(opt_.count) + ")");
+  std::vector<char> seen(static_cast<std::size_t>(n), 0);
+  for (std::int32_t k = 0; k < n; ++k) {
+    if (order[k] < 0 || order[k] >= n || seen[static_cast<std::size_t>(order[k])])
+      throw std::invalid_argument("AdjointBatch: the claim order is not a permutation of the instances (position " + std::to_string(k) + ")");
+    seen[static_cast<std::size_t>(order[k])] = 1;
+  }
+  I_->hOrder.assign(order, order + n);
 }
 
 void AdjointBatch::set_tape_budget(std::uint64_t bytes) {

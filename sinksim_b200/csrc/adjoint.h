@@ -52,6 +52,10 @@ class AdjointBatch {
   // the team's time on the instance in the last run, ns: forward, recomputation of the segments, reverse steps
   const long long* phase_ns(std::int32_t inst) const;
   std::int64_t recomputed_steps(std::int32_t inst) const;  // steps recomputed from checkpoints in the last run
+  // The order in which the teams claim the instances (a permutation of 0 .. count-1; null or n = 0: by index). Longest
+  // runs first lets the others fill in around them when there are more instances than teams; the results do not
+  // depend on it.
+  void set_claim_order(const std::int32_t* order, std::int32_t n);
   // Bytes of step records all teams together may keep (0: a whole run's with two passes per node, within half the
   // device memory free at the next run). With room for a whole run the reverse recomputes nothing; the least is one
   // segment of K records per team, every segment then recomputed.

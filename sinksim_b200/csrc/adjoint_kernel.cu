@@ -299,7 +299,10 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
   const adj::Tape sp = adj::tape_at(A.tape, TL);
   const int NS = B.nsamples;
   for (;;) {
-    if (T.leader()) S.misc[0] = atomicAdd(B.queue, 1);
+    if (T.leader()) {
+      const int q = atomicAdd(B.queue, 1);
+      S.misc[0] = B.order == nullptr || q >= B.count ? q : B.order[q];
+    }
     T.sync();
     const int inst = S.misc[0];
     T.sync();

@@ -30,6 +30,7 @@ struct AdjRun {
   long long* steps;                             // [count]
   std::int32_t* error;                          // [count] adjoint error bits (adj::AdjointError), zeroed by the host
   std::int32_t* queue;                          // work-queue head, zeroed by the host
+  const std::int32_t* order;                    // [count] or null: queue position k claims instance order[k]
   std::int32_t K;                               // steps between checkpoints
   std::int32_t maxCkpt;                         // checkpoints per team
   double* ckpt;                                 // [teams x maxCkpt x (7 + 5 nn)]

@@ -594,6 +594,13 @@ int ssb_adjoint_set_objective(ssb_adjoint* a, int32_t n, const double* times, co
   });
 }
 
+int ssb_adjoint_set_claim_order(ssb_adjoint* a, const int32_t* order, int32_t n) {
+  return guard([&] {
+    need(a, "adjoint");
+    a->adj->set_claim_order(order, n);
+  });
+}
+
 int ssb_adjoint_set_tape_budget(ssb_adjoint* a, uint64_t bytes) {
   return guard([&] {
     need(a, "adjoint");

@@ -42,9 +42,10 @@ def _setup(ship, sim, steps, count=len(SCALES)):
     return bconns, areas, samples, times, np.array(trim), np.array(heave)
 
 
-def _run(ship_p, sim_p, ship, sim, steps, k_every=256, count=len(SCALES), tape_budget=0):
+def _run(ship_p, sim_p, ship, sim, steps, k_every=256, count=len(SCALES), tape_budget=0, order=None):
     bconns, areas, samples, times, trim, heave = _setup(ship, sim, steps, count)
     a = ssb.Adjoint(ship_p, sim_p, count=count, t_max=steps * sim["dt"], checkpoint_every=k_every, tape_budget=tape_budget)
+    a.set_claim_order(order)
     a.set_connection_areas(0, bconns, areas)
     a.set_objective(times, trim, heave)
     J, g, st, err, ms = a.run()
@@ -120,7 +121,9 @@ def test_gpu_adjoint_does_not_depend_on_the_memory_for_step_records():
     # a record is about a third of the largest, so the ring holds the last few of the 20 segments
     assert ((some["recomputed"] > 0) & (some["recomputed"] < steps - 2 * k_every)).all(), some["recomputed"]
     assert (some["recomputed"] % k_every == 0).all()
-    for name, r in (("one segment", one), ("a few segments", some)):
+    # the claim order (last instance first) changes which team takes which instance, not the results
+    rev = _run(ship_p, sim_p, ship, sim, steps, k_every, count=count, order=list(range(count - 1, -1, -1)))
+    for name, r in (("one segment", one), ("a few segments", some), ("reversed claims", rev)):
         np.testing.assert_array_equal(r["J"], whole["J"], err_msg=name)
         np.testing.assert_array_equal(r["g"], whole["g"], err_msg=name)
         np.testing.assert_array_equal(r["steps"], whole["steps"], err_msg=name)
