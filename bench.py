@@ -57,15 +57,16 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--numerics", default="portable", choices=("portable", "portable32"))
-    ap.add_argument("--count", type=int, default=4096, help="instances per GPU")
-    ap.add_argument("--tmax", type=float, default=5 * 3600.0)
+    ap.add_argument("--count", type=int, default=None, help="instances per GPU (uneven: 4096, perturbed: 264)")
+    ap.add_argument("--tmax", type=float, default=None, help="s (uneven: 5 h, perturbed: 2.6 h)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--model", default=None, choices=("titanic64", "liner"),
                     help="titanic64: the reference's compiled model; liner: the generated benchmark liner "
                          "(default: liner for --workload gradient, else titanic64)")
-    ap.add_argument("--workload", default="uneven", choices=("uneven", "fleet", "gradient"),
-                    help="uneven: one model, uneven run lengths; fleet: a mixed fleet of generated hulls in one batch; "
-                         "gradient: central-difference gradients of a trajectory objective, all stencils in one batch")
+    ap.add_argument("--workload", default="uneven", choices=("uneven", "perturbed", "fleet", "gradient"),
+                    help="uneven: one model, uneven run lengths; perturbed: the plain method's GPU form, seed-perturbed copies "
+                         "of one model (the reference's --perturb: breach areas x (1 + 0.02 i / count)) run to founder or tmax; "
+                         "fleet: a mixed fleet of generated hulls in one batch; gradient: gradients of a trajectory objective")
     ap.add_argument("--hulls", type=int, default=2048, help="fleet: hulls per GPU (one instance each)")
     ap.add_argument("--fleet-tmax", type=float, default=7200.0, help="fleet: s; instances also stop when they founder or calm down")
     ap.add_argument("--points", type=int, default=256, help="gradient: parameter points per GPU (one gradient each)")
@@ -76,7 +77,11 @@ def parse():
     ap.add_argument("--autotune", action="store_true", help="pick the launch shape by timing candidates first (outside the timed region)")
     args = ap.parse_args()
     if args.model is None:
-        args.model = "liner" if args.workload == "gradient" else "titanic64"
+        args.model = "liner" if args.workload in ("gradient", "perturbed") else "titanic64"
+    if args.count is None:
+        args.count = 264 if args.workload == "perturbed" else 4096
+    if args.tmax is None:
+        args.tmax = 2.6 * 3600.0 if args.workload == "perturbed" else 5 * 3600.0
     return args
 
 
@@ -177,12 +182,35 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_batch(ssb, ship_p, sim_p, sim, rule, count, first, args, device, **shape):
+def instance_params(sim, count, first, args, total=None):
+    """(area {conn: area}, enabled {conn: 0/1}) of instances first .. first+count-1 of the workload: the uneven batch's
+    draws, or for `perturbed` the reference's --perturb (apps/sinksim_cuda_run.cpp:126-135): every breach connection's
+    compiled area x (1 + 0.02 i / total) for instance i of `total` (i >= 1), one product each."""
     from sinksim_b200.workloads import batch_uneven
 
+    if args.workload != "perturbed":
+        return batch_uneven(sim, count, first=first)
+    total = total or count
+    kinds = list(sim["kindNames"])
+    breach = [int(c) for c in range(len(sim["kind"])) if "breach" in kinds and sim["kind"][c] == kinds.index("breach")]
+    out = []
+    for i in range(first, first + count):
+        area = {} if i == 0 else {c: float(sim["area"][c]) * (1 + 0.02 * i / total) for c in breach}
+        out.append((area, {}))
+    return out
+
+
+def workload_rule(ship, args):
+    """The uneven batch's sink/settle retire rule; the perturbed copies stop at their founder or tmax only."""
+    from sinksim_b200.workloads import deck_edge_rule
+
+    return None if args.workload == "perturbed" else deck_edge_rule(ship)
+
+
+def make_batch(ssb, ship_p, sim_p, sim, rule, count, first, args, device, total=None, **shape):
     b = ssb.Batch(ship_p, sim_p, count=count, numerics=args.numerics, t_max=args.tmax, device=device, rule=rule,
                   stage_columns=getattr(args, "stage_columns", False), **shape)
-    for i, (area, enabled) in enumerate(batch_uneven(sim, count, first=first)):
+    for i, (area, enabled) in enumerate(instance_params(sim, count, first, args, total)):
         for c, a in area.items():
             b.set_connection_area(i, c, a)
         for c, e in enabled.items():
@@ -232,13 +260,11 @@ def _reference_sweep(ship_p, sim_p, sw, numerics, threads):
     return int(m.group(1)), float(m.group(2))
 
 
-def workload_sweep(sim, count, t_max):
-    """The uneven workload's instances 0 .. count-1 as a sweep document (each instance's areas and door overrides)."""
-    from sinksim_b200.workloads import batch_uneven
-
+def workload_sweep(sim, count, t_max, args):
+    """The workload's instances 0 .. count-1 as a sweep document (each instance's areas and door overrides)."""
     sw = {"format": "sinksim.sweep", "formatVersion": 1, "ship": "", "sim": "", "tMax": t_max, "every": 30, "stopWhenStable": False,
           "instances": []}
-    for i, (area, enabled) in enumerate(batch_uneven(sim, count)):
+    for i, (area, enabled) in enumerate(instance_params(sim, count, 0, args)):
         conns = [{"conn": c, "area": a} for c, a in area.items()] + [{"conn": c, "enabled": bool(e)} for c, e in enabled.items()]
         sw["instances"].append({"id": f"i{i}", "connections": conns})
     return sw
@@ -247,7 +273,7 @@ def workload_sweep(sim, count, t_max):
 RUN_SAMPLE_SEED = 20261206
 
 
-def cpu_whole_runs_rate(ship_p, sim_p, ship, sim, numerics, count, sample, t_max, threads):
+def cpu_whole_runs_rate(ship_p, sim_p, ship, sim, numerics, count, sample, t_max, threads, args):
     """The reference CPU engine (oracle/_ref/libsinksim_ref.so, Simulation::run) on a seeded random sample of whole runs
     of the GPU workload's `count` instances: each sampled instance from its initial state to its founder, the sink or
     settle rule or t_max, exactly as the GPU batch runs it, so both engines take the same mix of steps. Returns
@@ -256,39 +282,24 @@ def cpu_whole_runs_rate(ship_p, sim_p, ship, sim, numerics, count, sample, t_max
 
     import numpy as np
 
-    from sinksim_b200.workloads import deck_edge_rule
-
     lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libsinksim_ref.so"))
     f = lib.ssref_time_sweep_runs
     f.restype = C.c_longlong
     f.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_int, C.POINTER(C.c_double)]
     lib.ssref_last_error.restype = C.c_char_p
     picks = np.sort(np.random.default_rng(RUN_SAMPLE_SEED).choice(count, size=min(sample, count), replace=False)).astype(np.int32)
-    r = deck_edge_rule(ship)
-    rule = np.array([r["pitch"], r["x"], r["y"], r["z"], r["wth"], r["settle"]], dtype=np.float64)
+    r = workload_rule(ship, args)
+    rule = None if r is None else np.array([r["pitch"], r["x"], r["y"], r["z"], r["wth"], r["settle"]], dtype=np.float64)
     with tempfile.TemporaryDirectory() as d:
         path = os.path.join(d, "workload.sweep.json")
         with open(path, "w") as fh:
-            json.dump(workload_sweep(sim, count, t_max), fh)
+            json.dump(workload_sweep(sim, count, t_max, args), fh)
         secs = C.c_double()
-        steps = f(ship_p.encode(), sim_p.encode(), path.encode(), numerics.encode(), picks.ctypes.data, picks.size, t_max, rule.ctypes.data,
-                  threads, C.byref(secs))
+        steps = f(ship_p.encode(), sim_p.encode(), path.encode(), numerics.encode(), picks.ctypes.data, picks.size, t_max,
+                  None if rule is None else rule.ctypes.data, threads, C.byref(secs))
     if steps < 0:
         raise RuntimeError(lib.ssref_last_error().decode())
     return steps / secs.value, int(steps), secs.value, picks
-
-
-def cpu_reference_rate(ship_p, sim_p, sim, numerics, instances, t_max, threads, first=0):
-    """The reference CPU engine's own sweep tool on `instances` instances of the workload; returns (steps/s, steps, s)."""
-    from sinksim_b200.workloads import batch_uneven
-
-    sw = {"format": "sinksim.sweep", "formatVersion": 1, "ship": "", "sim": "", "tMax": t_max, "every": 30, "stopWhenStable": False,
-          "instances": []}
-    for i, (area, enabled) in enumerate(batch_uneven(sim, instances, first=first)):
-        conns = [{"conn": c, "area": a} for c, a in area.items()] + [{"conn": c, "enabled": True} for c in enabled]
-        sw["instances"].append({"id": f"i{first + i}", "connections": conns})
-    steps, secs = _reference_sweep(ship_p, sim_p, sw, numerics, threads)
-    return steps / secs, steps, secs
 
 
 # The gradient workload: gradients of a trajectory objective over 10 parameters, by the adjoint (one run forward and back
@@ -341,14 +352,15 @@ def reference_arm(args):
     ship, _ = load_model(ship_p, sim_p)
     n = 8 * threads
     for _ in range(args.warmup):
-        cpu_whole_runs_rate(ship_p, sim_p, ship, sim, args.numerics, args.count, n, args.tmax, threads)
+        cpu_whole_runs_rate(ship_p, sim_p, ship, sim, args.numerics, args.count, n, args.tmax, threads, args)
     tot_steps, tot_s = 0, 0.0
     for _ in range(args.steps):
-        _, s, secs, _ = cpu_whole_runs_rate(ship_p, sim_p, ship, sim, args.numerics, args.count, n, args.tmax, threads)
+        _, s, secs, _ = cpu_whole_runs_rate(ship_p, sim_p, ship, sim, args.numerics, args.count, n, args.tmax, threads, args)
         tot_steps += s
         tot_s += secs
     v = tot_steps / tot_s
-    sample = (f"a seeded random sample of {n} of the {args.count} instances, each run whole (to its founder, the sink or settle rule or "
+    ends = "its founder or" if args.workload == "perturbed" else "its founder, the sink or settle rule or"
+    sample = (f"a seeded random sample of {n} of the {args.count} instances, each run whole (to {ends} "
               f"{args.tmax:.0f} s) by the reference engine's Simulation::run on {threads} threads; the same runs every step")
     print(json.dumps({"impl": "reference", "metric": "sim-steps/s", "value": v, "unit": "sim-steps/s", "n_gpus": args.gpus,
                       "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps, "higher_is_better": True,
@@ -429,6 +441,13 @@ def workload_config(args):
                 "retire": "founder | the reference's calm rule (stopWhenStable) | tMax",
                 "parallelism": f"hulls sharded over {args.gpus} GPU(s), no collective in the step",
                 "l2": "working set exceeds L2 for the largest hulls' geometry only; every step is a full batch from initial state"}
+    if args.workload == "perturbed":
+        return {"workload": f"{args.model}: {args.count} seed-perturbed copies per GPU (breach areas x (1 + 0.02 i / count), the "
+                            f"reference's --perturb)", "model": MODELS[args.model], "global_batch": args.count * args.gpus,
+                "numerics": args.numerics, "t_max_s": args.tmax, "dt_s": 0.25, "retire": "founder | tMax",
+                "parallelism": f"instances sharded over {args.gpus} GPU(s), no collective in the step",
+                "l2": "working set (geometry 0.6 MB, per-instance state) is L2-resident by design; every step is a full batch from initial state",
+                "column_table": "shared memory of every block (bulk asynchronous copies)" if args.stage_columns else "global memory, through L1"}
     return {"workload": f"{args.model} uneven-run-length batch, {args.count} instances per GPU", "model": MODELS[args.model],
             "global_batch": args.count * args.gpus, "numerics": args.numerics, "t_max_s": args.tmax, "dt_s": 0.25,
             "retire": "founder | sink (|trim|>15 deg, bow deck edge under) | settle (|pitch rate|<1e-5 rad/s for 600 s) | tMax",
@@ -560,8 +579,6 @@ def main():
 
     import sinksim_b200 as ssb
     from sinksim_b200.files import load_model
-    from sinksim_b200.workloads import deck_edge_rule
-
     from sinksim_b200.shard import Ranks, shard_bounds
 
     # one process per GPU; each rank steps its own contiguous block of the instances (weak scaling: count per GPU)
@@ -581,14 +598,15 @@ def main():
     else:
         ship_p, sim_p = model_paths(args.model)
         ship, sim = load_model(ship_p, sim_p)
-        rule = deck_edge_rule(ship)
+        rule = workload_rule(ship, args)
         first, _ = shard_bounds(args.count * world, world, rank)
+        total = args.count * world
         shape = {}
         if args.autotune:
             from sinksim_b200.autotune import tune
 
-            shape, _ = tune(lambda **s: make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local, **s))
-        batch = make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local, **shape)
+            shape, _ = tune(lambda **s: make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local, total, **s))
+        batch = make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local, total, **shape)
     # warm-up: full batches, untimed
     for _ in range(args.warmup):
         batch.reset()
@@ -664,10 +682,11 @@ def main():
         elif world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             n = 8 * threads
-            v, s, secs, _ = cpu_whole_runs_rate(ship_p, sim_p, ship, sim, args.numerics, args.count, n, args.tmax, threads)
+            v, s, secs, _ = cpu_whole_runs_rate(ship_p, sim_p, ship, sim, args.numerics, args.count, n, args.tmax, threads, args)
             out["cpu_baseline"] = {"value": v, "unit": "sim-steps/s", "cores": threads, "kind": "reference",
-                                   "sample": f"a seeded random sample of {n} of the {args.count} instances, each run whole (founder, sink or "
-                                             f"settle rule, {args.tmax:.0f} s) by the reference engine on {threads} threads "
+                                   "sample": f"a seeded random sample of {n} of the {args.count} instances, each run whole ("
+                                             f"{'founder' if args.workload == 'perturbed' else 'founder, sink or settle rule'}, "
+                                             f"{args.tmax:.0f} s) by the reference engine on {threads} threads "
                                              f"({s} steps in {secs:.1f} s): the same step mix as the GPU batch"}
         print(json.dumps(out))
     batch.close()
