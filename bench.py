@@ -73,6 +73,7 @@ def parse():
     ap.add_argument("--fd-steps", type=int, default=1, help="gradient: timed calls of the finite-difference arm (0: none)")
     ap.add_argument("--t-end", type=float, default=7920.0, help="gradient: s, the last of the objective's 8 times and the runs' end")
     ap.add_argument("--tape-gb", type=float, default=0.0, help="gradient: device memory for the adjoint's step records (0: chosen)")
+    ap.add_argument("--adjoint-warps", type=int, default=0, help="gradient: warps per adjoint team, 4, 8 or 16 (0: chosen)")
     ap.add_argument("--stage-columns", action="store_true", help="uneven: every block holds the column table in shared memory")
     ap.add_argument("--autotune", action="store_true", help="pick the launch shape by timing candidates first (outside the timed region)")
     args = ap.parse_args()
@@ -477,7 +478,8 @@ def gradient_bench(args):
     times, every = gradient_times(args.t_end)
     ev = BatchEvaluator(ship_p, sim_p, space=space, numerics="portable", t_max=times[-1], curve_every=every, device=local)
     target = TrajectoryObjective.from_target(ev.run(gradient_point(space, -1)[None, :])[0], times)
-    adj = AdjointEvaluator(ship_p, sim_p, space=space, t_max=times[-1], device=local, tape_budget=int(args.tape_gb * 2 ** 30))
+    adj = AdjointEvaluator(ship_p, sim_p, space=space, t_max=times[-1], device=local, tape_budget=int(args.tape_gb * 2 ** 30),
+                           team_warps=args.adjoint_warps)
     first, _ = shard_bounds(args.points * world, world, rank)
     thetas = np.stack([gradient_point(space, first + k) for k in range(args.points)])
     for _ in range(args.warmup):

@@ -347,13 +347,13 @@ class AdjointEvaluator:
     area parameter moves its connection's area one for one (and takes that connection out of its kind's sum, as it
     overrides the scaled area)."""
 
-    def __init__(self, ship_path, sim_path, space=None, t_max=7920.0, device=0, checkpoint_every=256, tape_budget=0):
+    def __init__(self, ship_path, sim_path, space=None, t_max=7920.0, device=0, checkpoint_every=256, tape_budget=0, team_warps=0):
         from .files import load_model
 
         self.ship_path, self.sim_path = ship_path, sim_path
         _, self.sim = load_model(ship_path, sim_path)
         self.space = space or ParamSpace(self.sim)
-        self.t_max, self.device, self.k, self.tape_budget = float(t_max), device, checkpoint_every, tape_budget
+        self.t_max, self.device, self.k, self.tape_budget, self.team_warps = float(t_max), device, checkpoint_every, tape_budget, team_warps
         self._adj = None
         self._steps = None
         self.device_ms = 0.0
@@ -367,7 +367,7 @@ class AdjointEvaluator:
             if self._adj is not None:
                 self._adj.close()
             self._adj = Adjoint(self.ship_path, self.sim_path, count=count, t_max=self.t_max, checkpoint_every=self.k, device=self.device,
-                                tape_budget=self.tape_budget)
+                                tape_budget=self.tape_budget, team_warps=self.team_warps)
         return self._adj
 
     def close(self):
