@@ -265,7 +265,8 @@ int ssb_batch_run_noalloc(const ssb_batch* b, int32_t count, const uint8_t* en, 
  * The gradient is d J_i / d area[c] along the branch path the run takes. */
 typedef struct ssb_adjoint ssb_adjoint;
 
-/* count instances; checkpoint_every steps between checkpoints (256 if 0); team_warps 4, 8 or 16 (0: chosen). */
+/* count instances; checkpoint_every steps between checkpoints (256 if 0); team_warps 4, 8 or 16 (0: 16 for at most two
+ * instances per SM, else 8). */
 int ssb_adjoint_create(const char* ship_path, const char* sim_path, int32_t count, double t_max, int32_t checkpoint_every,
                        int32_t team_warps, int32_t device, ssb_adjoint** out);
 void ssb_adjoint_destroy(ssb_adjoint* a);
