@@ -129,6 +129,7 @@ __device__ __forceinline__ AdjSmem carve_adjoint(unsigned char* base, const AdjL
   m.rs.faHA = d(A.faHA); m.rs.faHB = d(A.faHB); m.rs.faAA = d(A.faAA); m.rs.faAB = d(A.faAB);
   m.rs.red = d(A.red);
   m.rs.work = reinterpret_cast<adj::UnitWork*>(base + A.work);
+  m.rs.plain = base + A.plain;
   m.as.aVol = d(A.aVol); m.as.aLevel = d(A.aLevel); m.as.aCx = d(A.aCx); m.as.aCy = d(A.aCy); m.as.aCz = d(A.aCz);
   m.grad = d(A.grad);
   m.sampleS = d(A.sampleS);
@@ -418,6 +419,13 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
       const long long tRev = global_ns();
       tRecompute += tRev - tSeg;
       for (long long st = s1 - 1; st >= s0; --st) {
+        if (T.leader() && st > s0) {
+          // the next step's record (the one before this) into L2 while this one is reversed: it runs from its own
+          // offset to this record's (a whole number of 16-byte units inside the ring, the unused end of a lap included)
+          const long long o0 = off[st - 1], o1 = off[st];
+          const auto* next = ring + o0 % static_cast<long long>(B.arenaBytes);
+          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(next), "r"(static_cast<unsigned>(o1 - o0)) : "memory");
+        }
         load_record(ring + off[st] % static_cast<long long>(B.arenaBytes), sp, M.nn, A.poff, T);
         adj::reverse_step(AT, M, sp, I.en(), I.area(), I.tOn(), A.rs, A.as, aSc, A.grad, &err);
         for (int q = 0; q < NS; ++q)
@@ -463,6 +471,7 @@ AdjLayout adjoint_layout(int nn, int nc, int ng, int nsamples, int W) {
   A.faHA = take16(C); A.faHB = take16(C); A.faAA = take16(C); A.faAB = take16(C);
   A.red = take16(sizeof(double) * 16 * static_cast<std::size_t>(W));
   A.work = take16(sizeof(adj::UnitWork) * static_cast<std::size_t>(W));
+  A.plain = take16(static_cast<std::size_t>(std::max(nn, 1)));
   A.aVol = take16(N); A.aLevel = take16(N); A.aCx = take16(N); A.aCy = take16(N); A.aCz = take16(N);
   A.grad = take16(C);
   A.sampleS = take16(sizeof(double) * static_cast<std::size_t>(std::max(nsamples, 1)));

@@ -180,12 +180,19 @@ SSB_HD int pass_extreme(const DevModel& M, const PoseD& F, int n, bool want_min,
   if (width == 32) {
     double best = want_min ? 1e9 : -1e9;
     int idx = -1;
-    for (int j = s0 + lane; j < s1; j += 32) {
-      const double2 xy = M.segXY[j], ab = M.segLH[j];
+    auto seg = [&](const double2 xy, const double2 ab, int j) {
       const double base = F.R20 * xy.x + F.R21 * xy.y + F.tz;
       const double w = want_min ? base + F.R22 * ab.x : base + F.R22 * ab.y;
       if (want_min ? (w < best) : (w > best)) { best = w; idx = j; }
+    };
+    // two segments per round, both loaded before either is compared; each lane keeps its segments' order
+    int j = s0 + lane;
+    for (; j + 32 < s1; j += 64) {
+      const double2 xy0 = M.segXY[j], ab0 = M.segLH[j], xy1 = M.segXY[j + 32], ab1 = M.segLH[j + 32];
+      seg(xy0, ab0, j);
+      seg(xy1, ab1, j + 32);
     }
+    if (j < s1) seg(M.segXY[j], M.segLH[j], j);
     for (int off = 16; off > 0; off >>= 1) {
       const double ob = __shfl_xor_sync(0xffffffffu, best, off);
       const int oi = __shfl_xor_sync(0xffffffffu, idx, off);
@@ -237,18 +244,26 @@ SSB_HD double pass_sweep1(const DevModel& M, const PoseD& F, int n, double h, do
   const int s0 = M.segStart[n], s1 = s0 + M.segCount[n];
   const double mu = M.mu[n];
   double aR20 = 0, aR21 = 0, atz = 0, aiR = 0, ah = 0;
-  for (int j = s0 + lane; j < s1; j += width) {
-    const double2 xy = M.segXY[j], ab = M.segLH[j];
+  auto seg = [&](const double2 xy, const double2 ab, const double A) {
     const double base = F.R20 * xy.x + F.R21 * xy.y + F.tz;
     const double zp = (h - base) * F.iR;
-    if (!(zp > ab.x && zp < ab.y)) continue;
+    if (!(zp > ab.x && zp < ab.y)) return;
     const double L = zp - ab.x;
-    const double aL = M.segAr[j] * mu * (av + amx * xy.x + amy * xy.y + amz * (ab.x + L));
+    const double aL = A * mu * (av + amx * xy.x + amy * xy.y + amz * (ab.x + L));
     ah += aL * F.iR;
     aiR += aL * (h - base);
     const double abase = -aL * F.iR;
     aR20 += abase * xy.x; aR21 += abase * xy.y; atz += abase;
+  };
+  // two segments per round, both loaded before either is used; each lane still visits its segments in order
+  int j = s0 + lane;
+  for (; j + width < s1; j += 2 * width) {
+    const double2 xy0 = M.segXY[j], ab0 = M.segLH[j], xy1 = M.segXY[j + width], ab1 = M.segLH[j + width];
+    const double A0 = M.segAr[j], A1 = M.segAr[j + width];
+    seg(xy0, ab0, A0);
+    seg(xy1, ab1, A1);
   }
+  if (j < s1) seg(M.segXY[j], M.segLH[j], M.segAr[j]);
   aP.R20 += aR20; aP.R21 += aR21; aP.tz += atz; aP.iR += aiR;
   return ah;
 }
@@ -260,9 +275,7 @@ SSB_HD void pass_sweep_levels(const DevModel& M, const PoseD& F, int n, int np, 
   const int s0 = M.segStart[n], s1 = s0 + M.segCount[n];
   const double mu = M.mu[n];
   double aR20 = 0, aR21 = 0, atz = 0, aiR = 0;
-  for (int j = s0 + lane; j < s1; j += width) {
-    const double2 xy = M.segXY[j], ab = M.segLH[j];
-    const double A = M.segAr[j];
+  auto seg = [&](const double2 xy, const double2 ab, const double A) {
     const double base = F.R20 * xy.x + F.R21 * xy.y + F.tz;
     for (int i = 0; i < np; ++i) {
       const double zp = (h[i] - base) * F.iR;
@@ -272,7 +285,15 @@ SSB_HD void pass_sweep_levels(const DevModel& M, const PoseD& F, int n, int np, 
       const double abase = -aL * F.iR;
       aR20 += abase * xy.x; aR21 += abase * xy.y; atz += abase;
     }
+  };
+  int j = s0 + lane;
+  for (; j + width < s1; j += 2 * width) {
+    const double2 xy0 = M.segXY[j], ab0 = M.segLH[j], xy1 = M.segXY[j + width], ab1 = M.segLH[j + width];
+    const double A0 = M.segAr[j], A1 = M.segAr[j + width];
+    seg(xy0, ab0, A0);
+    seg(xy1, ab1, A1);
   }
+  if (j < s1) seg(M.segXY[j], M.segLH[j], M.segAr[j]);
   aP.R20 += aR20; aP.R21 += aR21; aP.tz += atz; aP.iR += aiR;
 }
 
@@ -281,17 +302,25 @@ SSB_HD void pass_sweep_levels(const DevModel& M, const PoseD& F, int n, int np, 
 SSB_HD void buoyancy_sweep(const DevModel& M, const PoseD& F, double aV, double aMx, double aMy, double aMz, int first, int stride,
                            AdjPose& aP) {
   double aR20 = 0, aR21 = 0, atz = 0, aiR = 0;
-  for (int i = first; i < M.ncol; i += stride) {
-    const double2 xy = M.colXY[i], lh = M.colLH[i];
+  auto col = [&](const double2 xy, const double2 lh, const double A) {
     const double base = F.R20 * xy.x + F.R21 * xy.y + F.tz;
     const double zp = -base * F.iR;
-    if (!(zp > lh.x && zp < lh.y)) continue;
+    if (!(zp > lh.x && zp < lh.y)) return;
     const double s = zp - lh.x;
-    const double as = M.colA[i] * (aV + aMx * xy.x + aMy * xy.y + aMz * (lh.x + s));
+    const double as = A * (aV + aMx * xy.x + aMy * xy.y + aMz * (lh.x + s));
     aiR -= as * base;
     const double abase = -as * F.iR;
     aR20 += abase * xy.x; aR21 += abase * xy.y; atz += abase;
+  };
+  // two columns per round, both loaded before either is used; each thread keeps its columns' order
+  int i = first;
+  for (; i + stride < M.ncol; i += 2 * stride) {
+    const double2 xy0 = M.colXY[i], lh0 = M.colLH[i], xy1 = M.colXY[i + stride], lh1 = M.colLH[i + stride];
+    const double A0 = M.colA[i], A1 = M.colA[i + stride];
+    col(xy0, lh0, A0);
+    col(xy1, lh1, A1);
   }
+  if (i < M.ncol) col(M.colXY[i], M.colLH[i], M.colA[i]);
   aP.R20 += aR20; aP.R21 += aR21; aP.tz += atz; aP.iR += aiR;
 }
 
@@ -884,6 +913,7 @@ struct RevSlot {
   double *faHA, *faHB, *faAA, *faAB;     // per connection: its flow's adjoints at its a and b ends
   double* red;                           // team reduction scratch: nwarps x 16
   UnitWork* work;                        // one per warp: the level solve's reverse, unit by unit
+  std::uint8_t* plain;                   // per node: 1 when its unit's reverse was the empty node's pass-through
 };
 
 // The adjoint of the state between steps: per node in memory, the scalars (zO, pitch, roll, vz, wth, wph) in every
@@ -1018,8 +1048,26 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
   }
   team.sync();
 
-  // ---- the level solve, unit by unit: a warp per merged group or node alone, lane 0 replaying it into the warp's
-  // work area
+  // ---- the level solve. First, thread-parallel, the units that are a node alone and empty (most of them in a
+  // flooding run), when neither its level nor its extent top has an adjoint and its one pass is the recorded start:
+  // the solver set the level to the node's extent bottom and left volume and centroid as they were, so their adjoints
+  // pass through (what unit_reverse does for such a unit, without its replay)
+  for (int g = team.rank; g < M.ng; g += team.size) {
+    const int N = M.gCount[g];
+    const int* mem = M.gNodes + M.gStart[g];
+    const bool isMerged = merged[g] != 0;
+    for (int k = 0; k < N; ++k) {
+      const int n = mem[k];
+      S.plain[n] = !isMerged && tp.d[L.volIn + n] <= kEmptyVolume && tp.i[L.npass + n] == 1 && tp.pass(n, 0)[0] == tp.d[L.levelIn + n] &&
+                   S.aLs[n] == 0 && S.aZmx[n] == 0;
+      if (!S.plain[n]) continue;
+      a.aVol[n] = 0.0 + (0.0 + S.aVs[n]);
+      a.aLevel[n] = 0.0 + 0.0;
+      a.aCx[n] = 0.0 + S.aCxs[n]; a.aCy[n] = 0.0 + S.aCys[n]; a.aCz[n] = 0.0 + S.aCzs[n];
+    }
+  }
+  team.sync();
+  // then the other units: a warp per merged group or node alone, lane 0 replaying it into the warp's work area
   bool ok = true;
   UnitWork& w = S.work[team.warp];
   for (int g = team.warp; g < M.ng; g += team.nwarps) {
@@ -1030,6 +1078,7 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
     for (int u = 0; u < units; ++u) {
       const int* um = isMerged ? mem : mem + u;
       const int un = isMerged ? N : 1;
+      if (!isMerged && S.plain[um[0]]) continue;
       if (un > kMaxMembers) { ok = false; *err |= kErrGroupSize; continue; }
       if (team.lane == 0) {
         replay_unit(M, tp, um, un, !isMerged, w.r);
