@@ -162,6 +162,30 @@ SSB_HD void trim_heave_reverse(const DevModel& M, double a_trim, double a_heave,
 
 // ----------------------------------------------------------------------------- reductions over lanes
 
+// Inclusive prefix sum of v over the lanes 0 .. lane of the warp (width 1: v itself).
+SSB_HD int lane_prefix(int v, int lane, int width) {
+#if defined(__CUDA_ARCH__)
+  if (width == 32)
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+#endif
+  (void)lane;
+  (void)width;
+  return v;
+}
+
+// The value of lane `src` (width 1: v itself).
+SSB_HD int lane_value(int v, int src, int width) {
+#if defined(__CUDA_ARCH__)
+  if (width == 32) return __shfl_sync(0xffffffffu, v, src);
+#endif
+  (void)src;
+  (void)width;
+  return v;
+}
+
 SSB_HD double lane_sum(double v, int width) {
 #if defined(__CUDA_ARCH__)
   if (width == 32)
@@ -914,6 +938,8 @@ struct RevSlot {
   double* red;                           // team reduction scratch: nwarps x 16
   UnitWork* work;                        // one per warp: the level solve's reverse, unit by unit
   std::uint8_t* plain;                   // per node: 1 when its unit's reverse was the empty node's pass-through
+  std::int32_t* units;                   // the other units in group order: group << 16 | member (0xffff: the merged group)
+  std::int32_t* nunits;                  // their number
 };
 
 // The adjoint of the state between steps: per node in memory, the scalars (zO, pitch, roll, vz, wth, wph) in every
@@ -1067,18 +1093,50 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
     }
   }
   team.sync();
-  // then the other units: a warp per merged group or node alone, lane 0 replaying it into the warp's work area
+  // then the other units, listed in group order by warp 0 (a prefix sum over the groups, a warp's width of them at a
+  // time) and dealt to the warps in turn: a warp per merged group or node alone, lane 0 replaying it into the warp's
+  // work area
+  if (team.warp == 0) {
+    int base = 0;
+    for (int g0 = 0; g0 < M.ng; g0 += team.width) {
+      const int g = g0 + team.lane;
+      int c = 0;
+      if (g < M.ng) {
+        if (merged[g]) {
+          c = 1;
+        } else {
+          const int* mem = M.gNodes + M.gStart[g];
+          for (int k = 0; k < M.gCount[g]; ++k) c += S.plain[mem[k]] ? 0 : 1;
+        }
+      }
+      const int incl = lane_prefix(c, team.lane, team.width);
+      int at = base + incl - c;
+      if (g < M.ng) {
+        if (merged[g]) {
+          S.units[at] = (g << 16) | 0xffff;
+        } else {
+          const int* mem = M.gNodes + M.gStart[g];
+          for (int k = 0; k < M.gCount[g]; ++k)
+            if (!S.plain[mem[k]]) S.units[at++] = (g << 16) | k;
+        }
+      }
+      base += lane_value(incl, team.width - 1, team.width);
+    }
+    if (team.lane == 0) *S.nunits = base;
+  }
+  team.sync();
   bool ok = true;
   UnitWork& w = S.work[team.warp];
-  for (int g = team.warp; g < M.ng; g += team.nwarps) {
-    const int N = M.gCount[g];
-    const int* mem = M.gNodes + M.gStart[g];
-    const bool isMerged = merged[g] != 0;
-    const int units = isMerged ? 1 : N;
-    for (int u = 0; u < units; ++u) {
+  const int nu = *S.nunits;
+  for (int i = team.warp; i < nu; i += team.nwarps) {
+    {
+      const int e = S.units[i];
+      const int g = e >> 16, u = e & 0xffff;
+      const int N = M.gCount[g];
+      const int* mem = M.gNodes + M.gStart[g];
+      const bool isMerged = u == 0xffff;
       const int* um = isMerged ? mem : mem + u;
       const int un = isMerged ? N : 1;
-      if (!isMerged && S.plain[um[0]]) continue;
       if (un > kMaxMembers) { ok = false; *err |= kErrGroupSize; continue; }
       if (team.lane == 0) {
         replay_unit(M, tp, um, un, !isMerged, w.r);
