@@ -43,7 +43,8 @@ struct AdjTeam {
     else asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(W * 32) : "memory");
   }
   __device__ __forceinline__ void add_int(int* p, int v) const { atomicAdd(p, v); }
-  // team-wide sums of K values (K <= 16), every thread receives them
+  // team-wide sums of K values (K <= 16), every thread receives them: each warp's sums in shared memory, then lane k
+  // of every warp adds value k over the warps (in warp order) and the lanes pass the K totals round by shuffles
   __device__ __forceinline__ void reduce(double* v, int K, double* red) const {
     for (int k = 0; k < K; ++k) {
       double x = v[k];
@@ -51,11 +52,10 @@ struct AdjTeam {
       if (lane == 0) red[warp * 16 + k] = x;
     }
     sync();
-    for (int k = 0; k < K; ++k) {
-      double s = 0;
-      for (int w = 0; w < nwarps; ++w) s += red[w * 16 + k];
-      v[k] = s;
-    }
+    double s = 0;
+    if (lane < K)
+      for (int w = 0; w < nwarps; ++w) s += red[w * 16 + lane];
+    for (int k = 0; k < K; ++k) v[k] = __shfl_sync(0xffffffffu, s, k);
     sync();
   }
 };
