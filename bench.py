@@ -209,8 +209,8 @@ def workload_rule(ship, args):
 
 
 def make_batch(ssb, ship_p, sim_p, sim, rule, count, first, args, device, total=None, **shape):
-    b = ssb.Batch(ship_p, sim_p, count=count, numerics=args.numerics, t_max=args.tmax, device=device, rule=rule,
-                  stage_columns=getattr(args, "stage_columns", False), **shape)
+    shape.setdefault("stage_columns", getattr(args, "stage_columns", False))
+    b = ssb.Batch(ship_p, sim_p, count=count, numerics=args.numerics, t_max=args.tmax, device=device, rule=rule, **shape)
     for i, (area, enabled) in enumerate(instance_params(sim, count, first, args, total)):
         for c, a in area.items():
             b.set_connection_area(i, c, a)
@@ -587,6 +587,7 @@ def main():
     ranks = Ranks(backend="nccl", timeout_s=600)
     world, rank, local = ranks.world, ranks.rank, ranks.local
     barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum
+    shape = {}
     if args.workload == "fleet":
         first, _ = shard_bounds(args.hulls * world, world, rank)
         hulls = fleet_models(args.hulls, first)
@@ -603,11 +604,10 @@ def main():
         rule = workload_rule(ship, args)
         first, _ = shard_bounds(args.count * world, world, rank)
         total = args.count * world
-        shape = {}
         if args.autotune:
-            from sinksim_b200.autotune import tune
+            from sinksim_b200.autotune import search
 
-            shape, _ = tune(lambda **s: make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local, total, **s))
+            shape, _ = search(lambda **s: make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local, total, **s))
         batch = make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local, total, **shape)
     # warm-up: full batches, untimed
     for _ in range(args.warmup):
@@ -667,6 +667,7 @@ def main():
                "dtype": "f64" if args.numerics == "portable" else "f32+f64", "data": "synthetic", "config": workload_config(args),
                "e2e": {"value": e2e, "unit": "sim-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                "gpu_launches": args.steps * info["kernels"], "launch": info, "sim_steps_per_launch": steps_per_launch,
+               "autotuned_shape": shape if args.autotune else None,
                "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
                             "frac": achieved / fp64_peak, "traffic": traffic, "ops_source": ops_source,
                             "kernel": f"run_batch<{args.numerics}, {top_warps}-warp teams> (launch phase {top})",
