@@ -599,7 +599,10 @@ __device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, S
   else L.mask = ((1u << LANES) - 1u) << (grp * LANES);
   const int unit = T.warp * PER_WARP + grp;
   PassR* P = S.passes + static_cast<std::size_t>(unit) * M.maxGroup;
-  for (int g = unit; g < M.ng; g += W * PER_WARP) {
+  // each lane group starts with the group of its own index, then takes the next one from the team's counter
+  // (S.misc[2], set to the number of lane groups at the start of the step): the groups take different numbers of
+  // passes, and a node's results do not depend on which lane group computes them
+  for (int g = unit; g < M.ng;) {
     const int N = __ldg(M.gCount + g);
     const int* m = M.gNodes + __ldg(M.gStart + g);
     const int mode = __ldg(M.gMode + g);
@@ -619,6 +622,9 @@ __device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, S
     S.merged[g] = merged ? 1 : 0;
     if (merged) solve_group<MIXED>(M, F, S, P, m, N, L, tape);
     else for (int k = 0; k < N; ++k) solve_single<MIXED>(M, F, S, __ldg(m + k), L, tape);
+    int next = 0;
+    if (L.sub == 0) next = atomicAdd(&S.misc[2], 1);
+    g = __shfl_sync(L.mask, next, grp * LANES);
   }
   __syncwarp();  // the lane groups leave the loop after different numbers of groups
 }
@@ -762,6 +768,8 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
   const int lane = T.lane, rank = T.rank;
   const double tNow = R.t;
   park(S.parked, R);  // until the volume update; no thread reads it before the barrier that ends that phase
+  // the level solve's group counter, read after the buoyancy's barrier (the last step's solve ended at a barrier)
+  if (T.leader()) S.misc[2] = W * (32 / kLevelLanes<MIXED>);
   *S.buoy = buoyancy<MIXED, W>(M, F, T, S.hydro, S.cols);  // every thread stores the same values
   solve_levels<MIXED, W>(M, F, S, T, tape);
   T.sync();
