@@ -689,8 +689,10 @@ struct FlowRec {
   double zo, ha, hb, Ha, Hb, d, u, H1, H2, r, p1, g, f, q, dV, dVpre, lim, inv, diff, hs, hd, share;
 };
 
+// The two powers of a submerged weir (r^1.5 and g^0.385) are kept per connection in pw (2 doubles each): the reverse
+// recomputes a step's flows twice, and with `reuse` the second time takes them from there instead of calling pow.
 SSB_HD FlowRec flow_forward(const DevModel& M, const PoseD& F, double t, const std::uint8_t* en, const double* area, const double* tOn,
-                            const double* hEff, const double* aEff, const int* deg, const std::int32_t* merged, int c) {
+                            const double* hEff, const double* aEff, const int* deg, const std::int32_t* merged, int c, double* pw, bool reuse) {
   FlowRec f{};
   f.active = false;
   if (!en[c] || tOn[c] > t) return f;
@@ -717,9 +719,10 @@ SSB_HD FlowRec flow_forward(const DevModel& M, const PoseD& F, double t, const s
       f.f = 1;
       if (f.H2 > 0) {
         f.r = f.H2 / f.H1;
-        f.p1 = pm::pow(f.r, kWeirExponent);
+        f.p1 = reuse ? pw[2 * c] : pm::pow(f.r, kWeirExponent);
         f.g = 1 - f.p1;
-        f.f = pm::pow(jmax(0.0, f.g), kVillemonteExponent);
+        f.f = reuse ? pw[2 * c + 1] : pm::pow(jmax(0.0, f.g), kVillemonteExponent);
+        if (!reuse) { pw[2 * c] = f.p1; pw[2 * c + 1] = f.f; }
       }
       q = M.coef[c] * area[c] * kWeirCoefficient * M.sq2g * f.H1 * pm::sqrt_rn(f.H1) * f.f * (f.Ha >= f.Hb ? 1.0 : -1.0);
     }
@@ -940,6 +943,7 @@ struct RevSlot {
   std::uint8_t* plain;                   // per node: 1 when its unit's reverse was the empty node's pass-through
   std::int32_t* units;                   // the other units in group order: group << 16 | member (0xffff: the merged group)
   std::int32_t* nunits;                  // their number
+  double* pw;                            // per connection: its weir's two powers (flow_forward)
 };
 
 // The adjoint of the state between steps: per node in memory, the scalars (zO, pitch, roll, vz, wth, wph) in every
@@ -986,7 +990,7 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
   }
   team.sync();
   for (int c = team.rank; c < NC; c += team.size)
-    S.dV[c] = flow_forward(M, F, t, en, area, tOn, S.hEff, S.aEff, S.deg, merged, c).dV;
+    S.dV[c] = flow_forward(M, F, t, en, area, tOn, S.hEff, S.aEff, S.deg, merged, c, S.pw, false).dV;
   team.sync();
   LoadSums Ls = loads_buoyancy(M, F, hb);
   double part[6] = {0, 0, 0, 0, 0, 0};
@@ -1054,7 +1058,7 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
     const int ca = M.ca[c], cb = M.cb[c];
     const double aDV = S.aAcc[cb] - (ca >= 0 ? S.aAcc[ca] : 0.0);
     FlowAdj fa;
-    const FlowRec fr = flow_forward(M, F, t, en, area, tOn, S.hEff, S.aEff, S.deg, merged, c);
+    const FlowRec fr = flow_forward(M, F, t, en, area, tOn, S.hEff, S.aEff, S.deg, merged, c, S.pw, true);
     grad[c] += flow_reverse(M, F, fr, S.aEff, area, c, aDV, fa, aP);
     S.faHA[c] = fa.hA; S.faHB[c] = fa.hB; S.faAA[c] = fa.aA; S.faAB[c] = fa.aB;
   }
