@@ -181,9 +181,10 @@ int ssa_gradient(const sso_ship* ship, const sso_sim* sim, const uint8_t* en, co
   std::vector<std::uint8_t> plain(nn);
   std::vector<std::int32_t> units(nn + 1), nunits(1);
   std::vector<double> pw(2 * static_cast<std::size_t>(nc));
+  std::vector<Replay> replays(static_cast<std::size_t>(nn));
   RevSlot S{hEff.data(), aEff.data(), dV.data(), volPost.data(), deg.data(), clip.data(), w[0].data(), w[1].data(), w[2].data(), w[3].data(),
             w[4].data(), w[5].data(), w[6].data(), w[7].data(), w[8].data(), fa[0].data(), fa[1].data(), fa[2].data(), fa[3].data(), red.data(),
-            &unitWork, plain.data(), units.data(), nunits.data(), pw.data()};
+            &unitWork, plain.data(), units.data(), nunits.data(), pw.data(), replays.data()};
   for (int c = 0; c < nc; ++c) grad[c] = 0;
   auto add_samples = [&](int64_t s) {
     for (int k = 0; k < nsamples; ++k) {

@@ -133,6 +133,7 @@ __device__ __forceinline__ AdjSmem carve_adjoint(unsigned char* base, const AdjL
   m.rs.units = reinterpret_cast<std::int32_t*>(base + A.units);
   m.rs.nunits = reinterpret_cast<std::int32_t*>(base + A.nunits);
   m.rs.pw = d(A.pw);
+  m.rs.replays = reinterpret_cast<adj::Replay*>(base + A.replays);
   m.as.aVol = d(A.aVol); m.as.aLevel = d(A.aLevel); m.as.aCx = d(A.aCx); m.as.aCy = d(A.aCy); m.as.aCz = d(A.aCz);
   m.grad = d(A.grad);
   m.sampleS = d(A.sampleS);
@@ -478,6 +479,7 @@ AdjLayout adjoint_layout(int nn, int nc, int ng, int nsamples, int W) {
   A.units = take16(sizeof(std::int32_t) * static_cast<std::size_t>(std::max(nn, 1)));
   A.nunits = take16(sizeof(std::int32_t));
   A.pw = take16(2 * C);
+  A.replays = take16(sizeof(adj::Replay) * static_cast<std::size_t>(std::max(nn, 1)));
   A.aVol = take16(N); A.aLevel = take16(N); A.aCx = take16(N); A.aCy = take16(N); A.aCz = take16(N);
   A.grad = take16(C);
   A.sampleS = take16(sizeof(double) * static_cast<std::size_t>(std::max(nsamples, 1)));

@@ -50,7 +50,7 @@ struct AdjRun {
 
 // Byte offsets of a team's reverse arrays in shared memory, after its forward slot.
 struct AdjLayout {
-  std::uint32_t hEff, aEff, dV, volPost, deg, clip, aVolPost, aCxs, aCys, aCzs, aVs, aAcc, aZmx, aLs, aAs, faHA, faHB, faAA, faAB, red, work, plain, units, nunits, pw;
+  std::uint32_t hEff, aEff, dV, volPost, deg, clip, aVolPost, aCxs, aCys, aCzs, aVs, aAcc, aZmx, aLs, aAs, faHA, faHB, faAA, faAB, red, work, plain, units, nunits, pw, replays;
   std::uint32_t aVol, aLevel, aCx, aCy, aCz, grad, sampleS, tape, poff, bytes;
 };
 

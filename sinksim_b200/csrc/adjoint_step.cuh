@@ -371,6 +371,8 @@ struct Replay {
   bool ok;
 };
 
+static_assert(sizeof(Replay) % sizeof(std::int32_t) == 0, "a replay is copied in 32-bit words");
+
 SSB_HD const double* rec(const Tape& t, int n, int k) { return t.pass(n, k); }
 
 // Replays the solver's decisions (levels.hpp:13-49 for a node alone, :54-162 for a merged group) on the recorded passes,
@@ -944,6 +946,7 @@ struct RevSlot {
   std::int32_t* units;                   // the other units in group order: group << 16 | member (0xffff: the merged group)
   std::int32_t* nunits;                  // their number
   double* pw;                            // per connection: its weir's two powers (flow_forward)
+  Replay* replays;                       // per listed unit: its replay
 };
 
 // The adjoint of the state between steps: per node in memory, the scalars (zO, pitch, roll, vz, wth, wph) in every
@@ -1129,9 +1132,24 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
     if (team.lane == 0) *S.nunits = base;
   }
   team.sync();
+  const int nu = *S.nunits;
+  // every unit's replay at once, a thread per unit (the replay is a chain of scalar decisions over the recorded passes)
+  for (int i = team.rank; i < nu; i += team.size) {
+    const int e = S.units[i];
+    const int g = e >> 16, u = e & 0xffff;
+    const bool isMerged = u == 0xffff;
+    const int* um = M.gNodes + M.gStart[g] + (isMerged ? 0 : u);
+    const int un = isMerged ? M.gCount[g] : 1;
+    Replay& r = S.replays[i];
+    replay_unit(M, tp, um, un, !isMerged, r);
+    for (int k = 0; k < un && k < kMaxMembers; ++k) {
+      const int want = r.cs == 0 ? 1 : (r.cs == 1 ? 2 : r.K + 1);
+      r.ok = r.ok && tp.i[L.npass + um[k]] == want;
+    }
+  }
+  team.sync();
   bool ok = true;
   UnitWork& w = S.work[team.warp];
-  const int nu = *S.nunits;
   for (int i = team.warp; i < nu; i += team.nwarps) {
     {
       const int e = S.units[i];
@@ -1142,12 +1160,13 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
       const int* um = isMerged ? mem : mem + u;
       const int un = isMerged ? N : 1;
       if (un > kMaxMembers) { ok = false; *err |= kErrGroupSize; continue; }
+      // the unit's replay into the warp's work area, a word per lane
+      {
+        const auto* src = reinterpret_cast<const std::int32_t*>(&S.replays[i]);
+        auto* dst = reinterpret_cast<std::int32_t*>(&w.r);
+        for (int k = team.lane; k < static_cast<int>(sizeof(Replay) / sizeof(std::int32_t)); k += team.width) dst[k] = src[k];
+      }
       if (team.lane == 0) {
-        replay_unit(M, tp, um, un, !isMerged, w.r);
-        for (int k = 0; k < un; ++k) {
-          const int want = w.r.cs == 0 ? 1 : (w.r.cs == 1 ? 2 : w.r.K + 1);
-          w.r.ok = w.r.ok && tp.i[L.npass + um[k]] == want;
-        }
         for (int k = 0; k < un; ++k) {
           const int n = um[k];
           w.u.aLevel[k] = S.aLs[n]; w.u.aArea[k] = S.aAs[n]; w.u.aCx[k] = S.aCxs[n]; w.u.aCy[k] = S.aCys[n]; w.u.aCz[k] = S.aCzs[n];
@@ -1176,9 +1195,9 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
       warp_sync();  // every lane is done with the work area before lane 0 fills it for the next unit
     }
   }
-  team.sync();
 
-  // ---- buoyancy (reduce.hpp:39-49): the adjoint of V, x, y, z into V, Mx, My, Mz, then the columns
+  // ---- buoyancy (reduce.hpp:39-49): the adjoint of V, x, y, z into V, Mx, My, Mz, then the columns. It needs only the
+  // loads' adjoint, so each warp sweeps its columns as soon as its level-solve units are done, before the barrier
   {
     double aV = aHb[0], aMx = 0, aMy = 0, aMz = 0;
     if (hb[0] > 0) {
@@ -1187,6 +1206,7 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
     }
     buoyancy_sweep(M, F, aV, aMx, aMy, aMz, team.rank, team.size, aP);
   }
+  team.sync();
 
   // ---- the pose: every thread's share summed over the team, then (zO, pitch, roll)
   double red[kAdjPoseFields + 1];
