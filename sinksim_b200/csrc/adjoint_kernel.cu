@@ -169,16 +169,17 @@ __device__ __forceinline__ void load_state(const double* c, SimRegs& R, Slot& S,
   T.sync();
 }
 
-// A packed step record: the tape's int32 (pass counts, merged flags; padded to 8 bytes), its doubles up to the pass
-// records, then only the pass records the step used, node by node (min(count, kMaxPasses) per node), the whole
-// rounded up to 16 bytes. The pass records dominate the unpacked tape (kMaxPasses slots per node), and a node takes
-// about 1.2 passes per step, so a record is about a third of the tape.
-__host__ __device__ __forceinline__ std::size_t record_ints_bytes(const adj::TapeLayout& L) {
-  return (L.ints * sizeof(std::int32_t) + 7) & ~static_cast<std::size_t>(7);
+// A packed step record: the tape's int32 (pass counts, merged flags), each node's first pass record in the packed
+// order and their total (nn + 1 int32; padded to 8 bytes), the tape's doubles up to the pass records, then only the
+// pass records the step used, node by node (min(count, kMaxPasses) per node), the whole rounded up to 16 bytes. The
+// pass records dominate the unpacked tape (kMaxPasses slots per node), and a node takes about 1.2 passes per step, so a
+// record is about a third of the tape; the stored offsets let its reader place every pass without a scan.
+__host__ __device__ __forceinline__ std::size_t record_ints_bytes(const adj::TapeLayout& L, int nn) {
+  return ((L.ints + static_cast<std::size_t>(nn) + 1) * sizeof(std::int32_t) + 7) & ~static_cast<std::size_t>(7);
 }
 
-__host__ __device__ __forceinline__ std::size_t record_bytes(const adj::TapeLayout& L, int records) {
-  return (record_ints_bytes(L) + (L.passes + static_cast<std::size_t>(records) * adj::kPassFields) * sizeof(double) + 15) &
+__host__ __device__ __forceinline__ std::size_t record_bytes(const adj::TapeLayout& L, int nn, int records) {
+  return (record_ints_bytes(L, nn) + (L.passes + static_cast<std::size_t>(records) * adj::kPassFields) * sizeof(double) + 15) &
          ~static_cast<std::size_t>(15);
 }
 
@@ -211,33 +212,34 @@ __device__ __forceinline__ std::size_t store_record(const adj::Tape& tp, int nn,
   pass_offsets(tp.i + L.npass, nn, poff, T);
   std::int32_t* di = reinterpret_cast<std::int32_t*>(dst);
   for (std::size_t i = T.rank; i < L.ints; i += 32 * W) di[i] = tp.i[i];
-  double* dd = reinterpret_cast<double*>(dst + record_ints_bytes(L));
+  for (int n = T.rank; n <= nn; n += 32 * W) di[L.ints + n] = poff[n];
+  double* dd = reinterpret_cast<double*>(dst + record_ints_bytes(L, nn));
   for (std::size_t i = T.rank; i < L.passes; i += 32 * W) dd[i] = tp.d[i];
   constexpr int kPerNode = adj::kMaxPasses * adj::kPassFields;
   for (int i = T.rank; i < nn * kPerNode; i += 32 * W) {
     const int n = i / kPerNode, k = (i / adj::kPassFields) % adj::kMaxPasses, f = i % adj::kPassFields;
     if (k < tp.i[L.npass + n]) dd[L.passes + static_cast<std::size_t>(poff[n] + k) * adj::kPassFields + f] = tp.d[L.passes + i];
   }
-  const std::size_t bytes = record_bytes(L, poff[nn]);
+  const std::size_t bytes = record_bytes(L, nn, poff[nn]);
   T.sync();
   return bytes;
 }
 
-// Unpacks a record (global) into the step's tape in shared memory: the pass records go to their slots; slots the
-// step did not use are left as they are (the replay reads only the used ones).
+// Unpacks a record (global) into the step's tape in shared memory, in one round of loads and one barrier: the pass
+// records go to their slots by the record's own offsets; slots the step did not use are left as they are (the replay
+// reads only the used ones).
 template <int W>
-__device__ __forceinline__ void load_record(const unsigned char* src, const adj::Tape& tp, int nn, std::int32_t* poff, const Team<W>& T) {
+__device__ __forceinline__ void load_record(const unsigned char* src, const adj::Tape& tp, int nn, const Team<W>& T) {
   const adj::TapeLayout& L = tp.L;
   const std::int32_t* si = reinterpret_cast<const std::int32_t*>(src);
+  const std::int32_t* soff = si + L.ints;
   for (std::size_t i = T.rank; i < L.ints; i += 32 * W) tp.i[i] = si[i];
-  const double* sd = reinterpret_cast<const double*>(src + record_ints_bytes(L));
+  const double* sd = reinterpret_cast<const double*>(src + record_ints_bytes(L, nn));
   for (std::size_t i = T.rank; i < L.passes; i += 32 * W) tp.d[i] = sd[i];
-  T.sync();
-  pass_offsets(tp.i + L.npass, nn, poff, T);
   constexpr int kPerNode = adj::kMaxPasses * adj::kPassFields;
   for (int i = T.rank; i < nn * kPerNode; i += 32 * W) {
     const int n = i / kPerNode, k = (i / adj::kPassFields) % adj::kMaxPasses, f = i % adj::kPassFields;
-    if (k < tp.i[L.npass + n]) tp.d[L.passes + i] = sd[L.passes + static_cast<std::size_t>(poff[n] + k) * adj::kPassFields + f];
+    if (k < si[L.npass + n]) tp.d[L.passes + i] = sd[L.passes + static_cast<std::size_t>(soff[n] + k) * adj::kPassFields + f];
   }
   T.sync();
 }
@@ -294,7 +296,7 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
   Slot S = carve_slot(smem, SL);
   AdjSmem A = carve_adjoint(smem + SL.bytes, AL);
   const adj::TapeLayout TL = adj::tape_layout(M.nn, M.ng);
-  const std::size_t recMax = record_bytes(TL, M.nn * adj::kMaxPasses);
+  const std::size_t recMax = record_bytes(TL, M.nn, M.nn * adj::kMaxPasses);
   const std::size_t recSize = 7 + 5 * static_cast<std::size_t>(M.nn);
   double* const ckpt = B.ckpt + static_cast<std::size_t>(team) * B.maxCkpt * recSize;
   unsigned char* const ring = B.arena + static_cast<std::size_t>(team) * B.arenaBytes;
@@ -430,7 +432,7 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
           const auto* next = ring + o0 % static_cast<long long>(B.arenaBytes);
           asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(next), "r"(static_cast<unsigned>(o1 - o0)) : "memory");
         }
-        load_record(ring + off[st] % static_cast<long long>(B.arenaBytes), sp, M.nn, A.poff, T);
+        load_record(ring + off[st] % static_cast<long long>(B.arenaBytes), sp, M.nn, T);
         adj::reverse_step(AT, M, sp, I.en(), I.area(), I.tOn(), A.rs, A.as, aSc, A.grad, &err);
         for (int q = 0; q < NS; ++q)
           if (static_cast<long long>(A.sampleS[q]) == st) {
@@ -489,8 +491,8 @@ AdjLayout adjoint_layout(int nn, int nc, int ng, int nsamples, int W) {
   return A;
 }
 
-std::size_t adjoint_tape_bytes(int nn, int ng) { return record_bytes(adj::tape_layout(nn, ng), nn * adj::kMaxPasses); }
-std::size_t adjoint_record_bytes(int nn, int ng, int passRecords) { return record_bytes(adj::tape_layout(nn, ng), passRecords); }
+std::size_t adjoint_tape_bytes(int nn, int ng) { return record_bytes(adj::tape_layout(nn, ng), nn, nn * adj::kMaxPasses); }
+std::size_t adjoint_record_bytes(int nn, int ng, int passRecords) { return record_bytes(adj::tape_layout(nn, ng), nn, passRecords); }
 
 cudaError_t configure_adjoint_kernel(int W, std::size_t smem) {
   const int b = static_cast<int>(smem);
