@@ -309,6 +309,7 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
     if (T.leader()) {
       const int q = atomicAdd(B.queue, 1);
       S.misc[0] = B.order == nullptr || q >= B.count ? q : B.order[q];
+      S.misc[2] = W * (32 / kLevelLanes<false>);  // the level solve's group counter for the first step (team_step resets it)
     }
     T.sync();
     const int inst = S.misc[0];

@@ -263,6 +263,7 @@ __global__ void __launch_bounds__(kMaxWarpsPerBlock * 32, kMinBlocksPerSM) run_b
     if (T.leader()) {
       const int q = atomicAdd(B.queue, 1);
       S.misc[0] = B.order == nullptr ? q : (q < *B.orderCount ? B.order[q] : B.count);
+      S.misc[2] = W * (32 / kLevelLanes<MIXED>);  // the level solve's group counter for the first step (team_step resets it)
     }
     T.sync();
     const int inst = S.misc[0];

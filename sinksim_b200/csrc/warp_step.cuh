@@ -191,7 +191,7 @@ __host__ __device__ __forceinline__ StagedColumns<T> staged_columns(int ncol) {
 // The eight trees are spread over the team's warps (warp v computes trees v, v + W, ...); the tree results meet in
 // shared memory and every thread adds them in the reference's order (trees 0..7).
 template <bool MIXED, int W>
-__device__ __forceinline__ Buoy buoyancy(const DevModel& M, const Pose& F, const Team<W>& T, double* trees, const unsigned char* cols) {
+__device__ __forceinline__ void buoyancy_trees(const DevModel& M, const Pose& F, const Team<W>& T, double* trees, const unsigned char* cols) {
   const int lane = T.lane;
   for (int w = T.warp; w < 8; w += W) {
     double g[5];
@@ -231,7 +231,11 @@ __device__ __forceinline__ Buoy buoyancy(const DevModel& M, const Pose& F, const
       for (int k = 0; k < 5; ++k) t[k] = g[k];
     }
   }
-  T.sync();
+}
+
+// The buoyancy result from the eight trees (after a team barrier that follows buoyancy_trees): every thread adds
+// them in the reference's order and holds the same values.
+__device__ __forceinline__ Buoy buoyancy_finish(const double* trees) {
   double V = trees[0], Mx = trees[1], My = trees[2], Mz = trees[3], top = trees[4];
   for (int w = 1; w < 8; ++w) {
     const double* t = trees + 5 * w;
@@ -245,6 +249,13 @@ __device__ __forceinline__ Buoy buoyancy(const DevModel& M, const Pose& F, const
   b.z = V > 0 ? Mz / V : 0;
   b.top = top;
   return b;
+}
+
+template <bool MIXED, int W>
+__device__ __forceinline__ Buoy buoyancy(const DevModel& M, const Pose& F, const Team<W>& T, double* trees, const unsigned char* cols) {
+  buoyancy_trees<MIXED, W>(M, F, T, trees, cols);
+  T.sync();
+  return buoyancy_finish(trees);
 }
 
 // ----------------------------------------------------------------------------- node pass (tree order)
@@ -768,11 +779,14 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
   const int lane = T.lane, rank = T.rank;
   const double tNow = R.t;
   park(S.parked, R);  // until the volume update; no thread reads it before the barrier that ends that phase
-  // the level solve's group counter, read after the buoyancy's barrier (the last step's solve ended at a barrier)
-  if (T.leader()) S.misc[2] = W * (32 / kLevelLanes<MIXED>);
-  *S.buoy = buoyancy<MIXED, W>(M, F, T, S.hydro, S.cols);  // every thread stores the same values
+  // The buoyancy's eight trees and the level solve need nothing from each other: warps without a tree (teams of more
+  // than 8 warps) or done with theirs go on to take node groups, and one barrier ends both
+  buoyancy_trees<MIXED, W>(M, F, T, S.hydro, S.cols);
   solve_levels<MIXED, W>(M, F, S, T, tape);
   T.sync();
+  // the group counter for the next step's level solve (read after this step's later barriers)
+  if (T.leader()) S.misc[2] = W * (32 / kLevelLanes<MIXED>);
+  *S.buoy = buoyancy_finish(S.hydro);  // every thread stores the same values
   tape.solved(M, S, T);
 
   // effective heads and areas, then degrees (flows.hpp:15-35)
