@@ -101,9 +101,9 @@ AdjointBatch::AdjointBatch(std::shared_ptr<const CompiledShip> ship, const Compi
     std::copy(M.cz0.begin(), M.cz0.end(), I.hCz.begin() + i * nn);
   }
   // team size: a whole 16-warp block per instance while the instances number at most two per SM, 8 warps beyond
-  // (the liner's gradient workload on B200: 256 points 2.98 s per call in 16-warp teams against 3.31 s in 8-warp
-  // teams; 512 points 4.68 s in 8-warp teams against 5.88 s in 16-warp and 6.18 s in 4-warp teams; the evaluator's
-  // claim order, longest runs first, in every case)
+  // (the liner's gradient workload on B200: 256 points 2.24 s per call in 16-warp teams against 2.40 s in 8-warp
+  // teams; 512 points 4.68 s in 8-warp teams against 5.88 s in 16-warp and 6.18 s in 4-warp teams, measured before
+  // the reverse's rework; the evaluator's claim order, longest runs first, in every case)
   teamWarps_ = opt_.teamWarps ? opt_.teamWarps : (opt_.count <= 2 * I.info.multiprocessors ? 16 : 8);
 }
 

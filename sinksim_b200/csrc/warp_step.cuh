@@ -779,14 +779,22 @@ __device__ __forceinline__ void team_step(const DevModel& M, const Pose& F, SimR
   const int lane = T.lane, rank = T.rank;
   const double tNow = R.t;
   park(S.parked, R);  // until the volume update; no thread reads it before the barrier that ends that phase
-  // The buoyancy's eight trees and the level solve need nothing from each other: warps without a tree (teams of more
-  // than 8 warps) or done with theirs go on to take node groups, and one barrier ends both
-  buoyancy_trees<MIXED, W>(M, F, T, S.hydro, S.cols);
-  solve_levels<MIXED, W>(M, F, S, T, tape);
-  T.sync();
+  if constexpr (W > 8) {
+    // The buoyancy's eight trees and the level solve need nothing from each other: the warps without a tree go on to
+    // take node groups, and one barrier ends both (16-warp teams: the tail phase 517 against 534 ms on the bench
+    // batch, the adjoint's forward 125 against 132 team-s per call; in teams of at most 8 warps, where every warp has
+    // trees, the same order made the main phase slower, 2.75 against 2.60 s)
+    buoyancy_trees<MIXED, W>(M, F, T, S.hydro, S.cols);
+    solve_levels<MIXED, W>(M, F, S, T, tape);
+    T.sync();
+    *S.buoy = buoyancy_finish(S.hydro);  // every thread stores the same values
+  } else {
+    *S.buoy = buoyancy<MIXED, W>(M, F, T, S.hydro, S.cols);  // every thread stores the same values
+    solve_levels<MIXED, W>(M, F, S, T, tape);
+    T.sync();
+  }
   // the group counter for the next step's level solve (read after this step's later barriers)
   if (T.leader()) S.misc[2] = W * (32 / kLevelLanes<MIXED>);
-  *S.buoy = buoyancy_finish(S.hydro);  // every thread stores the same values
   tape.solved(M, S, T);
 
   // effective heads and areas, then degrees (flows.hpp:15-35)
