@@ -43,7 +43,6 @@ struct DevModel {
   std::int32_t ng;
   const std::int32_t *gStart, *gCount, *gNodes;
   const std::uint8_t* gMode;
-  const std::int32_t* gOrder;     // the groups by decreasing segment count of their members (the level solve's order)
   const double *gpx, *gpy, *gpz;
   double gMargin;
   std::int32_t maxGroup;

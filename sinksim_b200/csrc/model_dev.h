@@ -3,7 +3,6 @@
 // and the adjoint engine (adjoint.cpp).
 #pragma once
 
-#include <algorithm>
 #include <cmath>
 #include <memory>
 #include <stdexcept>
@@ -78,7 +77,6 @@ struct ModelDev {
   DevBuf<float2> colXYf, colLHf, segXYf, segLHf;
   DevBuf<float> colAf, segArf;
   DevBuf<double> colA, segAr, mu, vmax, amin, aov;
-  DevBuf<std::int32_t> gOrder;
   DevBuf<std::int32_t> segStart, segCount, gStart, gCount, gNodes, ca, cb, skip, incStart, incCount, incConn, sea, monStart, monCount, monConn;
   DevBuf<std::uint8_t> gMode, law, incSide, mkWhen;
   DevBuf<double> gpx, gpy, gpz, kx, ky, kz, coef, mkx, mky, mkz;
@@ -128,17 +126,6 @@ struct ModelDev {
     segStart.upload(S.segStart, s); segCount.upload(S.segCount, s);
     gStart.upload(M.gNodeStart, s); gCount.upload(M.gNodeCount, s); gNodes.upload(M.gNodes, s); gMode.upload(M.gMode, s);
     gpx.upload(M.gpx, s); gpy.upload(M.gpy, s); gpz.upload(M.gpz, s);
-    {
-      // the order in which the level solve's lane groups take the groups: most segments first (a group's node passes
-      // take about that long), index order among equals, so that the smallest groups fill in at the end
-      std::vector<std::int64_t> work(static_cast<std::size_t>(NG), 0);
-      for (std::int32_t g = 0; g < NG; ++g)
-        for (std::int32_t k = 0; k < M.gNodeCount[g]; ++k) work[g] += S.segCount[M.gNodes[M.gNodeStart[g] + k]];
-      std::vector<std::int32_t> order(static_cast<std::size_t>(std::max(NG, 1)), 0);
-      for (std::int32_t g = 0; g < NG; ++g) order[g] = g;
-      std::stable_sort(order.begin(), order.begin() + NG, [&](std::int32_t a, std::int32_t b) { return work[a] > work[b]; });
-      gOrder.upload(order, s);
-    }
     ca.upload(M.ca, s); cb.upload(M.cb, s); skip.upload(M.cSkipGroup, s); law.upload(M.cLaw, s);
     kx.upload(M.cx, s); ky.upload(M.cy, s); kz.upload(M.cz, s); coef.upload(M.cCoef, s);
     incStart.upload(inc.start, s); incCount.upload(inc.count, s); incConn.upload(inc.conn, s); incSide.upload(inc.side, s);
@@ -163,7 +150,7 @@ struct ModelDev {
     d.mu = mu.get(); d.vmax = vmax.get(); d.amin = amin.get(); d.aov = aov.get();
     d.segStart = segStart.get(); d.segCount = segCount.get();
     d.ng = NG;
-    d.gStart = gStart.get(); d.gCount = gCount.get(); d.gNodes = gNodes.get(); d.gMode = gMode.get(); d.gOrder = gOrder.get();
+    d.gStart = gStart.get(); d.gCount = gCount.get(); d.gNodes = gNodes.get(); d.gMode = gMode.get();
     d.gpx = gpx.get(); d.gpy = gpy.get(); d.gpz = gpz.get(); d.gMargin = M.gMargin; d.maxGroup = maxGroup;
     d.nc = NC;
     d.ca = ca.get(); d.cb = cb.get(); d.skip = skip.get(); d.law = law.get();

@@ -610,11 +610,10 @@ __device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, S
   else L.mask = ((1u << LANES) - 1u) << (grp * LANES);
   const int unit = T.warp * PER_WARP + grp;
   PassR* P = S.passes + static_cast<std::size_t>(unit) * M.maxGroup;
-  // each lane group starts with the group at its own index in the model's order (most segments first), then takes the
-  // next one from the team's counter (S.misc[2], the number of lane groups at the start of the step): the groups take
-  // different numbers of passes, and a node's results do not depend on which lane group computes them
-  for (int idx = unit; idx < M.ng;) {
-    const int g = __ldg(M.gOrder + idx);
+  // each lane group starts with the group of its own index, then takes the next one from the team's counter
+  // (S.misc[2], set to the number of lane groups at the start of the step): the groups take different numbers of
+  // passes, and a node's results do not depend on which lane group computes them
+  for (int g = unit; g < M.ng;) {
     const int N = __ldg(M.gCount + g);
     const int* m = M.gNodes + __ldg(M.gStart + g);
     const int mode = __ldg(M.gMode + g);
@@ -636,7 +635,7 @@ __device__ __forceinline__ void solve_levels(const DevModel& M, const Pose& F, S
     else for (int k = 0; k < N; ++k) solve_single<MIXED>(M, F, S, __ldg(m + k), L, tape);
     int next = 0;
     if (L.sub == 0) next = atomicAdd(&S.misc[2], 1);
-    idx = __shfl_sync(L.mask, next, grp * LANES);
+    g = __shfl_sync(L.mask, next, grp * LANES);
   }
   __syncwarp();  // the lane groups leave the loop after different numbers of groups
 }
