@@ -1081,28 +1081,12 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
   }
   team.sync();
 
-  // ---- the level solve. First, thread-parallel, the units that are a node alone and empty (most of them in a
-  // flooding run), when neither its level nor its extent top has an adjoint and its one pass is the recorded start:
-  // the solver set the level to the node's extent bottom and left volume and centroid as they were, so their adjoints
-  // pass through (what unit_reverse does for such a unit, without its replay)
-  for (int g = team.rank; g < M.ng; g += team.size) {
-    const int N = M.gCount[g];
-    const int* mem = M.gNodes + M.gStart[g];
-    const bool isMerged = merged[g] != 0;
-    for (int k = 0; k < N; ++k) {
-      const int n = mem[k];
-      S.plain[n] = !isMerged && tp.d[L.volIn + n] <= kEmptyVolume && tp.i[L.npass + n] == 1 && tp.pass(n, 0)[0] == tp.d[L.levelIn + n] &&
-                   S.aLs[n] == 0 && S.aZmx[n] == 0;
-      if (!S.plain[n]) continue;
-      a.aVol[n] = 0.0 + (0.0 + S.aVs[n]);
-      a.aLevel[n] = 0.0 + 0.0;
-      a.aCx[n] = 0.0 + S.aCxs[n]; a.aCy[n] = 0.0 + S.aCys[n]; a.aCz[n] = 0.0 + S.aCzs[n];
-    }
-  }
-  team.sync();
-  // then the other units, listed in group order by warp 0 (a prefix sum over the groups, a warp's width of them at a
-  // time) and dealt to the warps in turn: a warp per merged group or node alone, lane 0 replaying it into the warp's
-  // work area
+  // ---- the level solve. Warp 0 lists the units in group order (a prefix sum over the groups, a warp's width of them
+  // at a time), except the units that are a node alone and empty (most of them in a flooding run) when neither its
+  // level nor its extent top has an adjoint and its one pass is the recorded start: the solver set the level to the
+  // node's extent bottom and left volume and centroid as they were, so their adjoints pass through (what unit_reverse
+  // does for such a unit, without its replay), written by the listing lane. The listed units are then dealt to the
+  // warps in turn: a warp per merged group or node alone, lane 0 doing its scalar chain in the warp's work area.
   if (team.warp == 0) {
     int base = 0;
     for (int g0 = 0; g0 < M.ng; g0 += team.width) {
@@ -1113,7 +1097,18 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
           c = 1;
         } else {
           const int* mem = M.gNodes + M.gStart[g];
-          for (int k = 0; k < M.gCount[g]; ++k) c += S.plain[mem[k]] ? 0 : 1;
+          for (int k = 0; k < M.gCount[g]; ++k) {
+            const int n = mem[k];
+            S.plain[n] = tp.d[L.volIn + n] <= kEmptyVolume && tp.i[L.npass + n] == 1 && tp.pass(n, 0)[0] == tp.d[L.levelIn + n] &&
+                         S.aLs[n] == 0 && S.aZmx[n] == 0;
+            if (!S.plain[n]) {
+              ++c;
+              continue;
+            }
+            a.aVol[n] = 0.0 + (0.0 + S.aVs[n]);
+            a.aLevel[n] = 0.0 + 0.0;
+            a.aCx[n] = 0.0 + S.aCxs[n]; a.aCy[n] = 0.0 + S.aCys[n]; a.aCz[n] = 0.0 + S.aCzs[n];
+          }
         }
       }
       const int incl = lane_prefix(c, team.lane, team.width);
@@ -1217,7 +1212,7 @@ SSB_HDT bool reverse_step(const T& team, const DevModel& M, const Tape& tp, cons
   for (int k = 0; k < kAdjPoseFields; ++k) fields(tot)[k] = red[k];
   aSc[0] += red[kAdjPoseFields];
   pose_reverse(M, F, tot, aSc[0], aSc[1], aSc[2]);
-  team.sync();
+  // (no barrier here: the caller synchronises the team before the tape or these work arrays are written again)
   return ok;
 }
 
