@@ -591,8 +591,17 @@ def main():
     if args.workload == "fleet":
         first, _ = shard_bounds(args.hulls * world, world, rank)
         hulls = fleet_models(args.hulls, first)
-        batch = ssb.Batch.fleet(hulls, list(range(len(hulls))), numerics=args.numerics, t_max=args.fleet_tmax, device=local,
-                                stop_when_stable=True)
+
+        def make_fleet(**s):
+            return ssb.Batch.fleet(hulls, list(range(len(hulls))), numerics=args.numerics, t_max=args.fleet_tmax, device=local,
+                                   stop_when_stable=True, **s)
+
+        if args.autotune:
+            from sinksim_b200.autotune import DEFAULT_SPACE, search
+
+            # a fleet's slot is set by its largest hull and the column table is per model: no staged table
+            shape, _ = search(make_fleet, space=tuple(d for d in DEFAULT_SPACE if d[0] != "stage_columns"))
+        batch = make_fleet(**shape)
         hull_ops = []
         for ship_p, sim_p in hulls:
             s_doc, m_doc = load_model(ship_p, sim_p)
