@@ -208,6 +208,10 @@ def workload_rule(ship, args):
     return None if args.workload == "perturbed" else deck_edge_rule(ship)
 
 
+def _tune_log(shape, ms, steps):
+    print(f"autotune: {shape} {ms:.1f} ms ({steps} sim-steps)", file=sys.stderr)
+
+
 def make_batch(ssb, ship_p, sim_p, sim, rule, count, first, args, device, total=None, **shape):
     shape.setdefault("stage_columns", getattr(args, "stage_columns", False))
     b = ssb.Batch(ship_p, sim_p, count=count, numerics=args.numerics, t_max=args.tmax, device=device, rule=rule, **shape)
@@ -587,7 +591,7 @@ def main():
     ranks = Ranks(backend="nccl", timeout_s=600)
     world, rank, local = ranks.world, ranks.rank, ranks.local
     barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum
-    shape = {}
+    shape, tune_table = {}, []
     if args.workload == "fleet":
         first, _ = shard_bounds(args.hulls * world, world, rank)
         hulls = fleet_models(args.hulls, first)
@@ -600,7 +604,7 @@ def main():
             from sinksim_b200.autotune import DEFAULT_SPACE, search
 
             # a fleet's slot is set by its largest hull and the column table is per model: no staged table
-            shape, _ = search(make_fleet, space=tuple(d for d in DEFAULT_SPACE if d[0] != "stage_columns"))
+            shape, tune_table = search(make_fleet, space=tuple(d for d in DEFAULT_SPACE if d[0] != "stage_columns"), log=_tune_log)
         batch = make_fleet(**shape)
         hull_ops = []
         for ship_p, sim_p in hulls:
@@ -616,7 +620,8 @@ def main():
         if args.autotune:
             from sinksim_b200.autotune import search
 
-            shape, _ = search(lambda **s: make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local, total, **s))
+            shape, tune_table = search(lambda **s: make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local, total, **s),
+                                       log=_tune_log)
         batch = make_batch(ssb, ship_p, sim_p, sim, rule, args.count, first, args, local, total, **shape)
     # warm-up: full batches, untimed
     for _ in range(args.warmup):
@@ -677,6 +682,7 @@ def main():
                "e2e": {"value": e2e, "unit": "sim-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                "gpu_launches": args.steps * info["kernels"], "launch": info, "sim_steps_per_launch": steps_per_launch,
                "autotuned_shape": shape if args.autotune else None,
+               "autotune_table": [[t[0], t[1]] for t in tune_table] if args.autotune else None,
                "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
                             "frac": achieved / fp64_peak, "traffic": traffic, "ops_source": ops_source,
                             "kernel": f"run_batch<{args.numerics}, {top_warps}-warp teams> (launch phase {top})",
