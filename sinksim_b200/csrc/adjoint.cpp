@@ -27,6 +27,7 @@ struct AdjointBatch::Impl {
   DevBuf<double> area, tOn, st, vol, level, cx, cy, cz, times, trimT, heaveT, trim, heave, J, grad, ckpt, sink;
   DevBuf<unsigned char> arena;
   DevBuf<long long> steps, phase, stepOff, recomputed;
+  DevBuf<std::int32_t> recBytes;
   DevBuf<std::int32_t> error, queue, isink, order;
   std::vector<std::int32_t> hOrder;  // the caller's claim order (empty: by index)
   // results
@@ -159,8 +160,8 @@ float AdjointBatch::run() {
   const ModelDev& m = *I.model;
   const int W = teamWarps_;
   const SlotLayout SL = I.slot_for(W);
-  const AdjLayout AL = adjoint_layout(m.NN, m.NC, m.NG, I.nsamples, W);
-  const std::size_t smem = static_cast<std::size_t>(SL.bytes) + AL.bytes;
+  AdjLayout AL = adjoint_layout(m.NN, m.NC, m.NG, I.nsamples, W);
+  std::size_t smem = static_cast<std::size_t>(SL.bytes) + AL.bytes;
   if (smem > I.info.sharedPerBlockOptIn)
     throw std::runtime_error("AdjointBatch: a team needs " + std::to_string(smem) + " bytes of shared memory, the device allows " +
                              std::to_string(I.info.sharedPerBlockOptIn));
@@ -168,6 +169,24 @@ float AdjointBatch::run() {
   int perSM = 0;
   check(adjoint_occupancy(W, smem, &perSM), "occupancy");
   if (perSM < 1) throw std::runtime_error("AdjointBatch: the adjoint kernel cannot be resident");
+  // a buffer for the next step's record (copied while the current step is reversed) when it costs no team per SM
+  bool stageRecords = false;
+  {
+    const AdjLayout AR = adjoint_layout(m.NN, m.NC, m.NG, I.nsamples, W, true);
+    const std::size_t smemR = static_cast<std::size_t>(SL.bytes) + AR.bytes;
+    int perSMR = 0;
+    if (smemR <= I.info.sharedPerBlockOptIn) {
+      check(configure_adjoint_kernel(W, smemR), "cudaFuncSetAttribute");
+      check(adjoint_occupancy(W, smemR, &perSMR), "occupancy");
+    }
+    if (perSMR >= perSM) {
+      AL = AR;
+      smem = smemR;
+      stageRecords = true;
+    } else {
+      check(configure_adjoint_kernel(W, smem), "cudaFuncSetAttribute");
+    }
+  }
   teams_ = std::min(opt_.count, perSM * I.info.multiprocessors);
   const auto count = static_cast<std::size_t>(opt_.count);
   const auto NS = static_cast<std::size_t>(I.nsamples);
@@ -191,6 +210,7 @@ float AdjointBatch::run() {
   I.queue.alloc(1); check(cudaMemsetAsync(I.queue.get(), 0, I.queue.bytes(), s), "memset");
   I.ckpt.alloc(static_cast<std::size_t>(teams_) * maxCkpt * recSize);
   I.stepOff.alloc(static_cast<std::size_t>(teams_) * (static_cast<std::size_t>(maxSteps) + 1));
+  I.recBytes.alloc(static_cast<std::size_t>(teams_) * (static_cast<std::size_t>(maxSteps) + 1));
   // the rings: at least K records of the largest size per team (one segment); up to a whole run of them when memory
   // allows. Unless the caller set a budget: a whole run of records with two passes per node (nodes take about 1.2 on
   // average), within half the device memory free at the first run; the ring is kept for later runs.
@@ -224,7 +244,8 @@ float AdjointBatch::run() {
   if (!I.hOrder.empty()) I.order.upload(I.hOrder, s);
   R.order = I.hOrder.empty() ? nullptr : I.order.get();
   R.K = K; R.maxCkpt = maxCkpt; R.ckpt = I.ckpt.get();
-  R.arena = I.arena.get(); R.arenaBytes = I.ringBytes; R.stepOff = I.stepOff.get();
+  R.arena = I.arena.get(); R.arenaBytes = I.ringBytes; R.stepOff = I.stepOff.get(); R.recBytes = I.recBytes.get();
+  R.stageRecords = stageRecords ? 1 : 0;
   R.tapeForward = I.ringBytes > minRing ? 1 : 0; R.sink = I.sink.get(); R.isink = I.isink.get();
   R.phaseNs = I.phase.get();
   R.recomputed = I.recomputed.get();

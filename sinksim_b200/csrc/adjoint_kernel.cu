@@ -110,6 +110,7 @@ struct AdjInst {
 
 // Per-team shared memory: the forward slot, then the reverse's arrays.
 struct AdjSmem {
+  unsigned char* raw;   // one packed step record (stageRecords), or null
   adj::RevSlot rs;
   adj::AdjState as;
   double* grad;      // [nc]
@@ -138,6 +139,7 @@ __device__ __forceinline__ AdjSmem carve_adjoint(unsigned char* base, const AdjL
   m.grad = d(A.grad);
   m.sampleS = d(A.sampleS);
   m.tape = base + A.tape;
+  m.raw = A.raw ? base + A.raw : nullptr;
   m.poff = reinterpret_cast<std::int32_t*>(base + A.poff);
   return m;
 }
@@ -301,6 +303,7 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
   double* const ckpt = B.ckpt + static_cast<std::size_t>(team) * B.maxCkpt * recSize;
   unsigned char* const ring = B.arena + static_cast<std::size_t>(team) * B.arenaBytes;
   long long* const off = B.stepOff + static_cast<std::size_t>(team) * (B.maxSteps + 1);
+  std::int32_t* const rb = B.recBytes + static_cast<std::size_t>(team) * (B.maxSteps + 1);
   double* const sink = B.sink + static_cast<std::size_t>(team) * (M.evCap + M.nmon + M.nmark + 1);
   std::int32_t* const isink = B.isink + static_cast<std::size_t>(team) * (M.evCap + 1);
   const adj::Tape sp = adj::tape_at(A.tape, TL);
@@ -366,7 +369,9 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
         T.sync();
         v = ring_place(v, B.arenaBytes, recMax);
         if (T.leader()) off[s] = v;
-        v += static_cast<long long>(store_record(sp, M.nn, A.poff, ring + v % static_cast<long long>(B.arenaBytes), T));
+        const std::size_t bytes = store_record(sp, M.nn, A.poff, ring + v % static_cast<long long>(B.arenaBytes), T);
+        if (T.leader()) rb[s] = static_cast<std::int32_t>(bytes);
+        v += static_cast<long long>(bytes);
       } else {
         team_step<false, W>(M, F, R, S, I, T);
       }
@@ -417,7 +422,9 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
           team_step<false, W>(M, F, R, S, I, T, GpuTape{sp});
           T.sync();
           if (T.leader()) off[st] = w;
-          w += static_cast<long long>(store_record(sp, M.nn, A.poff, ring + w, T));
+          const std::size_t bytes = store_record(sp, M.nn, A.poff, ring + w, T);
+          if (T.leader()) rb[st] = static_cast<std::int32_t>(bytes);
+          w += static_cast<long long>(bytes);
           F = make_pose(M, R.zO, R.pitch, R.roll);
         }
       }
@@ -425,15 +432,34 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
       T.sync();
       const long long tRev = global_ns();
       tRecompute += tRev - tSeg;
+      bool staged = false;  // the record of step st is in the raw buffer (copied while step st + 1 was reversed)
       for (long long st = s1 - 1; st >= s0; --st) {
-        if (T.leader() && st > s0) {
-          // the next step's record (the one before this) into L2 while this one is reversed: it runs from its own
-          // offset to this record's (a whole number of 16-byte units inside the ring, the unused end of a lap included)
-          const long long o0 = off[st - 1], o1 = off[st];
-          const auto* next = ring + o0 % static_cast<long long>(B.arenaBytes);
-          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(next), "r"(static_cast<unsigned>(o1 - o0)) : "memory");
+        if (staged) {
+          asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's copies; the barrier makes all of them visible
+          T.sync();
+          load_record(A.raw, sp, M.nn, T);
+        } else {
+          load_record(ring + off[st] % static_cast<long long>(B.arenaBytes), sp, M.nn, T);
         }
-        load_record(ring + off[st] % static_cast<long long>(B.arenaBytes), sp, M.nn, T);
+        staged = false;
+        if (st > s0) {
+          const unsigned char* next = ring + off[st - 1] % static_cast<long long>(B.arenaBytes);
+          if (B.stageRecords) {
+            // the next step's record (the one before this) into shared memory while this one is reversed: 16-byte
+            // asynchronous copies spread over the team (records and the buffer are 16-byte aligned, their sizes whole
+            // numbers of 16 bytes)
+            const int chunks = rb[st - 1] / 16;
+            for (int k = T.rank; k < chunks; k += 32 * W) {
+              const auto dst = static_cast<unsigned>(__cvta_generic_to_shared(A.raw + 16 * k));
+              asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(next + 16 * k) : "memory");
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            staged = true;
+          } else if (T.leader()) {
+            // or at least into L2
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(next), "r"(static_cast<unsigned>(rb[st - 1])) : "memory");
+          }
+        }
         adj::reverse_step(AT, M, sp, I.en(), I.area(), I.tOn(), A.rs, A.as, aSc, A.grad, &err);
         for (int q = 0; q < NS; ++q)
           if (static_cast<long long>(A.sampleS[q]) == st) {
@@ -460,7 +486,7 @@ __global__ void __launch_bounds__(W * 32) adjoint_batch(DevModel M, AdjRun B, Sl
 
 }  // namespace
 
-AdjLayout adjoint_layout(int nn, int nc, int ng, int nsamples, int W) {
+AdjLayout adjoint_layout(int nn, int nc, int ng, int nsamples, int W, bool withRaw) {
   AdjLayout A{};
   std::uint32_t off = 0;
   auto take16 = [&](std::size_t bytes) {
@@ -483,6 +509,7 @@ AdjLayout adjoint_layout(int nn, int nc, int ng, int nsamples, int W) {
   A.nunits = take16(sizeof(std::int32_t));
   A.pw = take16(2 * C);
   A.replays = take16(sizeof(adj::Replay) * static_cast<std::size_t>(std::max(nn, 1)));
+  A.raw = withRaw ? take16(record_bytes(adj::tape_layout(nn, ng), nn, nn * adj::kMaxPasses)) : 0;
   A.aVol = take16(N); A.aLevel = take16(N); A.aCx = take16(N); A.aCy = take16(N); A.aCz = take16(N);
   A.grad = take16(C);
   A.sampleS = take16(sizeof(double) * static_cast<std::size_t>(std::max(nsamples, 1)));

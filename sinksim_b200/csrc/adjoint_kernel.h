@@ -40,7 +40,10 @@ struct AdjRun {
   unsigned char* arena;
   std::size_t arenaBytes;
   long long* stepOff;
+  std::int32_t* recBytes;                       // [teams x (maxSteps + 1)] each step record's bytes
   std::int32_t tapeForward;
+  std::int32_t stageRecords;                    // 1: the layout has a raw record buffer (AdjLayout::raw): the reverse
+                                                // copies the next step's record into it while it reverses this one
   double* sink;                                 // [teams x (evCap + nmon + nmark + 1)]
   std::int32_t* isink;                          // [teams x (evCap + 1)]
   long long* phaseNs;                           // [count x 3] the team's time on the instance (globaltimer ns):
@@ -50,11 +53,12 @@ struct AdjRun {
 
 // Byte offsets of a team's reverse arrays in shared memory, after its forward slot.
 struct AdjLayout {
-  std::uint32_t hEff, aEff, dV, volPost, deg, clip, aVolPost, aCxs, aCys, aCzs, aVs, aAcc, aZmx, aLs, aAs, faHA, faHB, faAA, faAB, red, work, plain, units, nunits, pw, replays;
+  std::uint32_t hEff, aEff, dV, volPost, deg, clip, aVolPost, aCxs, aCys, aCzs, aVs, aAcc, aZmx, aLs, aAs, faHA, faHB, faAA, faAB, red, work, plain, units, nunits, pw, replays, raw;
   std::uint32_t aVol, aLevel, aCx, aCy, aCz, grad, sampleS, tape, poff, bytes;
 };
 
-AdjLayout adjoint_layout(int nn, int nc, int ng, int nsamples, int teamWarps);
+// withRaw: room for one packed step record of the largest size (the reverse's asynchronous copy of the next record)
+AdjLayout adjoint_layout(int nn, int nc, int ng, int nsamples, int teamWarps, bool withRaw = false);
 std::size_t adjoint_tape_bytes(int nn, int ng);  // the largest packed step record
 std::size_t adjoint_record_bytes(int nn, int ng, int passRecords);  // a packed step record holding passRecords passes
 cudaError_t configure_adjoint_kernel(int teamWarps, std::size_t smem);
